@@ -1,0 +1,170 @@
+/*
+ * medusa_b200.h -- C ABI of libmedusa_b200.so, the B200 (sm_100a) BSP
+ * superstep engine for Medusa's BFS, SSSP and PageRank apps.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (MB_OK == 0).  Array arguments may be host or device pointers: device
+ * pointers are used in place, host pointers are staged through pinned memory.
+ * One mb_ctx per host thread; a context owns one CUDA stream and all device
+ * scratch; a graph is device-resident until mb_graph_destroy.
+ *
+ * Sentinels match the reference: BFS unreached level = -1
+ * (Algorithm/Message.h:10, Algorithm/main.cu:225-231), SSSP unreached
+ * distance = 1e9f (MEDUSA_MAX, SSSP/Configuration.h:6, SSSP/main.cu:324).
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef MEDUSA_B200_H
+#define MEDUSA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MB_OK 0
+#define MB_ERR_INVALID 1     /* bad argument (null handle, id out of range, ...) */
+#define MB_ERR_CUDA 2        /* a CUDA runtime call failed; see mb_last_error */
+#define MB_ERR_OOM 3         /* device or pinned allocation failed */
+#define MB_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define MB_ERR_UNSUPPORTED 5 /* size or feature outside this build's limits */
+
+/* ---- graph build flags ---------------------------------------------------- */
+/* Out-edges of a vertex in input order. */
+#define MB_ORDER_INPUT 0u
+/* Out-edges of a vertex in reverse input order: the AA order the reference
+ * gets from GraphIR::AddEdge prepending (MedusaRT/GraphConverter.cu:191-192)
+ * and EdgeArray::buildAA walking each list (SSSP/EdgeDataType.cu:146-157). */
+#define MB_ORDER_REFERENCE 1u
+
+/* ---- schedule policies (which kernel runs each superstep) ---------------- */
+#define MB_POLICY_FIXED 0       /* the fixed rule: frontier-size thresholds */
+#define MB_POLICY_LEARNED 1     /* the trained MLP scheduler, run on the device */
+#define MB_POLICY_FORCED 2      /* one schedule id for every superstep */
+#define MB_POLICY_ORACLE_BEST 3 /* replay a per-superstep schedule list */
+
+/* Schedule ids.  Every schedule computes identical results; they differ in
+ * direction, thread mapping, frontier format and combine fusion only. */
+#define MB_SCHED_PUSH_EDGE_QUEUE 0 /* push, edge-balanced (merge-path), queue */
+#define MB_SCHED_PUSH_WARP_QUEUE 1 /* push, warp-per-vertex + CTA-per-hub, queue */
+#define MB_SCHED_PUSH_EDGE_BITMAP 2 /* push, edge-balanced over a bitmap frontier */
+#define MB_SCHED_PUSH_WARP_BITMAP 3 /* push, warp-per-vertex over a bitmap frontier */
+#define MB_SCHED_PULL_THREAD 4     /* pull, thread-per-vertex, bitmap frontier */
+#define MB_SCHED_PULL_WARP 5       /* pull, warp-per-vertex, bitmap frontier */
+#define MB_SCHED_PUSH_UNFUSED 6    /* push into an E-slot message array, then a
+                                      separate segmented combine + update (the
+                                      reference's send/combine/update split) */
+#define MB_SCHED_PULL_UNFUSED 7    /* pull all edges into messages, then combine */
+#define MB_NUM_SCHEDULES 8
+
+/* ---- synthetic graph generators ------------------------------------------- */
+#define MB_GEN_RMAT 0    /* R-MAT, V = 2^scale, duplicates and self-loops kept */
+#define MB_GEN_UNIFORM 1 /* src and dst i.i.d. uniform in [0,V) */
+#define MB_GEN_GRID 2    /* rows x cols 4-neighbour grid, bidirectional, with
+                            dropped edges and random long-range shortcuts */
+
+typedef struct mb_ctx mb_ctx;
+typedef struct mb_graph mb_graph;
+
+typedef struct mb_gen_params {
+    int32_t kind;          /* MB_GEN_* */
+    int32_t scale;         /* RMAT: V = 2^scale */
+    int64_t num_vertices;  /* UNIFORM: V */
+    int64_t num_edges;     /* RMAT, UNIFORM: E */
+    double a, b, c;        /* RMAT quadrant probabilities (d = 1-a-b-c) */
+    int32_t rows, cols;    /* GRID */
+    double drop_frac;      /* GRID: fraction of undirected grid edges dropped */
+    double shortcut_frac;  /* GRID: shortcut pairs as a fraction of V */
+    int32_t wmin, wmax;    /* integer weights in [wmin,wmax] stored as float;
+                              wmax == 0: unweighted (all 1) */
+    uint64_t seed;
+} mb_gen_params;
+
+typedef struct mb_stats {
+    int32_t supersteps;        /* BSP supersteps run (for batched runs: max) */
+    int32_t status_flags;      /* nonzero: a device-side check tripped */
+    int64_t edges_traversed;   /* E_r: sum of out-degrees of reached vertices,
+                                  summed over sources (the reference's
+                                  traversal count, Algorithm/CPUFunctorHoster.cpp:21) */
+    int64_t vertices_reached;  /* summed over sources */
+    double device_ms;          /* device time of the superstep loop (CUDA events) */
+    int32_t schedule_count[MB_NUM_SCHEDULES]; /* supersteps run per schedule */
+} mb_stats;
+
+/* ---- library / context ---------------------------------------------------- */
+const char *mb_version(void);
+
+/* Create a context on CUDA device `device`.
+ * Replaces InitConfig + medusaSetDevice + InitCUDA
+ * (MultipleGPU/MultiPublicAPI.h:16-39, MultipleGPU/MultiGraphStorage.cu:31-47,
+ *  MedusaRT/Utilities.cu:InitCUDA); one GPU only. */
+int mb_create(int device, mb_ctx **out);
+int mb_destroy(mb_ctx *ctx);
+/* Text of the last error on this context (never NULL). */
+const char *mb_last_error(const mb_ctx *ctx);
+/* Select the per-superstep schedule policy (MB_POLICY_*); `schedule` is the
+ * schedule id for MB_POLICY_FORCED and ignored otherwise. */
+int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule);
+/* 1: run whole iteration loops as CUDA graphs with device-side convergence
+ * (no host round trip per superstep); 0: host-driven loop, one flag read per
+ * superstep, as the reference's ResetToExecute/RetriveToExecute loop
+ * (MultipleGPU/MultiUtilities.h:48-69). */
+int mb_set_graph_capture(mb_ctx *ctx, int enable);
+
+/* ---- graph storage ----------------------------------------------------------- */
+/* Build a device-resident graph (CSR + reverse CSR + message slots) from an
+ * edge list in insertion order.  w may be NULL (unweighted).
+ * Replaces GTGraph::get_parition's single-partition path + GraphIR::AddEdge +
+ * InitHostDS + InitDeviceDS (MultipleGPU/PartitionManager.cu:116-534,
+ * MedusaRT/GraphConverter.cu:180-196, MultipleGPU/MultiPublicAPI.h:43-96,144-308)
+ * and EdgeArray::buildAA / VertexArray::build (SSSP/EdgeDataType.cu:138-186,
+ * SSSP/VertexDataType.cu:64-85). */
+int mb_graph_from_edges(mb_ctx *ctx, int32_t num_vertices, int64_t num_edges,
+                        const int32_t *src, const int32_t *dst, const float *w,
+                        uint32_t flags, mb_graph **out);
+/* Generate a seeded synthetic graph directly in device memory (no reference
+ * counterpart: the reference reads GTgraph files). */
+int mb_graph_generate(mb_ctx *ctx, const mb_gen_params *params, uint32_t flags,
+                      mb_graph **out);
+/* The same generator on the host (CPU), for checking: with src == NULL only
+ * *num_edges_out is written (grid graphs have a seeded, data-dependent E). */
+int mb_generate_edges_host(const mb_gen_params *params, int32_t *src, int32_t *dst,
+                           float *w, int64_t *num_edges_out);
+int mb_graph_info(const mb_graph *g, int32_t *num_vertices, int64_t *num_edges);
+/* Copy the device layout back (any pointer may be NULL):
+ * row[V+1], col[E], w[E] (CSR); rrow[V+1], rcol[E] (reverse CSR);
+ * mslot[E] (the reference's msgDstID). Replaces D_EdgeArray/D_VertexArray::Dump. */
+int mb_graph_export(mb_ctx *ctx, const mb_graph *g, int32_t *row, int32_t *col,
+                    float *w, int32_t *rrow, int32_t *rcol, int32_t *mslot);
+int mb_graph_destroy(mb_graph *g);
+
+/* ---- apps (one BSP iteration loop each) ---------------------------------------- */
+/* BFS levels from each of nsrc sources: levels_out[s*V + v] (-1 unreached).
+ * nsrc > 1 runs the sources batched (64-bit per-vertex source masks).
+ * Replaces the BFS app's BSP loop + Medusa_Exec + FunctorHolder<EDGE>
+ * (Algorithm/main.cu:284-300, Algorithm/UserOperators.h:17-58,
+ *  MultipleGPU/MultiAPIHoster.h:653-679) and D_VertexArray::Dump. */
+int mb_bfs(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc,
+           int32_t *levels_out, mb_stats *stats);
+/* SSSP distances from each of nsrc sources: dist_out[s*V + v] (1e9 unreached).
+ * Replaces SSSP's BSP loop + Medusa_Exec (InitMessageBuffer, ssspEdgeProcAA,
+ * Medusa_Combiner::combineAllDevice with CUDPP_MIN, FunctorHolder<VERTEX>)
+ * (SSSP/main.cu:369-382, SSSP/UserOperators.h:10-29,151-168,200-264,
+ *  MedusaRT/Combiner.cu:82-142). */
+int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc,
+            float *dist_out, mb_stats *stats);
+/* `iters` PageRank supersteps, rank = 0.15 + 0.85 * sum(rank[u]/outdeg[u]),
+ * from a uniform initial rank `init`; rank_out[V].
+ * Replaces MPG's BSP loop + Medusa_Exec (InitMessageBuffer, SendMsgMEG,
+ * combineAllDevice with CUDPP_ADD, FunctorHolder<VERTEX>)
+ * (MPG/main.cu:148-169, MPG/UserOperators.h:16-43,119-144,175-270). */
+int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
+                float *rank_out, mb_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEDUSA_B200_H */

@@ -1,0 +1,270 @@
+"""ctypes binding of libmedusa_b200.so (the C ABI in include/medusa_b200.h).
+
+This is plumbing for Python callers, tests and the benchmark: every call goes
+straight to the CUDA library, and there is no CPU fallback -- if the shared
+library is missing or cannot load, importing the binding raises.
+
+Arrays may be numpy arrays (host memory; results are copied back) or CUDA
+torch tensors (device memory, used in place).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmedusa_b200.so")
+
+MB_OK = 0
+MB_ERR_INVALID, MB_ERR_CUDA, MB_ERR_OOM, MB_ERR_TIMEOUT, MB_ERR_UNSUPPORTED = 1, 2, 3, 4, 5
+MB_ORDER_INPUT, MB_ORDER_REFERENCE = 0, 1
+MB_POLICY_FIXED, MB_POLICY_LEARNED, MB_POLICY_FORCED, MB_POLICY_ORACLE_BEST = 0, 1, 2, 3
+MB_GEN_RMAT, MB_GEN_UNIFORM, MB_GEN_GRID = 0, 1, 2
+NUM_SCHEDULES = 8
+SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
+                  "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
+MEDUSA_MAX = np.float32(1e9)
+
+
+class MedusaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("medusa_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class GenParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("scale", ctypes.c_int32),
+                ("num_vertices", ctypes.c_int64), ("num_edges", ctypes.c_int64),
+                ("a", ctypes.c_double), ("b", ctypes.c_double), ("c", ctypes.c_double),
+                ("rows", ctypes.c_int32), ("cols", ctypes.c_int32),
+                ("drop_frac", ctypes.c_double), ("shortcut_frac", ctypes.c_double),
+                ("wmin", ctypes.c_int32), ("wmax", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("supersteps", ctypes.c_int32), ("status_flags", ctypes.c_int32),
+                ("edges_traversed", ctypes.c_int64), ("vertices_reached", ctypes.c_int64),
+                ("device_ms", ctypes.c_double),
+                ("schedule_count", ctypes.c_int32 * NUM_SCHEDULES)]
+
+    def as_dict(self):
+        return {"supersteps": self.supersteps, "status_flags": self.status_flags,
+                "edges_traversed": self.edges_traversed,
+                "vertices_reached": self.vertices_reached, "device_ms": self.device_ms,
+                "schedule_count": list(self.schedule_count)}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libmedusa_b200.so is not built: run `python -m medusa_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I32, I64, U32, F32 = (ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
+                             ctypes.c_float)
+    sigs = {
+        "mb_version": (ctypes.c_char_p, []),
+        "mb_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(P)]),
+        "mb_destroy": (ctypes.c_int, [P]),
+        "mb_last_error": (ctypes.c_char_p, [P]),
+        "mb_set_schedule_policy": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
+        "mb_set_graph_capture": (ctypes.c_int, [P, ctypes.c_int]),
+        "mb_graph_from_edges": (ctypes.c_int, [P, I32, I64, P, P, P, U32, ctypes.POINTER(P)]),
+        "mb_graph_generate": (ctypes.c_int, [P, ctypes.POINTER(GenParams), U32,
+                                             ctypes.POINTER(P)]),
+        "mb_generate_edges_host": (ctypes.c_int, [ctypes.POINTER(GenParams), P, P, P,
+                                                  ctypes.POINTER(I64)]),
+        "mb_graph_info": (ctypes.c_int, [P, ctypes.POINTER(I32), ctypes.POINTER(I64)]),
+        "mb_graph_export": (ctypes.c_int, [P, P, P, P, P, P, P, P]),
+        "mb_graph_destroy": (ctypes.c_int, [P]),
+        "mb_bfs": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
+        "mb_sssp": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
+        "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def version():
+    return lib.mb_version().decode()
+
+
+def _ptr(x):
+    """Address of a numpy array or torch tensor (host or device)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        if not x.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return x.data_ptr()
+    raise TypeError("expected a numpy array or a torch tensor, got %r" % type(x))
+
+
+def _check(rc, ctx=None):
+    if rc != MB_OK:
+        msg = lib.mb_last_error(ctx).decode(errors="replace")
+        raise MedusaError(rc, msg)
+
+
+def gen_params(kind, seed=1, scale=0, num_vertices=0, num_edges=0, a=0.57, b=0.19, c=0.19,
+               rows=0, cols=0, drop_frac=0.0, shortcut_frac=0.0, wmin=0, wmax=0):
+    return GenParams(kind, scale, num_vertices, num_edges, a, b, c, rows, cols, drop_frac,
+                     shortcut_frac, wmin, wmax, seed)
+
+
+def rmat_params(scale, num_edges, a, b, c, seed=1, wmin=0, wmax=0):
+    return gen_params(MB_GEN_RMAT, seed=seed, scale=scale, num_edges=num_edges, a=a, b=b, c=c,
+                      wmin=wmin, wmax=wmax)
+
+
+def uniform_params(num_vertices, num_edges, seed=1, wmin=0, wmax=0):
+    return gen_params(MB_GEN_UNIFORM, seed=seed, num_vertices=num_vertices, num_edges=num_edges,
+                      wmin=wmin, wmax=wmax)
+
+
+def grid_params(rows, cols, drop_frac=0.1, shortcut_frac=0.005, seed=1, wmin=1, wmax=100):
+    return gen_params(MB_GEN_GRID, seed=seed, rows=rows, cols=cols, drop_frac=drop_frac,
+                      shortcut_frac=shortcut_frac, wmin=wmin, wmax=wmax)
+
+
+def num_vertices_of(p):
+    if p.kind == MB_GEN_RMAT:
+        return 1 << p.scale
+    if p.kind == MB_GEN_UNIFORM:
+        return int(p.num_vertices)
+    return int(p.rows) * int(p.cols)
+
+
+def generate_edges_host(p, weighted=None):
+    """The seeded generator run on the host: (V, src, dst, w or None)."""
+    E = ctypes.c_int64(0)
+    _check(lib.mb_generate_edges_host(ctypes.byref(p), None, None, None, ctypes.byref(E)))
+    n = E.value
+    src = np.empty(max(n, 1), np.int32)
+    dst = np.empty(max(n, 1), np.int32)
+    if weighted is None:
+        weighted = p.wmax > 0
+    w = np.empty(max(n, 1), np.float32) if weighted else None
+    _check(lib.mb_generate_edges_host(ctypes.byref(p), src.ctypes.data, dst.ctypes.data,
+                                      None if w is None else w.ctypes.data, ctypes.byref(E)))
+    return num_vertices_of(p), src[:n], dst[:n], (None if w is None else w[:n])
+
+
+class Graph:
+    """A device-resident graph (CSR + reverse CSR + message slots)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = ctypes.c_void_p(handle)
+        V = ctypes.c_int32(0)
+        E = ctypes.c_int64(0)
+        _check(lib.mb_graph_info(self.h, ctypes.byref(V), ctypes.byref(E)))
+        self.V, self.E = V.value, E.value
+
+    def close(self):
+        if self.h:
+            lib.mb_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export(self):
+        """Device layout as numpy arrays: row, col, w, rrow, rcol, mslot."""
+        V, E = self.V, self.E
+        row = np.empty(V + 1, np.int32)
+        rrow = np.empty(V + 1, np.int32)
+        col = np.empty(max(E, 1), np.int32)
+        w = np.empty(max(E, 1), np.float32)
+        rcol = np.empty(max(E, 1), np.int32)
+        mslot = np.empty(max(E, 1), np.int32)
+        _check(lib.mb_graph_export(self.ctx.h, self.h, row.ctypes.data, col.ctypes.data,
+                                   w.ctypes.data, rrow.ctypes.data, rcol.ctypes.data,
+                                   mslot.ctypes.data), self.ctx.h)
+        return {"row": row, "col": col[:E], "w": w[:E], "rrow": rrow, "rcol": rcol[:E],
+                "mslot": mslot[:E]}
+
+    def bfs(self, sources, out=None):
+        src = np.ascontiguousarray(np.atleast_1d(sources), dtype=np.int32)
+        if out is None:
+            out = np.empty((len(src), self.V), np.int32)
+        st = Stats()
+        _check(lib.mb_bfs(self.ctx.h, self.h, src.ctypes.data, len(src), _ptr(out),
+                          ctypes.byref(st)), self.ctx.h)
+        return out, st.as_dict()
+
+    def sssp(self, sources, out=None):
+        src = np.ascontiguousarray(np.atleast_1d(sources), dtype=np.int32)
+        if out is None:
+            out = np.empty((len(src), self.V), np.float32)
+        st = Stats()
+        _check(lib.mb_sssp(self.ctx.h, self.h, src.ctypes.data, len(src), _ptr(out),
+                           ctypes.byref(st)), self.ctx.h)
+        return out, st.as_dict()
+
+    def pagerank(self, iters, init=None, out=None):
+        if init is None:
+            init = 1.0 / self.V
+        if out is None:
+            out = np.empty(self.V, np.float32)
+        st = Stats()
+        _check(lib.mb_pagerank(self.ctx.h, self.h, int(iters), float(init), _ptr(out),
+                               ctypes.byref(st)), self.ctx.h)
+        return out, st.as_dict()
+
+
+class Context:
+    """One CUDA device, one stream, and the device scratch of every run."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        _check(lib.mb_create(int(device), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.mb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_policy(self, policy, schedule=0):
+        _check(lib.mb_set_schedule_policy(self.h, int(policy), int(schedule)), self.h)
+
+    def set_graph_capture(self, enable):
+        _check(lib.mb_set_graph_capture(self.h, 1 if enable else 0), self.h)
+
+    def graph_from_edges(self, V, src, dst, w=None, reference_order=True):
+        src = src if hasattr(src, "data_ptr") else np.ascontiguousarray(src, dtype=np.int32)
+        dst = dst if hasattr(dst, "data_ptr") else np.ascontiguousarray(dst, dtype=np.int32)
+        if w is not None and not hasattr(w, "data_ptr"):
+            w = np.ascontiguousarray(w, dtype=np.float32)
+        E = int(src.shape[0])
+        g = ctypes.c_void_p()
+        flags = MB_ORDER_REFERENCE if reference_order else MB_ORDER_INPUT
+        _check(lib.mb_graph_from_edges(self.h, int(V), E, _ptr(src) if E else None,
+                                       _ptr(dst) if E else None, _ptr(w) if E else None,
+                                       flags, ctypes.byref(g)), self.h)
+        return Graph(self, g.value)
+
+    def generate(self, params, reference_order=True):
+        g = ctypes.c_void_p()
+        flags = MB_ORDER_REFERENCE if reference_order else MB_ORDER_INPUT
+        _check(lib.mb_graph_generate(self.h, ctypes.byref(params), flags, ctypes.byref(g)),
+               self.h)
+        return Graph(self, g.value)

@@ -1,0 +1,92 @@
+"""Build libmedusa_b200.so in-tree from medusa_b200/csrc/*.cu for sm_100a.
+
+    python -m medusa_b200.build [--force] [--jobs N]
+
+nvcc compiles each .cu file to an object (in parallel) with
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and links them into
+``medusa_b200/libmedusa_b200.so`` (static cudart, OpenMP for the host-side
+generators).  No GPU is needed to build.
+"""
+import argparse
+import glob
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libmedusa_b200.so")
+ROOT = os.path.dirname(HERE)
+NVCC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
+           "-Xcompiler", "-fPIC,-fopenmp,-O3", "-I", os.path.join(ROOT, "include")] + ARCH
+
+
+def _sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _headers():
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+            + glob.glob(os.path.join(ROOT, "include", "*.h")))
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, jobs=None, verbose=False):
+    """Compile (when stale) and return the path of the shared library."""
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = _sources()
+    hdrs = _headers()
+    todo = []
+    objs = []
+    for s in srcs:
+        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            todo.append((s, o))
+
+    def cc(job):
+        s, o = job
+        cmd = [NVCC] + NVFLAGS + ["-c", s, "-o", o]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed on %s:\n%s" % (s, r.stderr[-6000:]))
+        return r.stderr
+
+    if todo:
+        with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+            for err in ex.map(cc, todo):
+                if verbose and err.strip():
+                    print(err)
+    if force or todo or _stale(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n%s" % r.stderr[-6000:])
+    return LIB
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--force", action="store_true")
+    p.add_argument("--jobs", type=int, default=None)
+    p.add_argument("-v", "--verbose", action="store_true")
+    a = p.parse_args(argv)
+    print(build(force=a.force, jobs=a.jobs, verbose=a.verbose))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

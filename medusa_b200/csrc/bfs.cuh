@@ -1,0 +1,28 @@
+// bfs.cuh -- BFS app state (internal).
+#pragma once
+#include "engine.cuh"
+
+namespace mb {
+
+struct BfsState : FrontierState {
+    DevBuf level, vis;
+    ~BfsState() { release(); }
+    void release() {
+        release_frontier();
+        level.release();
+        vis.release();
+    }
+    void ensure(const Graph &g) {
+        if (ensure_frontier(g)) {
+            level.release();
+            vis.release();
+            level.reserve(sizeof(int32_t) * (size_t)g.V);
+            vis.reserve(sizeof(uint32_t) * (size_t)W);
+        }
+    }
+};
+
+// One BFS from `source`; levels are left in st.level (device).
+void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats);
+
+}  // namespace mb

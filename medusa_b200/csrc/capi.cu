@@ -1,0 +1,327 @@
+// capi.cu -- the extern "C" boundary of libmedusa_b200.so (include/medusa_b200.h).
+//
+// Every entry point catches everything and returns a status code; the text
+// of the last error is kept per context (and per thread for calls made
+// without a usable context).  Array arguments may be host or device pointers.
+#include <cstring>
+#include <new>
+#include "bfs.cuh"
+#include "pagerank.cuh"
+#include "sched.cuh"
+#include "sssp.cuh"
+
+namespace mb {
+struct AppStates {
+    BfsState bfs;
+    SsspState sssp;
+    PrState pr;
+};
+int64_t generate_edges_host(const mb_gen_params &p, int32_t *src, int32_t *dst, float *w);
+void graph_generate(Context &ctx, Graph &g, const mb_gen_params &p, uint32_t flags);
+}  // namespace mb
+
+struct mb_ctx {
+    mb::Context c;
+};
+struct mb_graph {
+    mb::Graph g;
+};
+
+namespace {
+
+thread_local std::string t_last_error;
+
+int set_error(mb_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->c.last_error = msg;
+    t_last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(mb_ctx *ctx, F &&f) {
+    try {
+        f();
+        return MB_OK;
+    } catch (const mb::ApiError &e) {
+        return set_error(ctx, e.code, e.msg);
+    } catch (const mb::CudaError &e) {
+        std::string m = std::string(cudaGetErrorName(e.err)) + " (" + cudaGetErrorString(e.err) +
+                        ") in " + e.what + " at " + e.file + ":" + std::to_string(e.line);
+        cudaGetLastError();
+        return set_error(ctx, e.err == cudaErrorMemoryAllocation ? MB_ERR_OOM : MB_ERR_CUDA, m);
+    } catch (const std::bad_alloc &) {
+        return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return set_error(ctx, MB_ERR_INVALID, e.what());
+    }
+}
+
+void use_device(mb_ctx *ctx) { MB_CUDA(cudaSetDevice(ctx->c.device)); }
+
+mb::AppStates &apps(mb_graph *g) {
+    if (!g->g.apps) g->g.apps = new mb::AppStates();
+    return *g->g.apps;
+}
+
+// Copy n int32 from a host or device pointer to host.
+std::vector<int32_t> fetch_i32(const int32_t *p, int64_t n) {
+    std::vector<int32_t> out((size_t)n);
+    if (n > 0) MB_CUDA(cudaMemcpy(out.data(), p, sizeof(int32_t) * (size_t)n, cudaMemcpyDefault));
+    return out;
+}
+
+void check_graph(mb_ctx *ctx, const mb_graph *g) {
+    if (!ctx || !g) mb::fail(MB_ERR_INVALID, "null context or graph");
+    if (g->g.device != ctx->c.device) mb::fail(MB_ERR_INVALID, "graph lives on another device");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mb_version(void) { return "medusa_b200 0.1 (sm_100a)"; }
+
+int mb_create(int device, mb_ctx **out) {
+    if (!out) return set_error(nullptr, MB_ERR_INVALID, "out is null");
+    *out = nullptr;
+    mb_ctx *ctx = new (std::nothrow) mb_ctx();
+    if (!ctx) return set_error(nullptr, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        int n = 0;
+        MB_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) mb::fail(MB_ERR_INVALID, "no such CUDA device");
+        MB_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        MB_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10) mb::fail(MB_ERR_UNSUPPORTED, "this build targets sm_100a (B200)");
+        ctx->c.device = device;
+        ctx->c.num_sms = prop.multiProcessorCount;
+        MB_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        MB_CUDA(cudaMallocHost((void **)&ctx->c.pinned_small, mb::Context::kSmallBytes));
+        ctx->c.mlp.reserve(sizeof(float) * mb::kMlpParams);
+        MB_CUDA(cudaMemset(ctx->c.mlp.p, 0, sizeof(float) * mb::kMlpParams));
+    });
+    if (rc != MB_OK) {
+        t_last_error = ctx->c.last_error;
+        mb_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return MB_OK;
+}
+
+int mb_destroy(mb_ctx *ctx) {
+    if (!ctx) return MB_OK;
+    cudaSetDevice(ctx->c.device);
+    if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    for (auto &b : ctx->c.scratch) b.release();
+    ctx->c.mlp.release();
+    if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
+    if (ctx->c.pinned_small) cudaFreeHost(ctx->c.pinned_small);
+    if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return MB_OK;
+}
+
+const char *mb_last_error(const mb_ctx *ctx) {
+    return ctx ? ctx->c.last_error.c_str() : t_last_error.c_str();
+}
+
+int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    if (policy < MB_POLICY_FIXED || policy > MB_POLICY_ORACLE_BEST)
+        return set_error(ctx, MB_ERR_INVALID, "unknown policy");
+    if (policy == MB_POLICY_FORCED && (schedule < 0 || schedule >= MB_NUM_SCHEDULES))
+        return set_error(ctx, MB_ERR_INVALID, "schedule id out of range");
+    if (policy == MB_POLICY_LEARNED && !ctx->c.mlp_ready)
+        return set_error(ctx, MB_ERR_INVALID, "the learned scheduler has no weights yet");
+    ctx->c.schedule_policy = policy;
+    ctx->c.fixed_schedule = schedule;
+    return MB_OK;
+}
+
+int mb_set_graph_capture(mb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    ctx->c.use_graphs = enable != 0;
+    return MB_OK;
+}
+
+int mb_graph_from_edges(mb_ctx *ctx, int32_t V, int64_t E, const int32_t *src, const int32_t *dst,
+                        const float *w, uint32_t flags, mb_graph **out) {
+    if (!ctx || !out) return set_error(ctx, MB_ERR_INVALID, "null context or out");
+    *out = nullptr;
+    if (V < 1) return set_error(ctx, MB_ERR_INVALID, "num_vertices must be >= 1");
+    if (E < 0 || (E > 0 && (!src || !dst))) return set_error(ctx, MB_ERR_INVALID, "bad edge arrays");
+    if (E > 0x7FFFFFFFll) return set_error(ctx, MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
+    if (flags & ~MB_ORDER_REFERENCE) return set_error(ctx, MB_ERR_INVALID, "unknown flags");
+    mb_graph *g = new (std::nothrow) mb_graph();
+    if (!g) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        mb::DevBuf bs, bd, bw;
+        try {
+            const size_t eb = sizeof(uint32_t) * (size_t)std::max<int64_t>(E, 1);
+            bs.reserve(eb);
+            bd.reserve(eb);
+            if (w) bw.reserve(eb);
+            if (E > 0) {
+                MB_CUDA(cudaMemcpy(bs.p, src, 4 * (size_t)E, cudaMemcpyDefault));
+                MB_CUDA(cudaMemcpy(bd.p, dst, 4 * (size_t)E, cudaMemcpyDefault));
+                if (w) MB_CUDA(cudaMemcpy(bw.p, w, 4 * (size_t)E, cudaMemcpyDefault));
+            }
+            mb::graph_build_from_device_edges(ctx->c, g->g, V, E, bs.as<uint32_t>(),
+                                              bd.as<uint32_t>(), w ? bw.as<float>() : nullptr, flags);
+        } catch (...) {
+            bs.release(); bd.release(); bw.release();
+            throw;
+        }
+        bs.release(); bd.release(); bw.release();
+    });
+    if (rc != MB_OK) {
+        mb_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return MB_OK;
+}
+
+int mb_graph_generate(mb_ctx *ctx, const mb_gen_params *p, uint32_t flags, mb_graph **out) {
+    if (!ctx || !out || !p) return set_error(ctx, MB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (flags & ~MB_ORDER_REFERENCE) return set_error(ctx, MB_ERR_INVALID, "unknown flags");
+    mb_graph *g = new (std::nothrow) mb_graph();
+    if (!g) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        if (p->kind != MB_GEN_GRID && p->num_edges > 0x7FFFFFFFll)
+            mb::fail(MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
+        mb::graph_generate(ctx->c, g->g, *p, flags);
+    });
+    if (rc != MB_OK) {
+        mb_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return MB_OK;
+}
+
+int mb_generate_edges_host(const mb_gen_params *p, int32_t *src, int32_t *dst, float *w,
+                           int64_t *num_edges_out) {
+    if (!p || !num_edges_out) return set_error(nullptr, MB_ERR_INVALID, "null argument");
+    return guarded(nullptr, [&] {
+        if (src && !dst) mb::fail(MB_ERR_INVALID, "dst is null");
+        *num_edges_out = mb::generate_edges_host(*p, src, dst, w);
+    });
+}
+
+int mb_graph_info(const mb_graph *g, int32_t *V, int64_t *E) {
+    if (!g) return set_error(nullptr, MB_ERR_INVALID, "null graph");
+    if (V) *V = g->g.V;
+    if (E) *E = g->g.E;
+    return MB_OK;
+}
+
+int mb_graph_export(mb_ctx *ctx, const mb_graph *g, int32_t *row, int32_t *col, float *w,
+                    int32_t *rrow, int32_t *rcol, int32_t *mslot) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, g);
+        use_device(ctx);
+        const mb::Graph &G = g->g;
+        const size_t vb = sizeof(int32_t) * (size_t)(G.V + 1), eb = sizeof(int32_t) * (size_t)G.E;
+        if (row) MB_CUDA(cudaMemcpy(row, G.row.p, vb, cudaMemcpyDefault));
+        if (rrow) MB_CUDA(cudaMemcpy(rrow, G.rrow.p, vb, cudaMemcpyDefault));
+        if (G.E > 0) {
+            if (col) MB_CUDA(cudaMemcpy(col, G.col.p, eb, cudaMemcpyDefault));
+            if (w) MB_CUDA(cudaMemcpy(w, G.wt.p, eb, cudaMemcpyDefault));
+            if (rcol) MB_CUDA(cudaMemcpy(rcol, G.rcol.p, eb, cudaMemcpyDefault));
+            if (mslot) MB_CUDA(cudaMemcpy(mslot, G.mslot.p, eb, cudaMemcpyDefault));
+        }
+    });
+}
+
+int mb_graph_destroy(mb_graph *g) {
+    if (!g) return MB_OK;
+    cudaSetDevice(g->g.device);
+    cudaDeviceSynchronize();
+    delete g->g.apps;
+    g->g.apps = nullptr;
+    g->g.release();
+    delete g;
+    return MB_OK;
+}
+
+int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc,
+           int32_t *levels_out, mb_stats *stats) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (nsrc < 1 || !sources || !levels_out) mb::fail(MB_ERR_INVALID, "bad sources/output");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        const int32_t V = g->g.V;
+        std::vector<int32_t> src = fetch_i32(sources, nsrc);
+        for (int32_t s : src)
+            if (s < 0 || s >= V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
+        mb_stats total{};
+        for (int32_t i = 0; i < nsrc; i++) {
+            mb_stats st{};
+            mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st);
+            MB_CUDA(cudaMemcpyAsync(levels_out + (size_t)i * V, apps(g).bfs.level.p,
+                                    sizeof(int32_t) * (size_t)V, cudaMemcpyDefault, ctx->c.stream));
+            total.supersteps = std::max(total.supersteps, st.supersteps);
+            total.status_flags |= st.status_flags;
+            total.edges_traversed += st.edges_traversed;
+            total.vertices_reached += st.vertices_reached;
+            total.device_ms += st.device_ms;
+            for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+        }
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        if (stats) *stats = total;
+    });
+}
+
+int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc, float *dist_out,
+            mb_stats *stats) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (nsrc < 1 || !sources || !dist_out) mb::fail(MB_ERR_INVALID, "bad sources/output");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        const int32_t V = g->g.V;
+        std::vector<int32_t> src = fetch_i32(sources, nsrc);
+        for (int32_t s : src)
+            if (s < 0 || s >= V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
+        mb_stats total{};
+        for (int32_t i = 0; i < nsrc; i++) {
+            mb_stats st{};
+            mb::run_sssp(ctx->c, g->g, apps(g).sssp, src[i], &st);
+            MB_CUDA(cudaMemcpyAsync(dist_out + (size_t)i * V, apps(g).sssp.dist.p,
+                                    sizeof(float) * (size_t)V, cudaMemcpyDefault, ctx->c.stream));
+            total.supersteps = std::max(total.supersteps, st.supersteps);
+            total.status_flags |= st.status_flags;
+            total.edges_traversed += st.edges_traversed;
+            total.vertices_reached += st.vertices_reached;
+            total.device_ms += st.device_ms;
+            for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+        }
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        if (stats) *stats = total;
+    });
+}
+
+int mb_pagerank(mb_ctx *ctx, const mb_graph *gc, int32_t iters, float init, float *rank_out,
+                mb_stats *stats) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (iters < 0 || !rank_out) mb::fail(MB_ERR_INVALID, "bad iters/output");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        const int sched = ctx->c.schedule_policy == MB_POLICY_FORCED ? ctx->c.fixed_schedule
+                                                                      : MB_SCHED_PUSH_EDGE_QUEUE;
+        mb::run_pagerank(ctx->c, g->g, apps(g).pr, iters, init, sched, stats);
+        MB_CUDA(cudaMemcpyAsync(rank_out, apps(g).pr.rank.p, sizeof(float) * (size_t)g->g.V,
+                                cudaMemcpyDefault, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+}  // extern "C"

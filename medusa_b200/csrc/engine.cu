@@ -1,0 +1,85 @@
+// engine.cu -- host side of the superstep engine: run parameters and the
+// loop driver (one CUDA-graph launch per run, or the host-driven loop).
+#include "engine.cuh"
+
+namespace mb {
+
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source) {
+    static_assert(sizeof(RunParams) <= Context::kCtrlOff, "params staging too small");
+    static_assert(sizeof(Ctrl) <= Context::kSmallBytes - Context::kCtrlOff, "ctrl readback too small");
+    RunParams *p = (RunParams *)(ctx.pinned_small + Context::kParamsOff);
+    p->source = source;
+    p->policy = ctx.schedule_policy;
+    p->forced = ctx.fixed_schedule < 0 ? 0 : ctx.fixed_schedule;
+    p->nreplay = (int32_t)std::min<size_t>(ctx.replay.size(), kMaxReplay);
+    for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
+    const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
+    MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));
+}
+
+void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
+    cudaStream_t s = ctx.stream;
+    const int nbranch = 2 * MB_NUM_SCHEDULES;
+    FrontierState &st = *sp.st;
+    const FrontierArgs &fa = sp.fa;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    try {
+        if (ctx.use_graphs) {
+            if (!st.lg.exec || st.owner != (const void *)&ctx || st.owner_mlp != (const void *)fa.mlp) {
+                const int cap = sp.cap;
+                build_loop_graph(
+                    st.lg, s, nbranch, sp.prologue,
+                    [&](cudaStream_t cs, cudaGraphConditionalHandle hc,
+                        cudaGraphConditionalHandle hb) {
+                        k_select<<<1, 32, 0, cs>>>(fa.ctrl, fa.mlp, cap, hc, hb, nbranch, 1);
+                        MB_CHECK_LAUNCH();
+                    },
+                    sp.branch, sp.epilogue);
+                st.owner = &ctx;
+                st.owner_mlp = fa.mlp;
+            }
+            MB_CUDA(cudaEventRecord(e0, s));
+            MB_CUDA(cudaGraphLaunch(st.lg.exec, s));
+            MB_CUDA(cudaEventRecord(e1, s));
+        } else {
+            MB_CUDA(cudaEventRecord(e0, s));
+            sp.prologue(s);
+            Ctrl *hc = (Ctrl *)ctx.ctrl_readback();
+            for (;;) {
+                k_select<<<1, 32, 0, s>>>(fa.ctrl, fa.mlp, sp.cap, 0, 0, nbranch, 0);
+                MB_CHECK_LAUNCH();
+                MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+                MB_CUDA(cudaStreamSynchronize(s));
+                if (hc->done) break;
+                sp.branch(hc->branch, s);
+            }
+            if (sp.epilogue) sp.epilogue(s);
+            MB_CUDA(cudaEventRecord(e1, s));
+        }
+        MB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        MB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        Ctrl *hc = (Ctrl *)ctx.ctrl_readback();
+        MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+        MB_CUDA(cudaStreamSynchronize(s));
+        if (hc->err & ERR_STEP_CAP) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": superstep cap reached");
+        if (stats) {
+            stats->supersteps = hc->supersteps;
+            stats->status_flags = hc->err;
+            stats->edges_traversed = (int64_t)hc->edges_reached;
+            stats->vertices_reached = (int64_t)hc->reached;
+            stats->device_ms = ms;
+            for (int i = 0; i < MB_NUM_SCHEDULES; i++) stats->schedule_count[i] = hc->sched_count[i];
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+}  // namespace mb

@@ -1,0 +1,303 @@
+// pagerank.cu -- the PageRank app's BSP superstep on sm_100a.
+//
+// Reference (MPG/UserOperators.h:16-43,119-144,175-270; combiner with
+// CUDPP_ADD; CPU form MPG/CPUFunctorHoster.cpp:17-31,60-93,143-163):
+//   send    msg = rank[u] / outdeg[u] (float) on every out-edge of u
+//   combine sum of the messages of each destination
+//   update  rank[v] = 0.15 + 0.85 * sum, with the reference's rounding:
+//           sum *= 0.85 is a double multiply rounded to float, and
+//           0.15 + sum a double add rounded to float.
+// No dangling-rank redistribution; a vertex with no in-edges gets 0.15.
+//
+// The sum runs in a fixed order, the same for every schedule, so schedules
+// never change a bit of the result:
+//   in-degree <= kHubBlock: a sequential fold over the in-edges in reverse-CSR
+//     order -- the order the reference's msgDstID hands out message slots, so
+//     these vertices match a sequential CPU sum bit for bit;
+//   larger in-degrees ("hubs"): sequential folds over consecutive blocks of
+//     kHubBlock in-edges, then a sequential fold of the block sums.
+// Schedules: 0 fused pull (gather rank/outdeg through shared memory, fold,
+// update, write the next contribution -- one kernel per superstep); 6 the
+// reference's split: send into the E-slot message array at msgDstID, then
+// the same combine+update reading the messages.
+#include <algorithm>
+#include <vector>
+#include "pagerank.cuh"
+
+namespace mb {
+namespace {
+
+constexpr int kHubBlock = 2048;          // in-edges per hub block
+constexpr int kWin = 1024;               // edges staged per warp per window
+constexpr int kPrWarps = 8;              // warps per CTA
+constexpr int kPrThreads = kPrWarps * 32;
+
+struct PrArgs {
+    int32_t V;
+    int64_t E;
+    const int32_t *rrow, *rcol, *outdeg, *row, *mslot;
+    const float *contrib_in;   // rank[u]/outdeg[u] of the previous superstep
+    float *contrib_out;
+    float *rank_out;
+    float *msg;                // E-slot message array (schedule 6)
+    const int32_t *hub_v;      // hub vertices
+    const int32_t *hub_first;  // first block of each hub (nhub+1 entries)
+    const int32_t *blk_v;      // hub of each block
+    int32_t nhub, nblk;
+    float *blk_sum;            // per-block partial sums
+};
+
+__device__ __forceinline__ float pr_update(float sum) {
+    // MPG/UserOperators.h:22-23: "msg_sum *= 0.85; set_level(0.15 + msg_sum)"
+    const float s = (float)((double)sum * 0.85);
+    return (float)(0.15 + (double)s);
+}
+
+__device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) {
+    const float r = pr_update(sum);
+    a.rank_out[v] = r;
+    const int32_t d = a.outdeg[v];
+    a.contrib_out[v] = d > 0 ? r / (float)d : 0.0f;  // MPG/CPUFunctorHoster.cpp:80-82
+}
+
+template <bool kFromMsg>
+__device__ __forceinline__ float edge_val(const PrArgs &a, int64_t j) {
+    if (kFromMsg) return a.msg[j];
+    return __ldg(&a.contrib_in[a.rcol[j]]);
+}
+
+// Hub blocks: thread per block, sequential fold of its kHubBlock edges.
+template <bool kFromMsg>
+__global__ void k_hub_blocks(PrArgs a) {
+    for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < a.nblk; b += gridDim.x * blockDim.x) {
+        const int32_t h = a.blk_v[b];
+        const int32_t v = a.hub_v[h];
+        const int64_t j0 = (int64_t)a.rrow[v] + (int64_t)(b - a.hub_first[h]) * kHubBlock;
+        const int64_t j1 = min((int64_t)a.rrow[v + 1], j0 + kHubBlock);
+        float s = 0.f;
+        for (int64_t j = j0; j < j1; j++) s += edge_val<kFromMsg>(a, j);
+        a.blk_sum[b] = s;
+    }
+}
+
+// Main combine+update: one warp per 32 consecutive vertices.  The warp
+// streams the group's in-edges (contiguous in reverse-CSR order) through a
+// shared-memory window, coalesced; each lane then folds its own vertex's
+// part of the window in order.
+template <bool kFromMsg>
+__global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
+    __shared__ float win[kPrWarps][kWin];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float *wv = win[wid];
+    const int64_t ngroups = ((int64_t)a.V + 31) / 32;
+    const int64_t warps = (int64_t)gridDim.x * kPrWarps;
+    for (int64_t grp = (int64_t)blockIdx.x * kPrWarps + wid; grp < ngroups; grp += warps) {
+        const int32_t v = (int32_t)(grp * 32 + lane);
+        const bool valid = v < a.V;
+        const int32_t vb = (int32_t)(grp * 32);
+        const int32_t ve = (int32_t)min(grp * 32 + 32, (int64_t)a.V);
+        int64_t b = 0, e = 0;
+        if (valid) {
+            b = a.rrow[v];
+            e = a.rrow[v + 1];
+        }
+        const bool hub = valid && (e - b) > kHubBlock;
+        const int64_t g0 = a.rrow[vb], g1 = a.rrow[ve];
+        float sum = 0.f;
+        // hub vertices are excluded from the window pass
+        const unsigned hubmask = __ballot_sync(0xffffffffu, hub);
+        for (int64_t w0 = g0; w0 < g1; w0 += kWin) {
+            const int64_t w1 = min(w0 + (int64_t)kWin, g1);
+            // skip windows that lie entirely inside hub ranges
+            const bool mine = !hub && b < w1 && e > w0;
+            if (!__any_sync(0xffffffffu, mine)) continue;
+#pragma unroll 8
+            for (int k = lane; k < kWin; k += 32) {
+                const int64_t j = w0 + k;
+                if (j < w1) wv[k] = edge_val<kFromMsg>(a, j);
+            }
+            __syncwarp();
+            if (mine) {
+                const int64_t lo = max(b, w0), hi = min(e, w1);
+                for (int64_t j = lo; j < hi; j++) sum += wv[j - w0];
+            }
+            __syncwarp();
+        }
+        if (hubmask && hub) {
+            // fold this hub's block sums in order (k_hub_blocks ran before)
+            int32_t h = 0, lo = 0, hi = a.nhub;  // binary search hub id
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (a.hub_v[mid] < v) lo = mid + 1; else hi = mid;
+            }
+            h = lo;
+            sum = 0.f;
+            for (int32_t k = a.hub_first[h]; k < a.hub_first[h + 1]; k++) sum += a.blk_sum[k];
+        }
+        if (valid) pr_write(a, v, sum);
+    }
+}
+
+// Schedule 6, send (SendMsgAA, MPG/UserOperators.h:48-70): every vertex
+// writes its contribution into the message slot of each out-edge.
+__global__ void k_pr_send(PrArgs a) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < a.V;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const float m = a.contrib_in[u];
+        for (int32_t e = a.row[u]; e < a.row[u + 1]; e++) a.msg[a.mslot[e]] = m;
+    }
+}
+
+__global__ void k_pr_init(const int32_t *outdeg, int32_t V, float init, float *contrib) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < V;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = outdeg[u];
+        contrib[u] = d > 0 ? init / (float)d : 0.0f;
+    }
+}
+
+__global__ void k_fill(float *x, int32_t n, float v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+
+}  // namespace
+
+void PrState::ensure(Context &ctx, const Graph &g) {
+    if (built && V == g.V && E == g.E) return;
+    release();
+    V = g.V;
+    E = g.E;
+    rank.reserve(sizeof(float) * (size_t)V);
+    contrib[0].reserve(sizeof(float) * (size_t)V);
+    contrib[1].reserve(sizeof(float) * (size_t)V);
+    msg.reserve(sizeof(float) * (size_t)std::max<int64_t>(E, 1));
+    // hub table, built once per graph from the in-degree offsets
+    std::vector<int32_t> rrow(V + 1);
+    MB_CUDA(cudaMemcpy(rrow.data(), g.rrow.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> hv, hf, bv;
+    for (int32_t v = 0; v < V; v++) {
+        const int64_t d = (int64_t)rrow[v + 1] - rrow[v];
+        if (d > kHubBlock) {
+            hf.push_back((int32_t)bv.size());
+            const int32_t nb = (int32_t)((d + kHubBlock - 1) / kHubBlock);
+            for (int32_t k = 0; k < nb; k++) bv.push_back((int32_t)hv.size());
+            hv.push_back(v);
+        }
+    }
+    hf.push_back((int32_t)bv.size());
+    nhub = (int32_t)hv.size();
+    nblk = (int32_t)bv.size();
+    hub_v.reserve(sizeof(int32_t) * std::max<size_t>(hv.size(), 1));
+    hub_first.reserve(sizeof(int32_t) * hf.size());
+    blk_v.reserve(sizeof(int32_t) * std::max<size_t>(bv.size(), 1));
+    blk_sum.reserve(sizeof(float) * std::max<size_t>(bv.size(), 1));
+    if (nhub) MB_CUDA(cudaMemcpy(hub_v.p, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice));
+    MB_CUDA(cudaMemcpy(hub_first.p, hf.data(), 4 * hf.size(), cudaMemcpyHostToDevice));
+    if (nblk) MB_CUDA(cudaMemcpy(blk_v.p, bv.data(), 4 * bv.size(), cudaMemcpyHostToDevice));
+    built = true;
+    (void)ctx;
+}
+
+void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init, int sched,
+                  mb_stats *stats) {
+    st.ensure(ctx, g);
+    cudaStream_t s = ctx.stream;
+    const bool unfused = sched == MB_SCHED_PUSH_UNFUSED;
+    auto args = [&](int parity) {
+        PrArgs a;
+        a.V = g.V;
+        a.E = g.E;
+        a.rrow = g.rrow.as<int32_t>();
+        a.rcol = g.rcol.as<int32_t>();
+        a.outdeg = g.outdeg.as<int32_t>();
+        a.row = g.row.as<int32_t>();
+        a.mslot = g.mslot.as<int32_t>();
+        a.contrib_in = st.contrib[parity].as<float>();
+        a.contrib_out = st.contrib[parity ^ 1].as<float>();
+        a.rank_out = st.rank.as<float>();
+        a.msg = st.msg.as<float>();
+        a.hub_v = st.hub_v.as<int32_t>();
+        a.hub_first = st.hub_first.as<int32_t>();
+        a.blk_v = st.blk_v.as<int32_t>();
+        a.nhub = st.nhub;
+        a.nblk = st.nblk;
+        a.blk_sum = st.blk_sum.as<float>();
+        return a;
+    };
+    const int grid_pull = ctx.num_sms * 8;
+    const int grid_vtx = ctx.num_sms * 8;
+    auto emit = [&](cudaStream_t cs) {
+        k_pr_init<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init, st.contrib[0].as<float>());
+        MB_CHECK_LAUNCH();
+        for (int it = 0; it < iters; it++) {
+            PrArgs a = args(it & 1);
+            if (unfused) {
+                k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
+                if (a.nblk) k_hub_blocks<true><<<grid_for(a.nblk, 128, 4096), 128, 0, cs>>>(a);
+                k_pr_pull<true><<<grid_pull, kPrThreads, 0, cs>>>(a);
+            } else {
+                if (a.nblk) k_hub_blocks<false><<<grid_for(a.nblk, 128, 4096), 128, 0, cs>>>(a);
+                k_pr_pull<false><<<grid_pull, kPrThreads, 0, cs>>>(a);
+            }
+            MB_CHECK_LAUNCH();
+        }
+        if (iters == 0) {  // no superstep: the ranks are the initial ranks
+            k_fill<<<grid_vtx, 256, 0, cs>>>(st.rank.as<float>(), g.V, init);
+            MB_CHECK_LAUNCH();
+        }
+    };
+    cudaEvent_t e0, e1;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    try {
+        if (ctx.use_graphs) {
+            if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_sched != sched) {
+                if (st.exec) cudaGraphExecDestroy(st.exec);
+                st.exec = nullptr;
+                cudaGraph_t gr;
+                MB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                try {
+                    emit(s);
+                } catch (...) {
+                    cudaStreamEndCapture(s, &gr);
+                    throw;
+                }
+                MB_CUDA(cudaStreamEndCapture(s, &gr));
+                cudaError_t e = cudaGraphInstantiate(&st.exec, gr, 0);
+                cudaGraphDestroy(gr);
+                MB_CUDA(e);
+                st.g_iters = iters;
+                st.g_init = init;
+                st.g_sched = sched;
+            }
+            MB_CUDA(cudaEventRecord(e0, s));
+            MB_CUDA(cudaGraphLaunch(st.exec, s));
+            MB_CUDA(cudaEventRecord(e1, s));
+        } else {
+            MB_CUDA(cudaEventRecord(e0, s));
+            emit(s);
+            MB_CUDA(cudaEventRecord(e1, s));
+        }
+        MB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        MB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (stats) {
+            *stats = mb_stats{};
+            stats->supersteps = iters;
+            stats->edges_traversed = (int64_t)iters * g.E;
+            stats->vertices_reached = g.V;
+            stats->device_ms = ms;
+            stats->schedule_count[unfused ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE] = iters;
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+}  // namespace mb

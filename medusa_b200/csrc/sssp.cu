@@ -1,0 +1,497 @@
+// sssp.cu -- the SSSP app's BSP superstep on sm_100a.
+//
+// Reference (SSSP/UserOperators.h:10-29,151-168,200-264; combiner
+// MedusaRT/Combiner.cu:82-142 with CUDPP_MIN; CPU form
+// SSSP/CPUFunctorHoster.cpp:15-99): each superstep fills an E-slot message
+// array with FLT_MAX, every updated vertex writes dist[u]+w into the slot of
+// each out-edge, a segmented min-scan combines the slots of each destination,
+// and every vertex whose combined message is below its distance takes it and
+// is "updated" for the next superstep.  The fixpoint is the exact
+// shortest-path distance (1e9 = MEDUSA_MAX when unreachable): the weights are
+// integers stored as float and every path length is an integer below 2^24,
+// so float sums and minima are exact and the result does not depend on
+// relaxation order.  Hence every schedule below yields bit-identical output.
+//
+// Fused schedules combine in the send: atomicMin on the float's bit pattern
+// (non-negative floats order like their uint32 bits) and the "updated" set
+// is the set of vertices whose distance dropped, deduplicated per superstep by
+// a stamp (stamp[v] == s+1 once v joined superstep s+1's frontier).
+//
+//   0 push, merge-path edge-balanced, queue frontier
+//   1 push, warp-per-vertex, queue frontier
+//   2 push, warp-wide edge-balanced over a bitmap frontier
+//   3 push, warp-per-vertex over a bitmap frontier
+//   4 pull (min over in-edges from frontier vertices), thread-per-vertex
+//   5 pull, warp-per-vertex
+//   6 the reference's split: message fill, send into msg[mslot[e]],
+//     segmented min per destination, update
+//   7 full Bellman-Ford pull over every in-edge (the reference CPU form)
+#include "sssp.cuh"
+
+namespace mb {
+namespace {
+
+struct SsspArgs {
+    FrontierArgs f;
+    const int32_t *row, *col, *rrow, *rcol, *mslot;
+    const float *wt, *rwt;
+    float *dist;
+    int32_t *stamp;
+    float *msg;
+};
+
+__device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
+    return __ldcg(&a.dist[v]);  // bypass L1: other SMs lower distances
+}
+
+// Lower dist[v] to nd; true for exactly one caller per (v, superstep) that
+// lowered it, who then puts v into the next frontier.
+__device__ __forceinline__ bool relax(const SsspArgs &a, int32_t v, float nd, int32_t stamp_val) {
+    if (!(nd < ld_dist(a, v))) return false;
+    const unsigned old = atomicMin((unsigned *)&a.dist[v], __float_as_uint(nd));
+    if (!(nd < __uint_as_float(old))) return false;
+    return atomicExch(&a.stamp[v], stamp_val) != stamp_val;
+}
+
+// schedule 0: push, merge-path edge-balanced over the queue
+__global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
+    __shared__ uint32_t s_off[kTile + 1];
+    __shared__ int32_t s_row[kTile + 1];
+    __shared__ float s_du[kTile + 1];
+    Ctrl *c = a.f.ctrl;
+    const int cur = c->cur, nxt = cur ^ 1;
+    const uint64_t q = c->q[cur];
+    const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
+    const int32_t sv = c->step + 1;
+    const int32_t *qv = a.f.qv[cur];
+    const uint32_t *qo = a.f.qo[cur];
+    const int32_t *tf = a.f.tf[cur];
+    const uint32_t tiles = (m + kTile - 1) / kTile;
+    uint32_t cn = 0;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t c0 = t * kTile, c1 = min(c0 + kTile, m);
+        const int32_t i0 = tf[t];
+        const int32_t i1 = (t + 1 < tiles) ? tf[t + 1] : (int32_t)n - 1;
+        const int k = i1 - i0 + 1;
+        for (int j = threadIdx.x; j < k; j += blockDim.x) {
+            const int32_t u = qv[i0 + j];
+            s_off[j] = qo[i0 + j];
+            s_row[j] = a.row[u];
+            s_du[j] = ld_dist(a, u);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kTileItems; r++) {
+            const uint32_t e_idx = c0 + r * kPushThreads + threadIdx.x;
+            bool own = false;
+            int32_t v = 0;
+            uint32_t deg = 0;
+            if (e_idx < c1) {
+                const int j = upper_bound_minus1(s_off, k, e_idx);
+                const int32_t e = s_row[j] + (int32_t)(e_idx - s_off[j]);
+                v = a.col[e];
+                if (relax(a, v, s_du[j] + a.wt[e], sv)) {
+                    deg = (uint32_t)a.f.outdeg[v];
+                    own = true;
+                    cn++;
+                }
+            }
+            enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], a.f.qv[nxt], a.f.qo[nxt], a.f.tf[nxt]);
+        }
+        __syncthreads();
+    }
+    flush_counts(c, cn, 0);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+}
+
+// schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
+__global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    const int cur = c->cur, nxt = cur ^ 1;
+    const uint32_t n = (uint32_t)(c->q[cur] >> 32);
+    const int32_t sv = c->step + 1;
+    const int32_t *qv = a.f.qv[cur];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    auto visit = [&](bool valid, int32_t e, float du) {
+        bool own = false;
+        int32_t v = 0;
+        uint32_t deg = 0;
+        if (valid) {
+            v = a.col[e];
+            if (relax(a, v, du + a.wt[e], sv)) {
+                deg = (uint32_t)a.f.outdeg[v];
+                own = true;
+                cn++;
+            }
+        }
+        enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], a.f.qv[nxt], a.f.qo[nxt], a.f.tf[nxt]);
+    };
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n;
+         base += warps * 32) {
+        const int64_t i = base + lane;
+        int32_t u = 0, st = 0;
+        uint32_t deg = 0;
+        float du = 0.f;
+        if (i < n) {
+            u = qv[i];
+            st = a.row[u];
+            deg = (uint32_t)a.f.outdeg[u];
+            du = ld_dist(a, u);
+        }
+        unsigned big = __ballot_sync(0xffffffffu, deg >= 32);
+        while (big) {
+            const int l = __ffs(big) - 1;
+            big &= big - 1;
+            const int32_t bst = __shfl_sync(0xffffffffu, st, l);
+            const uint32_t bdeg = __shfl_sync(0xffffffffu, deg, l);
+            const float bdu = __shfl_sync(0xffffffffu, du, l);
+            for (uint32_t k = 0; k < bdeg; k += 32)
+                visit(k + lane < bdeg, bst + (int32_t)(k + lane), bdu);
+        }
+        const uint32_t sd = deg < 32 ? deg : 0u;
+        const uint32_t incl = warp_incl_scan_u32(sd);
+        warp_gather(incl, sd, st, [&](bool valid, int32_t e, int owner) {
+            const float odu = __shfl_sync(0xffffffffu, du, owner);
+            visit(valid, e, odu);
+        });
+    }
+    flush_counts(c, cn, 0);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+}
+
+// an improved vertex joins the bitmap frontier of the next superstep
+__device__ __forceinline__ void improve_bm(const SsspArgs &a, uint32_t *next, int32_t v, float nd,
+                                           int32_t sv, uint32_t &cn, uint64_t &cm) {
+    if (relax(a, v, nd, sv)) {
+        atomicOr(&next[v >> 5], 1u << (v & 31));
+        cn++;
+        cm += (uint32_t)a.f.outdeg[v];
+    }
+}
+
+// schedules 2 and 3: push over a bitmap frontier; one warp per word
+template <bool kEdgeBalanced>
+__global__ void __launch_bounds__(kPushThreads) k_push_bm(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    const uint32_t *front = a.f.bm[c->bcur];
+    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const int32_t sv = c->step + 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    uint64_t cm = 0;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
+        const uint32_t word = front[w];
+        if (!word) continue;
+        const int32_t u = (int32_t)(w * 32 + lane);
+        const bool in = (word >> lane) & 1u;
+        const int32_t st = in ? a.row[u] : 0;
+        const uint32_t deg = in ? (uint32_t)a.f.outdeg[u] : 0u;
+        const float du = in ? ld_dist(a, u) : 0.f;
+        if (kEdgeBalanced) {
+            const uint32_t incl = warp_incl_scan_u32(deg);
+            warp_gather(incl, deg, st, [&](bool valid, int32_t e, int owner) {
+                const float odu = __shfl_sync(0xffffffffu, du, owner);
+                if (valid) improve_bm(a, next, a.col[e], odu + a.wt[e], sv, cn, cm);
+            });
+        } else {
+            unsigned live = __ballot_sync(0xffffffffu, deg > 0);
+            while (live) {
+                const int l = __ffs(live) - 1;
+                live &= live - 1;
+                const int32_t bst = __shfl_sync(0xffffffffu, st, l);
+                const uint32_t bdeg = __shfl_sync(0xffffffffu, deg, l);
+                const float bdu = __shfl_sync(0xffffffffu, du, l);
+                for (uint32_t k = lane; k < bdeg; k += 32) {
+                    const int32_t e = bst + (int32_t)k;
+                    improve_bm(a, next, a.col[e], bdu + a.wt[e], sv, cn, cm);
+                }
+            }
+        }
+    }
+    flush_counts(c, cn, cm);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+// Pull epilogue of one word: lanes whose `found` is set lowered their vertex
+// to `best`; the warp writes the next-frontier word (it owns it).
+__device__ __forceinline__ void pull_commit(const SsspArgs &a, uint32_t *next, int64_t w, int32_t v,
+                                            bool found, float best, int32_t sv, uint32_t &cn,
+                                            uint64_t &cm) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, found);
+    if ((threadIdx.x & 31) == 0) next[w] = mask;
+    if (found) {
+        a.dist[v] = best;
+        a.stamp[v] = sv;
+        cn++;
+        cm += (uint32_t)a.f.outdeg[v];
+    }
+}
+
+constexpr int kPullLaneCap = 64;
+
+// schedule 4: pull, thread-per-vertex with a warp-cooperative tail
+__global__ void __launch_bounds__(256) k_pull_thread(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    const uint32_t *front = a.f.bm[c->bcur];
+    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const int32_t sv = c->step + 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    uint64_t cm = 0;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
+        const int32_t v = (int32_t)(w * 32 + lane);
+        const bool valid = v < a.f.V;
+        int32_t j = 0, je = 0;
+        float cur_d = 0.f, best = 0.f;
+        if (valid) {
+            j = a.rrow[v];
+            je = a.rrow[v + 1];
+            cur_d = ld_dist(a, v);
+            best = cur_d;
+            const int32_t jcap = min(je, j + kPullLaneCap);
+            for (; j < jcap; j++) {
+                const int32_t u = a.rcol[j];
+                if (test_bit(front, u)) best = fminf(best, ld_dist(a, u) + a.rwt[j]);
+            }
+        }
+        unsigned pend = __ballot_sync(0xffffffffu, j < je);
+        while (pend) {
+            const int l = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const int32_t pj = __shfl_sync(0xffffffffu, j, l);
+            const int32_t pje = __shfl_sync(0xffffffffu, je, l);
+            float m = 3.0e38f;
+            for (int32_t b = pj + lane; b < pje; b += 32) {
+                const int32_t u = a.rcol[b];
+                if (test_bit(front, u)) m = fminf(m, ld_dist(a, u) + a.rwt[b]);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == l) best = fminf(best, m);
+        }
+        pull_commit(a, next, w, v, valid && best < cur_d, best, sv, cn, cm);
+    }
+    flush_counts(c, cn, cm);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+// schedule 5: pull, warp-per-vertex.  mode 1: full Bellman-Ford over every
+// in-edge (schedule 7), no frontier test.
+template <bool kAllEdges>
+__global__ void __launch_bounds__(256) k_pull_warp(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    const uint32_t *front = a.f.bm[c->bcur];
+    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const int32_t sv = c->step + 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    uint64_t cm = 0;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
+        const uint32_t valid = tail_mask(w, a.f.V);
+        float mybest = 0.f, mycur = 0.f;
+        for (int l = 0; l < 32; l++) {
+            if (!((valid >> l) & 1u)) break;
+            const int32_t v = (int32_t)(w * 32 + l);
+            const int32_t jb = a.rrow[v], je = a.rrow[v + 1];
+            float m = 3.0e38f;
+            for (int32_t b = jb + lane; b < je; b += 32) {
+                const int32_t u = a.rcol[b];
+                if (kAllEdges || test_bit(front, u)) m = fminf(m, ld_dist(a, u) + a.rwt[b]);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == l) {
+                mycur = ld_dist(a, v);
+                mybest = fminf(mycur, m);
+            }
+        }
+        const int32_t v = (int32_t)(w * 32 + lane);
+        pull_commit(a, next, w, v, ((valid >> lane) & 1u) && mybest < mycur, mybest, sv, cn, cm);
+    }
+    flush_counts(c, cn, cm);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+// schedule 6, step 1 (InitMessageBuffer, SSSP/InitMessage.h:4-9): msg[] = FLT_MAX
+__global__ void k_msg_fill(SsspArgs a) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.f.E;
+         i += (int64_t)gridDim.x * blockDim.x)
+        a.msg[i] = 3.402823466e+38f;
+}
+
+// schedule 6, step 2 (ssspEdgeProcAA, SSSP/UserOperators.h:10-29): every
+// vertex updated in the last superstep writes dist+w into its edges' slots
+__global__ void k_msg_send(SsspArgs a) {
+    const int32_t s = a.f.ctrl->step;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        if (a.stamp[v] != s) continue;
+        const float d = a.dist[v];
+        for (int32_t e = a.row[v]; e < a.row[v + 1]; e++) a.msg[a.mslot[e]] = d + a.wt[e];
+    }
+}
+
+// schedule 6, step 3 (segmented min + UpdateVertex, SSSP/UserOperators.h:151-168):
+// the combined message of v is the min of its slots [rrow[v], rrow[v+1]).
+__global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const int32_t sv = c->step + 1;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    uint64_t cm = 0;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
+        const int32_t v = (int32_t)(w * 32 + (threadIdx.x & 31));
+        bool found = false;
+        float m = 3.402823466e+38f, cur_d = 0.f;
+        if (v < a.f.V) {
+            for (int32_t i = a.rrow[v]; i < a.rrow[v + 1]; i++) m = fminf(m, a.msg[i]);
+            cur_d = a.dist[v];
+            found = m < cur_d;
+        }
+        pull_commit(a, next, w, v, found, m, sv, cn, cm);
+    }
+    flush_counts(c, cn, cm);
+    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+__global__ void k_sssp_init(SsspArgs a) {
+    Ctrl *c = a.f.ctrl;
+    const int32_t source = c->p.source;
+    const int32_t deg = a.f.outdeg[source];
+    if (threadIdx.x == 0) {
+        a.dist[source] = 0.0f;
+        a.stamp[source] = 0;
+        c->cur = 0;
+        c->bcur = 0;
+        c->step = 0;
+        c->mode = FMT_QUEUE;
+        c->done = 0;
+        c->err = 0;
+        c->iter = 0;
+        c->supersteps = 0;
+        for (int i = 0; i < MB_NUM_SCHEDULES; i++) c->sched_count[i] = 0;
+        c->acc_n = 0;
+        c->acc_m = 0;
+        c->blocks_done = 0;
+        c->prev_nf = 1;
+        c->reached = 0;
+        c->edges_reached = 0;
+        c->q[1] = 0ull;
+        c->m_unvisited = a.f.E - deg;
+        c->n_unvisited = a.f.V - 1;
+        if (deg > 0) {
+            a.f.qv[0][0] = source;
+            a.f.qo[0][0] = 0;
+            c->q[0] = (1ull << 32) | (uint32_t)deg;
+        } else {
+            c->q[0] = 0ull;
+        }
+    }
+    for (int32_t t = threadIdx.x; deg > 0 && t * kTile < deg; t += blockDim.x) a.f.tf[0][t] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) choose_next(c, APP_SSSP, a.f.V, a.f.E);
+}
+
+__global__ void k_fill_dist(float *d, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = kMedusaMax;
+}
+
+__global__ void k_stats(SsspArgs a) {
+    uint32_t n = 0;
+    uint64_t m = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        if (a.dist[v] < kMedusaMax) {
+            n++;
+            m += (uint32_t)a.f.outdeg[v];
+        }
+    }
+    n = warp_sum(n);
+    m = warp_sum(m);
+    if ((threadIdx.x & 31) == 0 && (n | m)) {
+        atomicAdd((unsigned long long *)&a.f.ctrl->reached, (unsigned long long)n);
+        atomicAdd((unsigned long long *)&a.f.ctrl->edges_reached, (unsigned long long)m);
+    }
+}
+
+}  // namespace
+
+void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats) {
+    st.ensure(g);
+    SsspArgs a;
+    a.f = st.frontier_args(g, ctx.mlp_ready ? ctx.mlp.as<float>() : nullptr);
+    a.row = g.row.as<int32_t>();
+    a.col = g.col.as<int32_t>();
+    a.rrow = g.rrow.as<int32_t>();
+    a.rcol = g.rcol.as<int32_t>();
+    a.mslot = g.mslot.as<int32_t>();
+    a.wt = g.wt.as<float>();
+    a.rwt = g.rwt.as<float>();
+    a.dist = st.dist.as<float>();
+    a.stamp = st.stamp.as<int32_t>();
+    a.msg = st.msg.as<float>();
+    upload_params(ctx, st.ctrl.p, source);
+
+    const int grid_push = ctx.num_sms * 4, grid_vtx = ctx.num_sms * 8, grid_edge = ctx.num_sms * 8;
+    LoopSpec sp;
+    sp.st = &st;
+    sp.fa = a.f;
+    // each superstep lowers some distance; with integer distances below 2^24
+    // a run cannot need more supersteps than this
+    sp.cap = (int)std::min<int64_t>((int64_t)g.V * 4 + 16, 1 << 30);
+    sp.name = "sssp";
+    sp.prologue = [&](cudaStream_t s) {
+        k_fill_dist<<<grid_vtx, 256, 0, s>>>(a.dist, a.f.V);
+        MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
+        k_sssp_init<<<1, 256, 0, s>>>(a);
+        MB_CHECK_LAUNCH();
+    };
+    sp.branch = [&](int branch, cudaStream_t s) {
+        const int sched = branch % MB_NUM_SCHEDULES;
+        if (branch >= MB_NUM_SCHEDULES) {
+            if (sched_input(sched) == FMT_BITMAP) {
+                k_bm_clear<<<grid_vtx, 256, 0, s>>>(a.f, 0);
+                k_q2bm<<<grid_vtx, 256, 0, s>>>(a.f);
+            } else {
+                k_bm2q<<<grid_vtx, 256, 0, s>>>(a.f);
+            }
+            MB_CHECK_LAUNCH();
+        }
+        switch (sched) {
+            case MB_SCHED_PUSH_EDGE_QUEUE: k_push_edge_q<<<grid_push, kPushThreads, 0, s>>>(a); break;
+            case MB_SCHED_PUSH_WARP_QUEUE: k_push_warp_q<<<grid_push, kPushThreads, 0, s>>>(a); break;
+            case MB_SCHED_PUSH_EDGE_BITMAP:
+                k_bm_clear<<<grid_vtx, 256, 0, s>>>(a.f, 1);
+                k_push_bm<true><<<grid_push, kPushThreads, 0, s>>>(a);
+                break;
+            case MB_SCHED_PUSH_WARP_BITMAP:
+                k_bm_clear<<<grid_vtx, 256, 0, s>>>(a.f, 1);
+                k_push_bm<false><<<grid_push, kPushThreads, 0, s>>>(a);
+                break;
+            case MB_SCHED_PULL_THREAD: k_pull_thread<<<grid_vtx, 256, 0, s>>>(a); break;
+            case MB_SCHED_PULL_WARP: k_pull_warp<false><<<grid_vtx, 256, 0, s>>>(a); break;
+            case MB_SCHED_PUSH_UNFUSED:
+                k_msg_fill<<<grid_edge, 256, 0, s>>>(a);
+                k_msg_send<<<grid_vtx, 256, 0, s>>>(a);
+                k_msg_combine_update<<<grid_vtx, 256, 0, s>>>(a);
+                break;
+            default: k_pull_warp<true><<<grid_vtx, 256, 0, s>>>(a); break;
+        }
+        MB_CHECK_LAUNCH();
+    };
+    sp.epilogue = [&](cudaStream_t s) {
+        k_stats<<<ctx.num_sms * 4, 256, 0, s>>>(a);
+        MB_CHECK_LAUNCH();
+    };
+    run_loop(ctx, sp, stats);
+}
+
+}  // namespace mb
