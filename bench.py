@@ -1,0 +1,364 @@
+#!/usr/bin/env python3
+"""Benchmark: Medusa's BSP superstep on B200 -- BFS/SSSP GTEPS (and PageRank edges/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl medusa|reference]
+
+Workload (N=1, the configuration the metric is quoted on): R-MAT with 2^20
+vertices and 2^24 directed edges, (a,b,c,d) = (0.45,0.15,0.15,0.25), seeded,
+duplicates kept; integer weights in [1,1000] stored as float32.  One step =
+one BFS and one SSSP from source 0, each a whole BSP iteration loop.
+`value` = (BFS + SSSP traversed edges) / device time of the two loops, in
+GTEPS, where traversed edges = sum of out-degrees of reached vertices (the
+reference's count).  Inputs are resident in HBM; L2 is flushed (256 MiB
+write) before every step.  `e2e` = the same metric through the C ABI with
+pinned host buffers: the source ids go host->device and the levels and
+distances come back device->host inside the timed region.
+
+`pagerank`: PageRank on the reference's CPU-runnable configuration (uniform,
+2^18 vertices, 2^22 edges, 10 supersteps from 1/N), edges/s per superstep.
+
+Multi-GPU (torchrun): the path does not shard (one graph per GPU, as the
+reference's single-GPU path); every rank runs the full workload on its own
+replica, `value` sums all ranks' traversed edges over the max device time.
+
+`--impl reference`: the reference's own CPU superstep code (oracle/_ref),
+on this host's cores, on the same graph and metric; rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 1
+C2 = dict(scale=20, num_edges=1 << 24, a=0.45, b=0.15, c=0.15, wmin=1, wmax=1000)
+C1 = dict(num_vertices=1 << 18, num_edges=1 << 22)
+PR_ITERS = 10
+METRIC = "BFS/SSSP GTEPS (R-MAT 2^20 V / 2^24 E, source 0)"
+WORKLOAD = ("R-MAT 2^20 vertices, 2^24 edges, (a,b,c,d)=(0.45,0.15,0.15,0.25), seed 1, "
+            "weights int [1,1000] as f32; one step = BFS + SSSP from source 0")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def c2_params(api):
+    return api.rmat_params(C2["scale"], C2["num_edges"], C2["a"], C2["b"], C2["c"], seed=SEED,
+                           wmin=C2["wmin"], wmax=C2["wmax"])
+
+
+def c1_params(api):
+    return api.uniform_params(C1["num_vertices"], C1["num_edges"], seed=SEED)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                         "sw_power_cap"]
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def flush_l2(buf):
+    buf.zero_()
+
+
+def bfs_bytes(st, V):
+    # algorithmic bytes of a BFS: 8 per reached edge, 20 per reached vertex, 4 per vertex
+    return 8 * st["edges_traversed"] + 20 * st["vertices_reached"] + 4 * V
+
+
+def sssp_bytes(st, V):
+    return 12 * st["edges_traversed"] + 20 * st["vertices_reached"] + 4 * V
+
+
+def run_medusa(args):
+    import torch
+    from medusa_b200 import api
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = api.Context(local)
+    p = c2_params(api)
+    g = ctx.generate(p)
+    V = g.V
+    lv_dev = torch.empty(V, dtype=torch.int32, device=dev)
+    d_dev = torch.empty(V, dtype=torch.float32, device=dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    def step(out_l, out_d):
+        _, sb = g.bfs([0], out=out_l)
+        _, ss = g.sssp([0], out=out_d)
+        return sb, ss
+
+    for _ in range(args.warmup):
+        step(lv_dev, d_dev)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    dev_ms, edges, launches, bts = 0.0, 0, 0, 0
+    sb_last = ss_last = None
+    wall0 = time.perf_counter()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            sb, ss = step(lv_dev, d_dev)
+            dev_ms += sb["device_ms"] + ss["device_ms"]
+            edges += sb["edges_traversed"] + ss["edges_traversed"]
+            launches += sb["kernel_launches"] + ss["kernel_launches"]
+            bts += bfs_bytes(sb, V) + sssp_bytes(ss, V)
+            sb_last, ss_last = sb, ss
+        torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    t_max = dev_ms
+    if dist:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        e = torch.tensor([edges], dtype=torch.float64, device=dev)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        edges_all = float(e.item())
+    else:
+        edges_all = float(edges)
+    value = edges_all / (t_max / 1e3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers
+    lv_h = torch.empty(V, dtype=torch.int32, pin_memory=True)
+    d_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
+    e2e_wall, e2e_edges = 0.0, 0
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sb, ss = step(lv_h, d_h)
+        e2e_wall += time.perf_counter() - t0
+        e2e_edges += sb["edges_traversed"] + ss["edges_traversed"]
+    e2e_val = e2e_edges / e2e_wall / 1e9
+
+    pk, pk_kind = peaks()
+    bfs_gb = bfs_bytes(sb_last, V) / 1e9
+    sssp_gb = sssp_bytes(ss_last, V) / 1e9
+    achieved = bts / (dev_ms / 1e3) / 1e9
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "vertices": V, "edges": g.E, "sources": [0],
+                   "l2": "flushed (256 MiB write) before every step",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "schedule_policy": "fixed (direction-optimising rule)",
+                   "loop": "one CUDA graph per BSP loop (device-side convergence)"},
+        "bfs": {"gteps": round(sb_last["edges_traversed"] / sb_last["device_ms"] / 1e6, 3),
+                "ms": round(sb_last["device_ms"], 4), "supersteps": sb_last["supersteps"],
+                "edges_traversed": sb_last["edges_traversed"],
+                "vertices_reached": sb_last["vertices_reached"],
+                "schedule_count": sb_last["schedule_count"]},
+        "sssp": {"gteps": round(ss_last["edges_traversed"] / ss_last["device_ms"] / 1e6, 3),
+                 "ms": round(ss_last["device_ms"], 4), "supersteps": ss_last["supersteps"],
+                 "edges_traversed": ss_last["edges_traversed"],
+                 "schedule_count": ss_last["schedule_count"]},
+        "e2e": {"value": round(e2e_val, 3), "unit": "GTEPS", "h2d_bytes_per_step": 8,
+                "d2h_bytes_per_step": 8 * V},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk,
+                     "unit": "GB/s", "frac": round(achieved / pk, 4), "traffic": None,
+                     "peak_kind": pk_kind,
+                     "kernel": "BFS + SSSP superstep loops (one CUDA graph each)",
+                     "bytes_per_step": {"bfs": round(bfs_gb, 4), "sssp": round(sssp_gb, 4),
+                                        "unit": "GB",
+                                        "formula": "BFS 8*E_r+20*V_r+4*V; SSSP 12*E_r+20*V_r+4*V"}},
+        "gpu_launches": int(launches),
+        "wall_s": round(wall, 3),
+        "clocks": clk.summary(),
+    }
+    if not args.no_pagerank:
+        out["pagerank"] = bench_pagerank(ctx, api, args, flush)
+    g.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(api, args)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def bench_pagerank(ctx, api, args, flush):
+    import torch
+    p = c1_params(api)
+    g = ctx.generate(p)
+    V, E = g.V, g.E
+    r = torch.empty(V, dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 1)):
+        g.pagerank(PR_ITERS, 1.0 / V, out=r)
+    ms = 0.0
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        _, st = g.pagerank(PR_ITERS, 1.0 / V, out=r)
+        ms += st["device_ms"]
+    per_iter_ms = ms / args.steps / PR_ITERS
+    pk, _ = peaks()
+    b = 8 * E + 16 * V + 4
+    ach = b / (per_iter_ms / 1e3) / 1e9
+    g.close()
+    return {"workload": "uniform 2^18 vertices, 2^22 edges, seed 1, 10 supersteps from 1/N",
+            "edges_per_s": round(E / (per_iter_ms / 1e3), 1), "ms_per_superstep": round(per_iter_ms, 5),
+            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": pk, "unit": "GB/s",
+                         "frac": round(ach / pk, 4),
+                         "bytes_per_superstep": b, "formula": "8*E + 16*V + 4"}}
+
+
+def cpu_baseline(api, args):
+    """The reference's CPU path (oracle/_ref) on the same graph: one BFS + one SSSP."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref not built"}
+    V, s, d, w = api.generate_edges_host(c2_params(api))
+    nthr = min(os.cpu_count() or 1, 24)
+    gb = O.RefGraph("bfs", V, s, d)
+    lv, ms_b = gb.bfs(0, nthr)
+    gb.close()
+    gs = O.RefGraph("sssp", V, s, d, w)
+    dd, ms_s = gs.sssp(0, nthr)
+    gs.close()
+    outdeg = np.bincount(s, minlength=V)
+    er = int(outdeg[lv >= 0].sum()) + int(outdeg[dd < 1e9].sum())
+    return {"value": round(er / ((ms_b + ms_s) / 1e3) / 1e9, 5), "unit": "GTEPS",
+            "cores": nthr, "kind": "reference",
+            "sample": "one BFS + one SSSP from source 0 on the full workload graph "
+                      "(reference Medusa_Exec_CPU, OpenMP)",
+            "bfs_ms": round(ms_b, 2), "sssp_ms": round(ms_s, 2)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from medusa_b200 import api
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return
+    V, s, d, w = api.generate_edges_host(c2_params(api))
+    nthr = min(os.cpu_count() or 1, 24)
+    gb = O.RefGraph("bfs", V, s, d)
+    gs = O.RefGraph("sssp", V, s, d, w)
+    outdeg = np.bincount(s, minlength=V)
+    for _ in range(args.warmup):
+        gb.bfs(0, nthr)
+        gs.sssp(0, nthr)
+    ms, edges = 0.0, 0
+    for _ in range(args.steps):
+        lv, mb = gb.bfs(0, nthr)
+        dd, msd = gs.sssp(0, nthr)
+        ms += mb + msd
+        edges += int(outdeg[lv >= 0].sum()) + int(outdeg[dd < 1e9].sum())
+    val = edges / (ms / 1e3) / 1e9
+    out = {"impl": "reference", "metric": METRIC, "value": round(val, 5), "unit": "GTEPS",
+           "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "int32/f32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "vertices": V, "edges": int(len(s)), "sources": [0]},
+           "cpu_baseline": {"value": round(val, 5), "unit": "GTEPS", "cores": nthr,
+                            "kind": "reference",
+                            "sample": "each step: one BFS + one SSSP from source 0 on the full graph"},
+           "e2e": {"value": round(val, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    gb.close()
+    gs.close()
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="medusa", choices=["medusa", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pagerank", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_medusa(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -92,6 +92,7 @@ typedef struct mb_stats {
     int64_t vertices_reached;  /* summed over sources */
     double device_ms;          /* device time of the superstep loop (CUDA events) */
     int32_t schedule_count[MB_NUM_SCHEDULES]; /* supersteps run per schedule */
+    int64_t kernel_launches;   /* kernels this library launched for the call */
 } mb_stats;
 
 /* ---- library / context ---------------------------------------------------- */
@@ -108,6 +109,10 @@ const char *mb_last_error(const mb_ctx *ctx);
 /* Select the per-superstep schedule policy (MB_POLICY_*); `schedule` is the
  * schedule id for MB_POLICY_FORCED and ignored otherwise. */
 int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule);
+/* Replay a per-superstep schedule list (MB_POLICY_ORACLE_BEST): superstep i
+ * runs schedules[i]; supersteps past n run schedules[n-1].  n <= 4096.
+ * No reference counterpart (the reference has one fixed schedule). */
+int mb_set_schedule_replay(mb_ctx *ctx, const int8_t *schedules, int32_t n);
 /* 1: run whole iteration loops as CUDA graphs with device-side convergence
  * (no host round trip per superstep); 0: host-driven loop, one flag read per
  * superstep, as the reference's ResetToExecute/RetriveToExecute loop

@@ -45,13 +45,15 @@ class Stats(ctypes.Structure):
     _fields_ = [("supersteps", ctypes.c_int32), ("status_flags", ctypes.c_int32),
                 ("edges_traversed", ctypes.c_int64), ("vertices_reached", ctypes.c_int64),
                 ("device_ms", ctypes.c_double),
-                ("schedule_count", ctypes.c_int32 * NUM_SCHEDULES)]
+                ("schedule_count", ctypes.c_int32 * NUM_SCHEDULES),
+                ("kernel_launches", ctypes.c_int64)]
 
     def as_dict(self):
         return {"supersteps": self.supersteps, "status_flags": self.status_flags,
                 "edges_traversed": self.edges_traversed,
                 "vertices_reached": self.vertices_reached, "device_ms": self.device_ms,
-                "schedule_count": list(self.schedule_count)}
+                "schedule_count": list(self.schedule_count),
+                "kernel_launches": self.kernel_launches}
 
 
 def _load():
@@ -67,6 +69,7 @@ def _load():
         "mb_last_error": (ctypes.c_char_p, [P]),
         "mb_set_schedule_policy": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
         "mb_set_graph_capture": (ctypes.c_int, [P, ctypes.c_int]),
+        "mb_set_schedule_replay": (ctypes.c_int, [P, P, I32]),
         "mb_graph_from_edges": (ctypes.c_int, [P, I32, I64, P, P, P, U32, ctypes.POINTER(P)]),
         "mb_graph_generate": (ctypes.c_int, [P, ctypes.POINTER(GenParams), U32,
                                              ctypes.POINTER(P)]),
@@ -245,6 +248,10 @@ class Context:
 
     def set_policy(self, policy, schedule=0):
         _check(lib.mb_set_schedule_policy(self.h, int(policy), int(schedule)), self.h)
+
+    def set_replay(self, schedules):
+        arr = np.ascontiguousarray(schedules, dtype=np.int8)
+        _check(lib.mb_set_schedule_replay(self.h, arr.ctypes.data, len(arr)), self.h)
 
     def set_graph_capture(self, enable):
         _check(lib.mb_set_graph_capture(self.h, 1 if enable else 0), self.h)

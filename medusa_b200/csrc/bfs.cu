@@ -45,6 +45,7 @@ __device__ __forceinline__ bool claim(const BfsArgs &a, int32_t v) {
 
 // schedule 0: push, merge-path edge-balanced over the queue
 __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(BfsArgs a) {
+    count_launch(a.f.ctrl);
     __shared__ uint32_t s_off[kTile + 1];
     __shared__ int32_t s_row[kTile + 1];
     Ctrl *c = a.f.ctrl;
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(BfsArgs a) {
 
 // schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
 __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int cur = c->cur, nxt = cur ^ 1;
     const uint32_t n = (uint32_t)(c->q[cur] >> 32);
@@ -158,6 +160,7 @@ __device__ __forceinline__ void discover_bm(const BfsArgs &a, uint32_t *next, in
 // schedules 2 and 3: push over a bitmap frontier; one warp per word.
 template <bool kEdgeBalanced>
 __global__ void __launch_bounds__(kPushThreads) k_push_bm(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -199,6 +202,7 @@ constexpr int kPullLaneCap = 32;  // in-edges a lane scans alone before the warp
 // schedule 4: pull, thread-per-vertex with a warp-cooperative tail.
 // Each warp owns one word of the output bitmap and of vis.
 __global__ void __launch_bounds__(256) k_pull_thread(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -265,6 +269,7 @@ __global__ void __launch_bounds__(256) k_pull_thread(BfsArgs a) {
 
 // schedule 5: pull, warp-per-vertex
 __global__ void __launch_bounds__(256) k_pull_warp(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -310,6 +315,7 @@ __global__ void __launch_bounds__(256) k_pull_warp(BfsArgs a) {
 // schedule 6: the reference's edge-centric superstep over all E edges
 // (UpdateLevel, Algorithm/UserOperators.h:17-35), next frontier as a bitmap.
 __global__ void __launch_bounds__(256) k_edge_sweep(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     uint32_t *next = a.f.bm[c->bcur ^ 1];
     const int32_t s = c->step;
@@ -328,6 +334,7 @@ __global__ void __launch_bounds__(256) k_edge_sweep(BfsArgs a) {
 
 // schedule 7: pull over all unvisited vertices testing level[u] == s.
 __global__ void __launch_bounds__(256) k_pull_level(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     uint32_t *next = a.f.bm[c->bcur ^ 1];
     const int32_t s = c->step;
@@ -362,6 +369,7 @@ __global__ void __launch_bounds__(256) k_pull_level(BfsArgs a) {
 
 // reached vertices and their out-edges (the reference's traversal count)
 __global__ void k_stats(BfsArgs a) {
+    count_launch(a.f.ctrl);
     uint32_t n = 0;
     uint64_t m = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
@@ -380,6 +388,7 @@ __global__ void k_stats(BfsArgs a) {
 }
 
 __global__ void k_bfs_init(BfsArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int32_t source = c->p.source;
     const int32_t deg = a.f.outdeg[source];

@@ -140,6 +140,19 @@ int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule) {
     return MB_OK;
 }
 
+int mb_set_schedule_replay(mb_ctx *ctx, const int8_t *schedules, int32_t n) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    if (n < 1 || n > mb::kMaxReplay || !schedules)
+        return set_error(ctx, MB_ERR_INVALID, "replay list must hold 1..4096 schedules");
+    for (int32_t i = 0; i < n; i++)
+        if (schedules[i] < 0 || schedules[i] >= MB_NUM_SCHEDULES)
+            return set_error(ctx, MB_ERR_INVALID, "schedule id out of range");
+    ctx->c.replay.assign(schedules, schedules + n);
+    ctx->c.schedule_policy = MB_POLICY_ORACLE_BEST;
+    ctx->c.fixed_schedule = schedules[n - 1];
+    return MB_OK;
+}
+
 int mb_set_graph_capture(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.use_graphs = enable != 0;

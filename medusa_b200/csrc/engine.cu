@@ -12,6 +12,7 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source) {
     p->policy = ctx.schedule_policy;
     p->forced = ctx.fixed_schedule < 0 ? 0 : ctx.fixed_schedule;
     p->nreplay = (int32_t)std::min<size_t>(ctx.replay.size(), kMaxReplay);
+    p->launches = 0;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));
@@ -72,6 +73,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
             stats->vertices_reached = (int64_t)hc->reached;
             stats->device_ms = ms;
             for (int i = 0; i < MB_NUM_SCHEDULES; i++) stats->schedule_count[i] = hc->sched_count[i];
+            stats->kernel_launches = hc->p.launches;
         }
     } catch (...) {
         cudaEventDestroy(e0);

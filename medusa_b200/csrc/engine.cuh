@@ -29,6 +29,7 @@ struct RunParams {
     int32_t policy;
     int32_t forced;
     int32_t nreplay;
+    uint32_t launches;          // kernels launched by this run (device-counted)
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 
@@ -152,6 +153,8 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
     } else {
         c->bcur ^= 1;
         c->mode = FMT_BITMAP;
+        c->q[0] = 0ull;  // bitmap mode: both queues empty (k_bm2q fills q[cur])
+        c->q[1] = 0ull;
         c->nf = c->acc_n;
         c->mf = c->acc_m;
         c->acc_n = 0;
@@ -164,6 +167,11 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
     choose_next(c, app, V, E);
     if (out_fmt != FMT_QUEUE) c->prev_nf = c->nf;
     (void)prev;
+}
+
+// Every engine kernel counts itself once (block 0, thread 0).
+__device__ __forceinline__ void count_launch(Ctrl *c) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&c->p.launches, 1u);
 }
 
 // Last-CTA detection; true in thread 0 of the last CTA to finish.
@@ -240,6 +248,7 @@ static __global__ void k_select(Ctrl *c, const float *mlp, int cap,
                                 cudaGraphConditionalHandle h_cont,
                                 cudaGraphConditionalHandle h_branch, int nbranch,
                                 int use_handles) {
+    count_launch(c);
     const bool learned = c->p.policy == MB_POLICY_LEARNED && !c->done && mlp;
     if (learned) {  // warp-uniform
         float f[kFeat];
@@ -269,6 +278,7 @@ static __global__ void k_select(Ctrl *c, const float *mlp, int cap,
 
 // Zero a bitmap picked at run time: which = 0 current, 1 next.
 static __global__ void k_bm_clear(FrontierArgs a, int which) {
+    count_launch(a.ctrl);
     uint32_t *bm = a.bm[a.ctrl->bcur ^ which];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.W;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -277,6 +287,7 @@ static __global__ void k_bm_clear(FrontierArgs a, int which) {
 
 // queue q[cur] -> bitmap bm[bcur] (cleared before)
 static __global__ void k_q2bm(FrontierArgs a) {
+    count_launch(a.ctrl);
     Ctrl *c = a.ctrl;
     const uint32_t n = (uint32_t)(c->q[c->cur] >> 32);
     const int32_t *qv = a.qv[c->cur];
@@ -296,6 +307,7 @@ static __global__ void k_q2bm(FrontierArgs a) {
 
 // bitmap bm[bcur] -> queue q[cur] (empty); one warp per word
 static __global__ void k_bm2q(FrontierArgs a) {
+    count_launch(a.ctrl);
     Ctrl *c = a.ctrl;
     const uint32_t *bm = a.bm[c->bcur];
     const int cur = c->cur;

@@ -113,6 +113,17 @@ __global__ void k_iota(uint32_t *vals, int64_t n, int reverse) {
         vals[i] = reverse ? (uint32_t)(n - 1 - i) : (uint32_t)i;
 }
 
+// keys[i] <-> keys[n-1-i]: with the edge numbers also reversed, a stable
+// sort then leaves each source's edges in reverse insertion order
+__global__ void k_reverse(uint32_t *keys, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 2;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = keys[i];
+        keys[i] = keys[n - 1 - i];
+        keys[n - 1 - i] = t;
+    }
+}
+
 __global__ void k_hist(const uint32_t *keys, int64_t n, uint32_t *cnt) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -217,8 +228,9 @@ void graph_build_from_device_edges(Context &ctx, Graph &g, int32_t V, int64_t E,
         }
         scan_exclusive_u32(ctx, cnt.as<uint32_t>(), (uint32_t *)g.row.p, V + 1, nullptr, s);
         if (E > 0) {
-            k_iota<<<gridE, 256, 0, s>>>(vals.as<uint32_t>(), E,
-                                         (flags & MB_ORDER_REFERENCE) ? 1 : 0);
+            const int rev = (flags & MB_ORDER_REFERENCE) ? 1 : 0;
+            k_iota<<<gridE, 256, 0, s>>>(vals.as<uint32_t>(), E, rev);
+            if (rev) k_reverse<<<gridE, 256, 0, s>>>(d_src, E);
             MB_CHECK_LAUNCH();
             radix_sort_pairs(ctx, d_src, vals.as<uint32_t>(), E, bits, s);
             k_gather_csr<<<gridE, 256, 0, s>>>(d_src, vals.as<uint32_t>(), d_dst, d_w, E,

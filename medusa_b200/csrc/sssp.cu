@@ -55,6 +55,7 @@ __device__ __forceinline__ bool relax(const SsspArgs &a, int32_t v, float nd, in
 
 // schedule 0: push, merge-path edge-balanced over the queue
 __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
+    count_launch(a.f.ctrl);
     __shared__ uint32_t s_off[kTile + 1];
     __shared__ int32_t s_row[kTile + 1];
     __shared__ float s_du[kTile + 1];
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
 
 // schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
 __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int cur = c->cur, nxt = cur ^ 1;
     const uint32_t n = (uint32_t)(c->q[cur] >> 32);
@@ -174,6 +176,7 @@ __device__ __forceinline__ void improve_bm(const SsspArgs &a, uint32_t *next, in
 // schedules 2 and 3: push over a bitmap frontier; one warp per word
 template <bool kEdgeBalanced>
 __global__ void __launch_bounds__(kPushThreads) k_push_bm(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -234,6 +237,7 @@ constexpr int kPullLaneCap = 64;
 
 // schedule 4: pull, thread-per-vertex with a warp-cooperative tail
 __global__ void __launch_bounds__(256) k_pull_thread(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -283,6 +287,7 @@ __global__ void __launch_bounds__(256) k_pull_thread(SsspArgs a) {
 // in-edge (schedule 7), no frontier test.
 template <bool kAllEdges>
 __global__ void __launch_bounds__(256) k_pull_warp(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const uint32_t *front = a.f.bm[c->bcur];
     uint32_t *next = a.f.bm[c->bcur ^ 1];
@@ -319,6 +324,7 @@ __global__ void __launch_bounds__(256) k_pull_warp(SsspArgs a) {
 
 // schedule 6, step 1 (InitMessageBuffer, SSSP/InitMessage.h:4-9): msg[] = FLT_MAX
 __global__ void k_msg_fill(SsspArgs a) {
+    count_launch(a.f.ctrl);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.f.E;
          i += (int64_t)gridDim.x * blockDim.x)
         a.msg[i] = 3.402823466e+38f;
@@ -327,6 +333,7 @@ __global__ void k_msg_fill(SsspArgs a) {
 // schedule 6, step 2 (ssspEdgeProcAA, SSSP/UserOperators.h:10-29): every
 // vertex updated in the last superstep writes dist+w into its edges' slots
 __global__ void k_msg_send(SsspArgs a) {
+    count_launch(a.f.ctrl);
     const int32_t s = a.f.ctrl->step;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
          v += (int64_t)gridDim.x * blockDim.x) {
@@ -339,6 +346,7 @@ __global__ void k_msg_send(SsspArgs a) {
 // schedule 6, step 3 (segmented min + UpdateVertex, SSSP/UserOperators.h:151-168):
 // the combined message of v is the min of its slots [rrow[v], rrow[v+1]).
 __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     uint32_t *next = a.f.bm[c->bcur ^ 1];
     const int32_t sv = c->step + 1;
@@ -361,6 +369,7 @@ __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
 }
 
 __global__ void k_sssp_init(SsspArgs a) {
+    count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int32_t source = c->p.source;
     const int32_t deg = a.f.outdeg[source];
@@ -398,13 +407,17 @@ __global__ void k_sssp_init(SsspArgs a) {
     if (threadIdx.x == 0) choose_next(c, APP_SSSP, a.f.V, a.f.E);
 }
 
-__global__ void k_fill_dist(float *d, int64_t n) {
+__global__ void k_fill_dist(SsspArgs a) {
+    count_launch(a.f.ctrl);
+    float *d = a.dist;
+    const int64_t n = a.f.V;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         d[i] = kMedusaMax;
 }
 
 __global__ void k_stats(SsspArgs a) {
+    count_launch(a.f.ctrl);
     uint32_t n = 0;
     uint64_t m = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
@@ -449,7 +462,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     sp.cap = (int)std::min<int64_t>((int64_t)g.V * 4 + 16, 1 << 30);
     sp.name = "sssp";
     sp.prologue = [&](cudaStream_t s) {
-        k_fill_dist<<<grid_vtx, 256, 0, s>>>(a.dist, a.f.V);
+        k_fill_dist<<<grid_vtx, 256, 0, s>>>(a);
         MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
         k_sssp_init<<<1, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();

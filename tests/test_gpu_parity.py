@@ -1,0 +1,235 @@
+"""GPU parity: the CUDA path through the C ABI against the reference's own
+outputs (golden fixtures) and the CPU oracle, for every schedule, in both
+loop modes (CUDA graph with device-side convergence, and host-driven)."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    from medusa_b200 import api as a
+    return a
+
+
+@pytest.fixture(params=[False, True], ids=["hostloop", "graph"])
+def ctx(request, gpu_ctx, api):
+    gpu_ctx.set_graph_capture(request.param)
+    gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    yield gpu_ctx
+    gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    gpu_ctx.set_graph_capture(True)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_layout_matches_reference_aa(gpu_ctx, name):
+    """CSR order, msg_index and msgDstID equal the reference's buildAA."""
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"], reference_order=True)
+    lay = g.export()
+    aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+    np.testing.assert_array_equal(lay["row"], aa.edge_index)
+    np.testing.assert_array_equal(lay["col"], aa.e_dst[:aa.E])
+    np.testing.assert_array_equal(lay["w"], aa.e_w[:aa.E])
+    np.testing.assert_array_equal(lay["rrow"], aa.msg_index)
+    np.testing.assert_array_equal(lay["mslot"], aa.msg_dst[:aa.E])
+    rcol = np.empty(aa.E, np.int32)
+    rcol[aa.msg_dst[:aa.E]] = aa.e_src[:aa.E]
+    np.testing.assert_array_equal(lay["rcol"], rcol)
+    g.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_bfs_matches_reference(ctx, name):
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    for i, s in enumerate(c["sources"]):
+        lv, st = g.bfs([s])
+        np.testing.assert_array_equal(lv[0], c["bfs_level"][i])
+        reached = c["bfs_level"][i] >= 0
+        outdeg = np.bincount(c["src"], minlength=c["V"])
+        assert st["vertices_reached"] == int(reached.sum())
+        assert st["edges_traversed"] == int(outdeg[reached].sum())
+    g.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_sssp_matches_reference(ctx, name):
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    for i, s in enumerate(c["sources"]):
+        d, st = g.sssp([s])
+        np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32))
+    g.close()
+
+
+def check_pagerank(got, ref, r64, indeg, tol=1e-5, hub=2048):
+    from test_oracle import check_pagerank as chk
+    chk(got, ref, r64, indeg, tol, hub)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_pagerank_matches_reference(ctx, name):
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    r, st = g.pagerank(c["pr_iters"], 1.0 / c["V"])
+    aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+    indeg = np.diff(aa.msg_index)
+    r64 = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], fp64=True)
+    check_pagerank(r, c["pr_rank"], r64, indeg)
+    # same summation order as the oracle for in-degree <= 2048 and no hubs
+    if indeg.max(initial=0) <= 2048:
+        ro = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"])
+        np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["tiny", "rmat_s10", "grid_24", "hub", "uniform_2k"])
+def test_every_schedule_bit_identical(gpu_ctx, api, name):
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    s = int(c["sources"][0])
+    try:
+        for sched in range(api.NUM_SCHEDULES):
+            gpu_ctx.set_policy(api.MB_POLICY_FORCED, sched)
+            lv, st = g.bfs([s])
+            np.testing.assert_array_equal(lv[0], c["bfs_level"][0], err_msg="bfs sched %d" % sched)
+            d, st = g.sssp([s])
+            np.testing.assert_array_equal(d[0], c["sssp_dist"][0], err_msg="sssp sched %d" % sched)
+        r = {}
+        for sched in (0, 6):
+            gpu_ctx.set_policy(api.MB_POLICY_FORCED, sched)
+            r[sched] = g.pagerank(c["pr_iters"], 1.0 / c["V"])[0]
+        np.testing.assert_array_equal(r[0].view(np.uint32), r[6].view(np.uint32))
+    finally:
+        gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+        g.close()
+
+
+def test_oracle_replay_policy(gpu_ctx, api):
+    """A per-superstep schedule list (alternating push/pull) gives the same levels."""
+    c = load_golden("rmat_s10")
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        for seq in ([0, 4, 0, 4, 0, 4, 0, 4], [4, 5, 2, 3, 1, 6, 7, 0], [6] * 20):
+            gpu_ctx.set_replay(seq)
+            lv, st = g.bfs([0])
+            np.testing.assert_array_equal(lv[0], c["bfs_level"][0])
+            d, _ = g.sssp([0])
+            np.testing.assert_array_equal(d[0], c["sssp_dist"][0])
+            n = st["supersteps"]
+            want = np.bincount(np.array(seq + [seq[-1]] * 64)[:n], minlength=8)
+            assert list(want) == st["schedule_count"]
+    finally:
+        gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    g.close()
+
+
+def test_device_generator_equals_host_generator(gpu_ctx, api):
+    for p in (api.rmat_params(12, 50000, 0.45, 0.15, 0.15, seed=4, wmin=1, wmax=1000),
+              api.uniform_params(3000, 20000, seed=8, wmin=1, wmax=1000),
+              api.grid_params(30, 17, seed=5)):
+        V, s, d, w = api.generate_edges_host(p)
+        g1 = gpu_ctx.generate(p)
+        g2 = gpu_ctx.graph_from_edges(V, s, d, w)
+        a, b = g1.export(), g2.export()
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        g1.close()
+        g2.close()
+
+
+def test_multi_source_equals_single(gpu_ctx):
+    c = load_golden("rmat_s10")
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    srcs = [0, 17, 5, 1000]
+    lv, st = g.bfs(srcs)
+    d, _ = g.sssp(srcs)
+    for i, s in enumerate(srcs):
+        np.testing.assert_array_equal(lv[i], O.bfs(c["V"], c["src"], c["dst"], [s])[0])
+        np.testing.assert_array_equal(d[i], O.sssp(c["V"], c["src"], c["dst"], c["w"], s)[0])
+    g.close()
+
+
+def test_bad_arguments_fail_loudly(gpu_ctx, api):
+    c = load_golden("tiny")
+    with pytest.raises(api.MedusaError) as e:
+        gpu_ctx.graph_from_edges(4, c["src"], c["dst"], c["w"])
+    assert e.value.code == api.MB_ERR_INVALID
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    with pytest.raises(api.MedusaError):
+        g.bfs([c["V"]])
+    with pytest.raises(api.MedusaError):
+        gpu_ctx.set_policy(api.MB_POLICY_FORCED, 99)
+    g.close()
+
+
+# ---- full-size property checks (BASELINE sizes) --------------------------------
+
+def bfs_certificate(V, src, dst, lv, s):
+    """Levels are BFS levels iff: lv[s]=0; every edge from a reached vertex
+    reaches a vertex at most one level deeper; every reached vertex other than
+    s has an in-edge from the level above; edges from unreached vertices are
+    irrelevant."""
+    assert lv[s] == 0
+    lu, lvv = lv[src], lv[dst]
+    reached_u = lu >= 0
+    assert (lvv[reached_u] >= 0).all()
+    assert (lvv[reached_u] <= lu[reached_u] + 1).all()
+    parent_ok = np.zeros(V, bool)
+    tight = reached_u & (lvv == lu + 1)
+    parent_ok[dst[tight]] = True
+    need = lv > 0
+    assert parent_ok[need].all()
+
+
+def sssp_certificate(V, src, dst, w, d, s):
+    assert d[s] == 0
+    du, dv = d[src], d[dst]
+    reached_u = du < 1e9
+    assert (dv[reached_u] <= du[reached_u] + w[reached_u]).all()
+    tight = reached_u & (dv == du + w)
+    ok = np.zeros(V, bool)
+    ok[dst[tight]] = True
+    need = (d < 1e9) & (np.arange(V) != s)
+    assert ok[need].all()
+    assert (d[~(d < 1e9)] == np.float32(1e9)).all()
+
+
+@pytest.mark.parametrize("which", ["c2_rmat", "c3_grid"])
+def test_full_size_bfs_sssp_certificates(gpu_ctx, api, which):
+    if which == "c2_rmat":
+        p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
+    else:
+        p = api.grid_params(1448, 1448, 0.1, 0.005, seed=1, wmin=1, wmax=100)
+    V, s_, d_, w_ = api.generate_edges_host(p)
+    g = gpu_ctx.generate(p)
+    lv, st = g.bfs([0])
+    bfs_certificate(V, s_, d_, lv[0], 0)
+    dist, st2 = g.sssp([0])
+    sssp_certificate(V, s_, d_, w_, dist[0], 0)
+    # every schedule policy path agrees at full size
+    gpu_ctx.set_policy(api.MB_POLICY_FORCED, api.SCHEDULE_NAMES.index("push_edge_queue"))
+    lv2, _ = g.bfs([0])
+    d2, _ = g.sssp([0])
+    gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    np.testing.assert_array_equal(lv2, lv)
+    np.testing.assert_array_equal(d2, dist)
+    g.close()
+
+
+def test_full_size_pagerank_c1_against_oracle(gpu_ctx, api):
+    """C1: uniform 2^18 vertices / 2^22 edges, 10 supersteps from 1/N."""
+    p = api.uniform_params(1 << 18, 1 << 22, seed=1)
+    V, s_, d_, _ = api.generate_edges_host(p)
+    g = gpu_ctx.generate(p)
+    r, st = g.pagerank(10, 1.0 / V)
+    aa = O.AAGraph(V, s_, d_)
+    ro = O.pagerank(V, aa, None, 10, 1.0 / V)
+    # in-degrees are far below the hub threshold: same order as the oracle
+    np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
+    g.close()
