@@ -286,6 +286,7 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
             total.vertices_reached += st.vertices_reached;
             total.device_ms += st.device_ms;
             for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+            total.kernel_launches += st.kernel_launches;
         }
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         if (stats) *stats = total;
@@ -315,6 +316,7 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
             total.vertices_reached += st.vertices_reached;
             total.device_ms += st.device_ms;
             for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+            total.kernel_launches += st.kernel_launches;
         }
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         if (stats) *stats = total;
