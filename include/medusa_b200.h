@@ -169,6 +169,23 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
+/* PageRank that allocates no memory, for callers that cannot call cudaMalloc
+ * (a host application that owns all GPU memory through its own pool, or a
+ * latency-bound caller that cannot accept cudaMalloc/cudaFree's device
+ * synchronisation).  No counterpart in the reference.
+ * Every array is DEVICE memory owned by the caller: row[V+1] out-edge
+ * offsets, rrow[V+1] in-edge offsets, rcol[E] in-edge sources grouped by
+ * destination (the reverse CSR), rank_out[V].  Same arithmetic and bits as
+ * mb_pagerank.  Scratch is one fixed device array in the library (8 MiB per
+ * GPU, held until exit), so num_vertices <= 1048576 (larger: MB_ERR_UNSUPPORTED).
+ * The first call on a device looks up that array's address; make it before
+ * any stream capture.  Runs asynchronously on `stream` (a cudaStream_t; NULL
+ * = the default stream).  All calls on a device share the scratch: calls that
+ * overlap on the GPU race.  Errors: mb_last_error(NULL). */
+int mb_pagerank_noalloc(const int32_t *row, const int32_t *rrow, const int32_t *rcol,
+                        int32_t num_vertices, int64_t num_edges, int32_t iters, float init,
+                        float *rank_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

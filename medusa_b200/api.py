@@ -81,6 +81,7 @@ def _load():
         "mb_bfs": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
         "mb_sssp": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
+        "mb_pagerank_noalloc": (ctypes.c_int, [P, P, P, I32, I64, I32, F32, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -159,6 +160,15 @@ def generate_edges_host(p, weighted=None):
     _check(lib.mb_generate_edges_host(ctypes.byref(p), src.ctypes.data, dst.ctypes.data,
                                       None if w is None else w.ctypes.data, ctypes.byref(E)))
     return num_vertices_of(p), src[:n], dst[:n], (None if w is None else w[:n])
+
+
+def pagerank_noalloc(row, rrow, rcol, num_vertices, iters, init, rank_out, stream=None):
+    """mb_pagerank_noalloc on caller-owned CUDA tensors (no allocation inside).
+    Asynchronous on `stream` (a raw cudaStream_t value, or None for the
+    default stream)."""
+    _check(lib.mb_pagerank_noalloc(_ptr(row), _ptr(rrow), _ptr(rcol), int(num_vertices),
+                                   int(rcol.shape[0]), int(iters), float(init), _ptr(rank_out),
+                                   stream))
 
 
 class Graph:

@@ -77,6 +77,11 @@ void check_graph(mb_ctx *ctx, const mb_graph *g) {
 
 }  // namespace
 
+namespace mb {
+// Error text for entry points that have no context (mb_last_error(NULL)).
+void record_thread_error(const std::string &msg) { t_last_error = msg; }
+}  // namespace mb
+
 extern "C" {
 
 const char *mb_version(void) { return "medusa_b200 0.1 (sm_100a)"; }
