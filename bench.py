@@ -149,6 +149,8 @@ def run_medusa(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = api.Context(local)
+    if args.hostloop:
+        ctx.set_graph_capture(False)
     p = c2_params(api)
     g = ctx.generate(p)
     V = g.V
@@ -219,7 +221,8 @@ def run_medusa(args):
                    "l2": "flushed (256 MiB write) before every step",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "schedule_policy": "fixed (direction-optimising rule)",
-                   "loop": "one CUDA graph per BSP loop (device-side convergence)"},
+                   "loop": ("host-driven loop (one flag read per superstep)" if args.hostloop
+                            else "one CUDA graph per BSP loop (device-side convergence)")},
         "bfs": {"gteps": round(sb_last["edges_traversed"] / sb_last["device_ms"] / 1e6, 3),
                 "ms": round(sb_last["device_ms"], 4), "supersteps": sb_last["supersteps"],
                 "edges_traversed": sb_last["edges_traversed"],
@@ -351,6 +354,8 @@ def main():
     ap.add_argument("--impl", default="medusa", choices=["medusa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pagerank", action="store_true")
+    ap.add_argument("--hostloop", action="store_true",
+                    help="host-driven superstep loop instead of one CUDA graph per loop")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
