@@ -227,11 +227,13 @@ def run_medusa(args):
                 "ms": round(sb_last["device_ms"], 4), "supersteps": sb_last["supersteps"],
                 "edges_traversed": sb_last["edges_traversed"],
                 "vertices_reached": sb_last["vertices_reached"],
-                "schedule_count": sb_last["schedule_count"]},
+                "schedule_count": sb_last["schedule_count"],
+                "edges_scanned": sb_last["edges_scanned"]},
         "sssp": {"gteps": round(ss_last["edges_traversed"] / ss_last["device_ms"] / 1e6, 3),
                  "ms": round(ss_last["device_ms"], 4), "supersteps": ss_last["supersteps"],
                  "edges_traversed": ss_last["edges_traversed"],
-                 "schedule_count": ss_last["schedule_count"]},
+                 "schedule_count": ss_last["schedule_count"],
+                 "edges_scanned": ss_last["edges_scanned"]},
         "e2e": {"value": round(e2e_val, 3), "unit": "GTEPS", "h2d_bytes_per_step": 8,
                 "d2h_bytes_per_step": 8 * V},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk,

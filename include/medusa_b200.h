@@ -93,6 +93,8 @@ typedef struct mb_stats {
     double device_ms;          /* device time of the superstep loop (CUDA events) */
     int32_t schedule_count[MB_NUM_SCHEDULES]; /* supersteps run per schedule */
     int64_t kernel_launches;   /* kernels this library launched for the call */
+    int64_t edges_scanned;     /* edges examined: frontier out-edges of push
+                                  supersteps plus E per pull/sweep superstep */
 } mb_stats;
 
 /* ---- library / context ---------------------------------------------------- */
@@ -113,6 +115,24 @@ int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule);
  * runs schedules[i]; supersteps past n run schedules[n-1].  n <= 4096.
  * No reference counterpart (the reference has one fixed schedule). */
 int mb_set_schedule_replay(mb_ctx *ctx, const int8_t *schedules, int32_t n);
+/* SSSP near-far (delta-stepping) bucket width: vertices whose new distance
+ * is below the current threshold are expanded next, the rest wait in a far
+ * pile until the threshold (raised by delta each time the near frontier runs
+ * dry) passes them.  delta > 0: that width; 0 (the default): plain frontier
+ * Bellman-Ford; < 0: 32 x mean weight / mean out-degree of the graph.
+ * Distances are identical for every delta.  No reference counterpart (the
+ * reference relaxes every edge every superstep, SSSP/CPUFunctorHoster.cpp:58-99). */
+int mb_set_sssp_delta(mb_ctx *ctx, float delta);
+/* 1 (default): supersteps of schedule 0 whose queue frontier is small (at
+ * most 2048 vertices and 16384 out-edges) run in one persistent CTA, several
+ * supersteps per launch; 0: every superstep is a grid-wide launch.  Results
+ * are identical either way. */
+int mb_set_persistent_tail(mb_ctx *ctx, int enable);
+/* 1: supersteps of schedules 0 and 4 (and near-far splits) run
+ * inside one persistent cooperative grid, many supersteps per launch, with
+ * grid barriers between them (bounded waits: MB_ERR_TIMEOUT if one gives up);
+ * 0 (the default): one launch per superstep.  Identical results either way. */
+int mb_set_persistent_grid(mb_ctx *ctx, int enable);
 /* 1: run whole iteration loops as CUDA graphs with device-side convergence
  * (no host round trip per superstep); 0: host-driven loop, one flag read per
  * superstep, as the reference's ResetToExecute/RetriveToExecute loop

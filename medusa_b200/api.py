@@ -46,14 +46,15 @@ class Stats(ctypes.Structure):
                 ("edges_traversed", ctypes.c_int64), ("vertices_reached", ctypes.c_int64),
                 ("device_ms", ctypes.c_double),
                 ("schedule_count", ctypes.c_int32 * NUM_SCHEDULES),
-                ("kernel_launches", ctypes.c_int64)]
+                ("kernel_launches", ctypes.c_int64), ("edges_scanned", ctypes.c_int64)]
 
     def as_dict(self):
         return {"supersteps": self.supersteps, "status_flags": self.status_flags,
                 "edges_traversed": self.edges_traversed,
                 "vertices_reached": self.vertices_reached, "device_ms": self.device_ms,
                 "schedule_count": list(self.schedule_count),
-                "kernel_launches": self.kernel_launches}
+                "kernel_launches": self.kernel_launches,
+                "edges_scanned": self.edges_scanned}
 
 
 def _load():
@@ -70,6 +71,9 @@ def _load():
         "mb_set_schedule_policy": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
         "mb_set_graph_capture": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_set_schedule_replay": (ctypes.c_int, [P, P, I32]),
+        "mb_set_sssp_delta": (ctypes.c_int, [P, F32]),
+        "mb_set_persistent_tail": (ctypes.c_int, [P, ctypes.c_int]),
+        "mb_set_persistent_grid": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_graph_from_edges": (ctypes.c_int, [P, I32, I64, P, P, P, U32, ctypes.POINTER(P)]),
         "mb_graph_generate": (ctypes.c_int, [P, ctypes.POINTER(GenParams), U32,
                                              ctypes.POINTER(P)]),
@@ -262,6 +266,16 @@ class Context:
     def set_replay(self, schedules):
         arr = np.ascontiguousarray(schedules, dtype=np.int8)
         _check(lib.mb_set_schedule_replay(self.h, arr.ctypes.data, len(arr)), self.h)
+
+    def set_sssp_delta(self, delta):
+        """SSSP near-far bucket width (> 0), 0 for plain Bellman-Ford, < 0 per-graph default."""
+        _check(lib.mb_set_sssp_delta(self.h, float(delta)), self.h)
+
+    def set_persistent_tail(self, enable):
+        _check(lib.mb_set_persistent_tail(self.h, 1 if enable else 0), self.h)
+
+    def set_persistent_grid(self, enable):
+        _check(lib.mb_set_persistent_grid(self.h, 1 if enable else 0), self.h)
 
     def set_graph_capture(self, enable):
         _check(lib.mb_set_graph_capture(self.h, 1 if enable else 0), self.h)

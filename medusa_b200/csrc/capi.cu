@@ -158,6 +158,25 @@ int mb_set_schedule_replay(mb_ctx *ctx, const int8_t *schedules, int32_t n) {
     return MB_OK;
 }
 
+int mb_set_sssp_delta(mb_ctx *ctx, float delta) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    if (!(delta == delta)) return set_error(ctx, MB_ERR_INVALID, "delta is NaN");
+    ctx->c.sssp_delta = delta;
+    return MB_OK;
+}
+
+int mb_set_persistent_tail(mb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    ctx->c.tail = enable != 0;
+    return MB_OK;
+}
+
+int mb_set_persistent_grid(mb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    ctx->c.persist = enable != 0;
+    return MB_OK;
+}
+
 int mb_set_graph_capture(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.use_graphs = enable != 0;
@@ -292,6 +311,7 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
             total.device_ms += st.device_ms;
             for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
             total.kernel_launches += st.kernel_launches;
+            total.edges_scanned += st.edges_scanned;
         }
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         if (stats) *stats = total;
@@ -322,6 +342,7 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
             total.device_ms += st.device_ms;
             for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
             total.kernel_launches += st.kernel_launches;
+            total.edges_scanned += st.edges_scanned;
         }
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         if (stats) *stats = total;

@@ -4,7 +4,7 @@
 
 namespace mb {
 
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source) {
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta) {
     static_assert(sizeof(RunParams) <= Context::kCtrlOff, "params staging too small");
     static_assert(sizeof(Ctrl) <= Context::kSmallBytes - Context::kCtrlOff, "ctrl readback too small");
     RunParams *p = (RunParams *)(ctx.pinned_small + Context::kParamsOff);
@@ -13,14 +13,24 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source) {
     p->forced = ctx.fixed_schedule < 0 ? 0 : ctx.fixed_schedule;
     p->nreplay = (int32_t)std::min<size_t>(ctx.replay.size(), kMaxReplay);
     p->launches = 0;
+    p->delta = delta;
+    p->tail = ctx.tail ? 1 : 0;
+    p->persist = ctx.persist ? 1 : 0;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));
 }
 
+int persistent_grid_size(const Context &ctx, const void *kernel, int threads) {
+    int per_sm = 0;
+    MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+    if (per_sm < 1) fail(MB_ERR_UNSUPPORTED, "persistent kernel does not fit on an SM");
+    return ctx.num_sms * std::min(per_sm, 4);
+}
+
 void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
     cudaStream_t s = ctx.stream;
-    const int nbranch = 2 * MB_NUM_SCHEDULES;
+    const int nbranch = kNumBranches;
     FrontierState &st = *sp.st;
     const FrontierArgs &fa = sp.fa;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -29,12 +39,12 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
     try {
         if (ctx.use_graphs) {
             if (!st.lg.exec || st.owner != (const void *)&ctx || st.owner_mlp != (const void *)fa.mlp) {
-                const int cap = sp.cap;
+                const int cap = sp.cap, app = sp.app;
                 build_loop_graph(
                     st.lg, s, nbranch, sp.prologue,
                     [&](cudaStream_t cs, cudaGraphConditionalHandle hc,
                         cudaGraphConditionalHandle hb) {
-                        k_select<<<1, 32, 0, cs>>>(fa.ctrl, fa.mlp, cap, hc, hb, nbranch, 1);
+                        k_select<<<1, 32, 0, cs>>>(fa, app, cap, hc, hb, nbranch, 1);
                         MB_CHECK_LAUNCH();
                     },
                     sp.branch, sp.epilogue);
@@ -49,7 +59,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
             sp.prologue(s);
             Ctrl *hc = (Ctrl *)ctx.ctrl_readback();
             for (;;) {
-                k_select<<<1, 32, 0, s>>>(fa.ctrl, fa.mlp, sp.cap, 0, 0, nbranch, 0);
+                k_select<<<1, 32, 0, s>>>(fa, sp.app, sp.cap, 0, 0, nbranch, 0);
                 MB_CHECK_LAUNCH();
                 MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
                 MB_CUDA(cudaStreamSynchronize(s));
@@ -66,6 +76,8 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
         MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
         MB_CUDA(cudaStreamSynchronize(s));
         if (hc->err & ERR_STEP_CAP) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": superstep cap reached");
+        if (hc->err & ERR_BARRIER)
+            fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a persistent-grid barrier timed out");
         if (stats) {
             stats->supersteps = hc->supersteps;
             stats->status_flags = hc->err;
@@ -74,6 +86,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
             stats->device_ms = ms;
             for (int i = 0; i < MB_NUM_SCHEDULES; i++) stats->schedule_count[i] = hc->sched_count[i];
             stats->kernel_launches = hc->p.launches;
+            stats->edges_scanned = (int64_t)hc->work;
         }
     } catch (...) {
         cudaEventDestroy(e0);

@@ -19,8 +19,24 @@ namespace mb {
 
 constexpr int FMT_QUEUE = 0, FMT_BITMAP = 1, FMT_NONE = 2;
 constexpr int ERR_STEP_CAP = 1;
+constexpr int ERR_BARRIER = 2;     // a grid barrier of the persistent kernel gave up
 constexpr int kMaxReplay = 4096;
 constexpr int APP_BFS = 0, APP_SSSP = 1;
+// Internal step of near-far SSSP (not a user schedule): raise the distance
+// threshold and move far-pile vertices below it into the near queue.
+constexpr int kSchedSplit = MB_NUM_SCHEDULES;
+constexpr int kBranchSplit = 2 * MB_NUM_SCHEDULES;
+// Persistent small-frontier tail: schedule 0 run by ONE CTA of kTailThreads
+// threads for as many consecutive supersteps as the frontier stays within
+// kTailEntries vertices and kTailEdges edges (no launch per superstep).
+constexpr int kBranchTail = kBranchSplit + 1;
+// Persistent BSP kernel: one cooperative grid runs consecutive supersteps of
+// schedules 0 and 4 (with their frontier conversions) and near-far splits,
+// separated by grid barriers, until a superstep needs anything else.
+constexpr int kBranchPersist = kBranchTail + 1;
+constexpr int kNumBranches = kBranchPersist + 1;
+constexpr int kTailThreads = 1024;
+constexpr uint32_t kTailEntries = 2048, kTailEdges = 16384;
 
 // Per-run parameters, written by the host before each run (one small copy),
 // so an instantiated loop graph serves every source and policy.
@@ -30,6 +46,9 @@ struct RunParams {
     int32_t forced;
     int32_t nreplay;
     uint32_t launches;          // kernels launched by this run (device-counted)
+    float delta;                // SSSP near-far bucket width (0: plain frontier Bellman-Ford)
+    int32_t tail;               // 1: small frontiers run in the persistent single-CTA tail
+    int32_t persist;            // 1: schedules 0/4 and splits run in the persistent grid
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 
@@ -61,6 +80,15 @@ struct Ctrl {
     float feat[8];
     int32_t sched_count[MB_NUM_SCHEDULES];
     uint64_t reached, edges_reached;
+    uint64_t work;            // edges examined: push frontier out-edges, E per pull/sweep
+    int32_t pending;          // a superstep ran and awaits finish_superstep
+    float thresh;             // SSSP near-far: vertices below go to the near queue
+    uint32_t far_n[2];        // SSSP near-far: far-pile sizes
+    int32_t fcur;             // far pile being filled
+    int32_t splits;           // near-far split steps run
+    uint32_t bar_count;       // persistent-grid barrier: arrivals
+    uint32_t bar_gen;         // persistent-grid barrier: generation
+    int32_t persist_go;       // persistent grid: run another superstep
 };
 
 // Frontier buffers and graph shape every engine kernel sees.
@@ -80,21 +108,34 @@ struct FrontierArgs {
 __host__ __device__ inline int sched_input(int s) {
     return s <= 1 ? FMT_QUEUE : (s <= 5 ? FMT_BITMAP : FMT_NONE);
 }
-__host__ __device__ inline int sched_output(int s) { return s <= 1 ? FMT_QUEUE : FMT_BITMAP; }
+__host__ __device__ inline int sched_output(int s) {
+    return (s <= 1 || s == kSchedSplit) ? FMT_QUEUE : FMT_BITMAP;
+}
 __host__ __device__ inline int branch_of(int s, int mode) {
+    if (s == kSchedSplit) return kBranchSplit;
     const int in = sched_input(s);
     return s + ((in != FMT_NONE && in != mode) ? MB_NUM_SCHEDULES : 0);
 }
+
+// Loads that bypass L1: counters other threads update with atomics (at L2)
+// are read this way by code that may run inside the same kernel.
+template <class T>
+__device__ __forceinline__ T ldg2(const T *p) { return __ldcg(p); }
+
+// The branch that runs schedule s from the current frontier: the persistent
+// tail for a small queue frontier under schedule 0.
+__device__ inline int route(const struct Ctrl *c, int s);
 
 // ---- the fixed rule ----------------------------------------------------------
 // BFS: direction-optimising (Beamer, Asanovic & Patterson, SC 2012) -- go
 // bottom-up when the frontier's out-edges exceed the unvisited out-edges /
 // alpha, come back top-down when the frontier shrinks below V / beta.
-// SSSP: pull (a full min over in-edges) once the frontier's out-edges are a
-// large share of E, push otherwise.
+// SSSP: always push, edge-balanced.  An SSSP pull must scan every in-edge to
+// find what a push reaches through the frontier's out-edges, and a minimum
+// has no early exit, so pulling never does less work.
 __device__ inline int fixed_rule(const Ctrl *c, int app, int32_t V, int64_t E, uint32_t n,
                                  uint64_t m) {
-    if (app == APP_SSSP) return (int64_t)m * 3 > E ? MB_SCHED_PULL_THREAD : MB_SCHED_PUSH_EDGE_QUEUE;
+    if (app == APP_SSSP) return MB_SCHED_PUSH_EDGE_QUEUE;
     const int64_t alpha = 15, beta = 20;
     if (c->mode == FMT_QUEUE) {
         if ((int64_t)m * alpha > c->m_unvisited) return MB_SCHED_PULL_THREAD;
@@ -104,13 +145,26 @@ __device__ inline int fixed_rule(const Ctrl *c, int app, int32_t V, int64_t E, u
     return MB_SCHED_PULL_THREAD;
 }
 
+__host__ __device__ inline bool persist_supported(int s) {
+    return s == MB_SCHED_PUSH_EDGE_QUEUE || s == MB_SCHED_PULL_THREAD || s == kSchedSplit;
+}
+
+__device__ inline int route(const Ctrl *c, int s) {
+    if (c->p.persist && persist_supported(s)) return kBranchPersist;
+    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.tail &&
+        c->front_n <= kTailEntries && c->front_m <= kTailEdges)
+        return kBranchTail;
+    return branch_of(s, c->mode);
+}
+
 // Decide the next superstep from the current frontier (one thread).
 __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     uint32_t n;
     uint64_t m;
     if (c->mode == FMT_QUEUE) {
-        n = (uint32_t)(c->q[c->cur] >> 32);
-        m = (uint32_t)c->q[c->cur];
+        const unsigned long long q = ldg2(&c->q[c->cur]);
+        n = (uint32_t)(q >> 32);
+        m = (uint32_t)q;
     } else {
         n = c->nf;
         m = c->mf;
@@ -118,6 +172,13 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     c->front_n = n;
     c->front_m = m;
     if (n == 0 || m == 0) {  // nothing left to expand
+        if (app == APP_SSSP && ldg2(&c->far_n[c->fcur]) > 0) {
+            // near-far: next bucket
+            c->thresh += c->p.delta;
+            c->sched = kSchedSplit;
+            c->branch = route(c, kSchedSplit);
+            return;
+        }
         c->done = 1;
         return;
     }
@@ -130,43 +191,57 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
         default: s = fixed_rule(c, app, V, E, n, m); break;
     }
     // features for the learned scheduler (the select kernel runs the MLP)
-    make_features(c->feat, (double)n, (double)m, (double)c->n_unvisited, (double)c->m_unvisited,
-                  (double)V, (double)E, (double)c->skew, c->mode);
+    make_features(c->feat, (float)n, (float)m, (float)c->n_unvisited, (float)c->m_unvisited,
+                  (float)V, (float)E, c->skew, c->mode);
     if (s < 0 || s >= MB_NUM_SCHEDULES) s = 0;
     c->sched = s;
-    c->branch = branch_of(s, c->mode);
+    c->branch = route(c, s);
 }
 
 // Called by thread 0 of the last CTA of a superstep kernel.
 __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, int out_fmt) {
-    c->sched_count[c->sched]++;
-    c->supersteps++;
+    if (c->sched == kSchedSplit) {
+        c->splits++;
+        c->far_n[c->fcur] = 0;
+        c->fcur ^= 1;
+        c->supersteps++;
+    } else {
+        c->sched_count[c->sched]++;
+        c->supersteps++;
+        c->work += c->sched <= MB_SCHED_PUSH_WARP_BITMAP ? c->front_m : (uint64_t)E;
+    }
+    // accumulators and queue counters were updated with atomics
+    const uint32_t acc_n = ldg2(&c->acc_n);
+    const uint64_t acc_m = ldg2((const unsigned long long *)&c->acc_m);
+    const unsigned long long qn = ldg2(&c->q[c->cur ^ 1]);
+    if (app == APP_BFS) {  // claimed vertices and their out-edges
+        c->reached += acc_n;
+        c->edges_reached += out_fmt == FMT_QUEUE ? (uint32_t)qn : acc_m;
+    }
     if (out_fmt == FMT_QUEUE) {
         c->cur ^= 1;
         c->q[c->cur ^ 1] = 0ull;
         c->mode = FMT_QUEUE;
-        c->m_unvisited -= (int64_t)(uint32_t)c->q[c->cur];
-        c->n_unvisited -= (int64_t)c->acc_n;  // every claimed vertex, queued or not
+        c->m_unvisited -= (int64_t)(uint32_t)qn;
+        c->n_unvisited -= (int64_t)acc_n;  // every claimed vertex, queued or not
         c->acc_n = 0;
         c->acc_m = 0;
-        c->prev_nf = (uint32_t)(c->q[c->cur] >> 32);
+        c->prev_nf = (uint32_t)(qn >> 32);
     } else {
         c->bcur ^= 1;
         c->mode = FMT_BITMAP;
         c->q[0] = 0ull;  // bitmap mode: both queues empty (k_bm2q fills q[cur])
         c->q[1] = 0ull;
-        c->nf = c->acc_n;
-        c->mf = c->acc_m;
+        c->nf = acc_n;
+        c->mf = acc_m;
         c->acc_n = 0;
         c->acc_m = 0;
         c->m_unvisited -= (int64_t)c->mf;
         c->n_unvisited -= (int64_t)c->nf;
     }
     c->step++;
-    const uint32_t prev = c->prev_nf;
     choose_next(c, app, V, E);
     if (out_fmt != FMT_QUEUE) c->prev_nf = c->nf;
-    (void)prev;
 }
 
 // Every engine kernel counts itself once (block 0, thread 0).
@@ -174,31 +249,29 @@ __device__ __forceinline__ void count_launch(Ctrl *c) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&c->p.launches, 1u);
 }
 
-// Last-CTA detection; true in thread 0 of the last CTA to finish.
-__device__ __forceinline__ bool last_block(Ctrl *c) {
-    __shared__ bool is_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned t = atomicAdd(&c->blocks_done, 1u);
-        is_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (is_last && threadIdx.x == 0) {
-        __threadfence();
-        c->blocks_done = 0;
-        return true;
-    }
-    return false;
-}
-
-// Warp-level accumulation of (new frontier vertices, their out-edges).
+// Block-level accumulation of (new frontier vertices, their out-edges): one
+// atomic pair per block.  Called by every thread of the block.
 __device__ __forceinline__ void flush_counts(Ctrl *c, uint32_t n, uint64_t m) {
+    __shared__ uint32_t s_n[32];
+    __shared__ unsigned long long s_m[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     n = warp_sum(n);
     m = warp_sum(m);
-    if ((threadIdx.x & 31) == 0 && (n | m)) {
-        atomicAdd(&c->acc_n, n);
-        atomicAdd((unsigned long long *)&c->acc_m, (unsigned long long)m);
+    if (lane == 0) {
+        s_n[wid] = n;
+        s_m[wid] = m;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        uint32_t bn = lane < nw ? s_n[lane] : 0u;
+        uint64_t bm = lane < nw ? s_m[lane] : 0ull;
+        bn = warp_sum(bn);
+        bm = warp_sum(bm);
+        if (lane == 0 && (bn | bm)) {
+            atomicAdd(&c->acc_n, bn);
+            atomicAdd((unsigned long long *)&c->acc_m, (unsigned long long)bm);
+        }
     }
 }
 
@@ -241,32 +314,53 @@ __device__ __forceinline__ uint32_t tail_mask(int64_t w, int32_t V) {
 
 // ---- kernels shared by the apps (internal linkage: one copy per app file) --
 
-// Top of every loop iteration (one warp): stop the loop when done or past
-// the superstep cap; otherwise, under the learned policy, run the MLP on the
-// features the last superstep left; then pick the branch.
-static __global__ void k_select(Ctrl *c, const float *mlp, int cap,
-                                cudaGraphConditionalHandle h_cont,
-                                cudaGraphConditionalHandle h_branch, int nbranch,
-                                int use_handles) {
-    count_launch(c);
-    const bool learned = c->p.policy == MB_POLICY_LEARNED && !c->done && mlp;
+// One full warp: finish the superstep that ran (frontier bookkeeping and
+// the choice of the next schedule), then, under the learned policy, run the
+// MLP on the features it left.
+__device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
+    Ctrl *c = a.ctrl;
+    if ((threadIdx.x & 31) == 0 && c->pending) {
+        c->pending = 0;
+        finish_superstep(c, app, a.V, a.E, sched_output(c->sched));
+    }
+    __syncwarp();
+    const bool learned = c->p.policy == MB_POLICY_LEARNED && !c->done && a.mlp &&
+                         c->sched != kSchedSplit;
     if (learned) {  // warp-uniform
         float f[kFeat];
 #pragma unroll
         for (int i = 0; i < kFeat; i++) f[i] = c->feat[i];
-        const int s = mlp_pick_warp(mlp, f, 0xffu);
-        if (threadIdx.x == 0) {
+        const int s = mlp_pick_warp(a.mlp, f, 0xffu);
+        if ((threadIdx.x & 31) == 0) {
             c->sched = s;
-            c->branch = branch_of(s, c->mode);
+            c->branch = route(c, s);
         }
         __syncwarp();
     }
-    if (threadIdx.x != 0) return;
+}
+
+// Count one loop iteration; past the cap the run stops with an error.
+__device__ inline void count_iteration(Ctrl *c, int cap) {
     c->iter++;
     if (c->iter > cap && !c->done) {
         c->err |= ERR_STEP_CAP;
         c->done = 1;
     }
+}
+
+// Top of every loop iteration (one warp): bookkeeping of the superstep that
+// just ran (so superstep kernels need no last-CTA detection), stop the loop
+// when done or past the superstep cap, else pick the branch.
+static __global__ void k_select(FrontierArgs a, int app, int cap,
+                                cudaGraphConditionalHandle h_cont,
+                                cudaGraphConditionalHandle h_branch, int nbranch,
+                                int use_handles) {
+    Ctrl *c = a.ctrl;
+    count_launch(c);
+    bookkeep_warp(a, app);
+    if (threadIdx.x != 0) return;
+    count_iteration(c, cap);
+    if (!c->done) c->pending = 1;
     if (!use_handles) return;
     if (c->done) {
         cudaGraphSetConditional(h_branch, (unsigned)nbranch);  // no branch
@@ -276,40 +370,80 @@ static __global__ void k_select(Ctrl *c, const float *mlp, int cap,
     }
 }
 
+// Grid barrier of the persistent kernel (all blocks co-resident: cooperative
+// launch).  The wait is bounded: past kBarrierSpins polls it records
+// ERR_BARRIER and returns false, and the caller leaves its loop.
+constexpr long kBarrierSpins = 1l << 22;
+__device__ inline bool grid_sync(Ctrl *c) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ldg2(&c->bar_gen);
+        __threadfence();
+        const unsigned arrived = atomicAdd(&c->bar_count, 1u);
+        int ok = 1;
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            ok = 0;
+            for (long it = 0; it < kBarrierSpins; it++) {
+                if (ldg2(&c->bar_gen) != gen) {
+                    ok = 1;
+                    break;
+                }
+                __nanosleep(32);
+            }
+            if (!ok) atomicOr(&c->err, ERR_BARRIER);
+        }
+        __threadfence();
+        s_ok = ok && !(ldg2(&c->err) & ERR_BARRIER);
+    }
+    __syncthreads();
+    return s_ok;
+}
+
+// The persistent kernel's bookkeeping between two barriers (block 0, warp 0):
+// finish the superstep that ran and decide whether the grid runs the next one.
+__device__ inline void persist_bookkeep(const FrontierArgs &a, int app, int cap) {
+    Ctrl *c = a.ctrl;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    if (threadIdx.x == 0) c->pending = 1;
+    __syncwarp();
+    bookkeep_warp(a, app);
+    if (threadIdx.x == 0) {
+        count_iteration(c, cap);
+        c->persist_go = !c->done && c->branch == kBranchPersist;
+        __threadfence();
+    }
+}
+
 // Zero a bitmap picked at run time: which = 0 current, 1 next.
-static __global__ void k_bm_clear(FrontierArgs a, int which) {
-    count_launch(a.ctrl);
-    uint32_t *bm = a.bm[a.ctrl->bcur ^ which];
+__device__ inline void work_bm_clear(const FrontierArgs &a, int which) {
+    uint32_t *bm = pick(a.bm, a.ctrl->bcur ^ which);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.W;
          i += (int64_t)gridDim.x * blockDim.x)
         bm[i] = 0u;
 }
 
 // queue q[cur] -> bitmap bm[bcur] (cleared before)
-static __global__ void k_q2bm(FrontierArgs a) {
-    count_launch(a.ctrl);
+__device__ inline void work_q2bm(const FrontierArgs &a) {
     Ctrl *c = a.ctrl;
     const uint32_t n = (uint32_t)(c->q[c->cur] >> 32);
-    const int32_t *qv = a.qv[c->cur];
-    uint32_t *bm = a.bm[c->bcur];
+    const int32_t *qv = pick(a.qv, c->cur);
+    uint32_t *bm = pick(a.bm, c->bcur);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = qv[i];
         atomicOr(&bm[v >> 5], 1u << (v & 31));
     }
-    if (last_block(c)) {
-        c->nf = n;
-        c->mf = (uint32_t)c->q[c->cur];
-        c->q[c->cur] = 0ull;  // both queues empty in bitmap mode
-        c->mode = FMT_BITMAP;
-    }
 }
 
 // bitmap bm[bcur] -> queue q[cur] (empty); one warp per word
-static __global__ void k_bm2q(FrontierArgs a) {
-    count_launch(a.ctrl);
+__device__ inline void work_bm2q(const FrontierArgs &a) {
     Ctrl *c = a.ctrl;
-    const uint32_t *bm = a.bm[c->bcur];
+    const uint32_t *bm = pick(a.bm, c->bcur);
     const int cur = c->cur;
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -319,9 +453,38 @@ static __global__ void k_bm2q(FrontierArgs a) {
         const int32_t v = (int32_t)(w * 32 + lane);
         const bool in = (word >> lane) & 1u;
         const uint32_t deg = in ? (uint32_t)a.outdeg[v] : 0u;
-        enqueue_warp(in && deg > 0, v, deg, &c->q[cur], a.qv[cur], a.qo[cur], a.tf[cur]);
+        enqueue_warp(in && deg > 0, v, deg, &c->q[cur], pick(a.qv, cur), pick(a.qo, cur), pick(a.tf, cur));
     }
-    if (last_block(c)) c->mode = FMT_QUEUE;
+}
+
+static __global__ void k_bm_clear(FrontierArgs a, int which) {
+    count_launch(a.ctrl);
+    work_bm_clear(a, which);
+}
+static __global__ void k_q2bm(FrontierArgs a) {
+    count_launch(a.ctrl);
+    work_q2bm(a);
+}
+static __global__ void k_bm2q(FrontierArgs a) {
+    count_launch(a.ctrl);
+    work_bm2q(a);
+}
+
+// Frontier conversion a persistent superstep of schedule s needs first
+// (grid-wide, with barriers); false if a barrier gave up.
+__device__ inline bool persist_convert(const FrontierArgs &a, int s, int mode) {
+    const int in = sched_input(s);
+    if (in == FMT_BITMAP && mode == FMT_QUEUE) {
+        work_bm_clear(a, 0);
+        if (!grid_sync(a.ctrl)) return false;
+        work_q2bm(a);
+        return grid_sync(a.ctrl);
+    }
+    if (in == FMT_QUEUE && mode == FMT_BITMAP) {
+        work_bm2q(a);
+        return grid_sync(a.ctrl);
+    }
+    return true;
 }
 
 // ---- host side ------------------------------------------------------------------
@@ -394,9 +557,9 @@ struct FrontierState {
     }
 };
 
-// Write this run's RunParams (policy, forced schedule, replay list, source)
-// to the control block (RunParams is its first member).
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source);
+// Write this run's RunParams (policy, forced schedule, replay list, source,
+// SSSP bucket width) to the control block (RunParams is its first member).
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f);
 
 // Run a loop (graph mode or host-driven mode) and time it; fills the common
 // part of stats from the control block.
@@ -404,11 +567,24 @@ struct LoopSpec {
     FrontierState *st;
     FrontierArgs fa;
     int cap;
+    int app;
     EmitFn prologue;
     EmitBranch branch;
     EmitFn epilogue;
     const char *name;
 };
 void run_loop(Context &ctx, LoopSpec &spec, mb_stats *stats);
+
+// Blocks of the persistent kernel: every SM holds min(resident, 4) of them,
+// so a cooperative launch always fits.
+int persistent_grid_size(const Context &ctx, const void *kernel, int threads);
+
+// Cooperative launch of kernel(args, cap) (capturable into a CUDA graph).
+template <class Args>
+void launch_cooperative(const void *kernel, int grid, int threads, cudaStream_t s, Args args,
+                        int cap) {
+    void *params[] = {(void *)&args, (void *)&cap};
+    MB_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(threads), params, 0, s));
+}
 
 }  // namespace mb

@@ -58,6 +58,89 @@ __device__ __forceinline__ void enqueue_warp(bool pred, int32_t v, uint32_t deg,
     }
 }
 
+// CTA-level enqueue buffer: a tile's discoveries are gathered in shared
+// memory and published with ONE global atomicAdd per tile (instead of one
+// per warp per round on the same counter, which serialises in L2).
+// Capacity kTile: a tile has kTile edges and each edge discovers at most one
+// vertex.
+struct BlockQueue {
+    int32_t v[kTile];
+    uint32_t d[kTile];
+    uint32_t n;
+    uint32_t warp_tot[kPushThreads / 32];
+    unsigned long long base;
+};
+
+// Warp-aggregated append to the block buffer (all 32 lanes call it).
+__device__ __forceinline__ void bq_push(BlockQueue &bq, bool pred, int32_t v, uint32_t deg) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&bq.n, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) {
+        const uint32_t i = base + __popc(mask & lanemask_lt());
+        bq.v[i] = v;
+        bq.d[i] = deg;
+    }
+}
+
+// Publish the block buffer to the global queue and reset it (all threads of
+// the block call it; it synchronises the block).
+__device__ __forceinline__ void bq_flush(BlockQueue &bq, unsigned long long *qctr, int32_t *qv,
+                                         uint32_t *qo, int32_t *tile_first) {
+    constexpr int kPer = kTile / kPushThreads;
+    __syncthreads();
+    const uint32_t n = bq.n;
+    if (n == 0) return;  // block-uniform
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t i0 = threadIdx.x * kPer;
+    uint32_t loc[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        loc[k] = (i0 + k < n) ? bq.d[i0 + k] : 0u;
+        sum += loc[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) bq.warp_tot[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < kPushThreads / 32; w++) {
+            const uint32_t t = bq.warp_tot[w];
+            bq.warp_tot[w] = tot;
+            tot += t;
+        }
+        bq.base = atomicAdd(qctr, ((unsigned long long)n << 32) | tot);
+    }
+    __syncthreads();
+    const unsigned long long base = bq.base;
+    uint32_t off = (uint32_t)base + bq.warp_tot[wid] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        const uint32_t i = i0 + k;
+        if (i < n) {
+            const uint32_t pos = (uint32_t)(base >> 32) + i;
+            const uint32_t d = loc[k];
+            qv[pos] = bq.v[i];
+            qo[pos] = off;
+            const uint32_t t0 = (off + kTile - 1) / kTile, t1 = (off + d - 1) / kTile;
+            for (uint32_t t = t0; t <= t1; t++) tile_first[t] = (int32_t)pos;
+            off += d;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) bq.n = 0;
+    __syncthreads();
+}
+
 // Index of the last element of s[0..n) that is <= x (s ascending, s[0] <= x).
 __device__ __forceinline__ int upper_bound_minus1(const uint32_t *s, int n, uint32_t x) {
     int lo = 0, hi = n;  // answer in [lo, hi)
@@ -67,6 +150,11 @@ __device__ __forceinline__ int upper_bound_minus1(const uint32_t *s, int n, uint
     }
     return lo;
 }
+
+// x[i] for a two-element parameter array, without dynamic indexing (which
+// would copy the kernel parameter array to local memory).
+template <class T>
+__device__ __forceinline__ T pick(T const (&x)[2], int i) { return i ? x[1] : x[0]; }
 
 __device__ __forceinline__ bool test_bit(const uint32_t *bm, int32_t v) {
     return (bm[v >> 5] >> (v & 31)) & 1u;

@@ -121,6 +121,9 @@ struct Context {
     int fixed_schedule = -1;
     std::vector<int8_t> replay;    // MB_POLICY_ORACLE_BEST schedule list
     bool use_graphs = true;
+    float sssp_delta = 0.f;        // near-far bucket width (0: off); < 0: chosen per graph
+    bool tail = true;              // persistent single-CTA tail for small frontiers
+    bool persist = false;          // persistent cooperative grid for schedules 0/4
     void *ctrl_readback() { return pinned_small + kCtrlOff; }
     void *pinned_reserve(size_t n) {
         if (n <= pinned_bytes && pinned) return pinned;

@@ -290,6 +290,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             stats->vertices_reached = g.V;
             stats->device_ms = ms;
             stats->schedule_count[unfused ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE] = iters;
+            stats->edges_scanned = (int64_t)iters * g.E;
             stats->kernel_launches = 1 + (int64_t)iters * (1 + (st.nblk > 0) + unfused) + (iters == 0);
         }
     } catch (...) {

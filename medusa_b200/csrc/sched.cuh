@@ -28,14 +28,14 @@ constexpr int kMlpParams = MlpLayout::total;
 //   3 unvisited out-edges log2(1+mu)/log2(1+E)
 //   4 degree skew         log2(max out-degree / mean out-degree) / 16
 //   5 current frontier format (0 queue, 1 bitmap)
-__host__ __device__ inline void make_features(float *f, double n, double m, double nu, double mu,
-                                              double V, double E, double skew, int mode) {
-    const double lv = log2(1.0 + V), le = log2(1.0 + E);
-    f[0] = (float)(log2(1.0 + n) / lv);
-    f[1] = (float)(le > 0 ? log2(1.0 + m) / le : 0.0);
-    f[2] = (float)(log2(1.0 + (nu > 0 ? nu : 0)) / lv);
-    f[3] = (float)(le > 0 ? log2(1.0 + (mu > 0 ? mu : 0)) / le : 0.0);
-    f[4] = (float)(skew / 16.0);
+__host__ __device__ inline void make_features(float *f, float n, float m, float nu, float mu,
+                                              float V, float E, float skew, int mode) {
+    const float lv = log2f(1.0f + V), le = log2f(1.0f + E);
+    f[0] = log2f(1.0f + n) / lv;
+    f[1] = le > 0.f ? log2f(1.0f + m) / le : 0.f;
+    f[2] = log2f(1.0f + fmaxf(nu, 0.f)) / lv;
+    f[3] = le > 0.f ? log2f(1.0f + fmaxf(mu, 0.f)) / le : 0.f;
+    f[4] = skew / 16.0f;
     f[5] = (float)mode;
 }
 

@@ -21,7 +21,8 @@
 //   1 push, warp-per-vertex, queue frontier
 //   2 push, warp-wide edge-balanced over a bitmap frontier
 //   3 push, warp-per-vertex over a bitmap frontier
-//   4 pull (min over in-edges from frontier vertices), thread-per-vertex
+//   4 pull (min over in-edges from frontier vertices), edge-streamed by a
+//     warp per 32 destinations
 //   5 pull, warp-per-vertex
 //   6 the reference's split: message fill, send into msg[mslot[e]],
 //     segmented min per destination, update
@@ -38,35 +39,71 @@ struct SsspArgs {
     float *dist;
     int32_t *stamp;
     float *msg;
+    int32_t *far[2];  // near-far piles (vertices whose distance is >= the threshold)
+    uint32_t *farbm;  // membership bitmap of the pile being filled
 };
 
 __device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
     return __ldcg(&a.dist[v]);  // bypass L1: other SMs lower distances
 }
 
-// Lower dist[v] to nd; true for exactly one caller per (v, superstep) that
-// lowered it, who then puts v into the next frontier.
-__device__ __forceinline__ bool relax(const SsspArgs &a, int32_t v, float nd, int32_t stamp_val) {
+// Lower dist[v] to nd; true if this call lowered it.
+__device__ __forceinline__ bool lower(const SsspArgs &a, int32_t v, float nd) {
     if (!(nd < ld_dist(a, v))) return false;
     const unsigned old = atomicMin((unsigned *)&a.dist[v], __float_as_uint(nd));
-    if (!(nd < __uint_as_float(old))) return false;
+    return nd < __uint_as_float(old);
+}
+
+// True for exactly one caller per (v, superstep): v joins the next frontier.
+__device__ __forceinline__ bool mark(const SsspArgs &a, int32_t v, int32_t stamp_val) {
     return atomicExch(&a.stamp[v], stamp_val) != stamp_val;
 }
 
+__device__ __forceinline__ bool relax(const SsspArgs &a, int32_t v, float nd, int32_t stamp_val) {
+    return lower(a, v, nd) && mark(a, v, stamp_val);
+}
+
+// Near-far: append v to the far pile being filled, once (all lanes call it).
+__device__ __forceinline__ void far_push(const SsspArgs &a, Ctrl *c, bool pred, int32_t v) {
+    if (pred) {
+        const uint32_t bit = 1u << (v & 31);
+        pred = !(atomicOr(&a.farbm[v >> 5], bit) & bit);
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    const int f = c->fcur;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&c->far_n[f], (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) pick(a.far, f)[base + __popc(mask & lanemask_lt())] = v;
+}
+
 // schedule 0: push, merge-path edge-balanced over the queue
-__global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
-    count_launch(a.f.ctrl);
-    __shared__ uint32_t s_off[kTile + 1];
-    __shared__ int32_t s_row[kTile + 1];
-    __shared__ float s_du[kTile + 1];
+struct PushSmem {
+    uint32_t off[kTile + 1];
+    int32_t row[kTile + 1];
+    float du[kTile + 1];
+    BlockQueue bq;
+};
+
+__device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm) {
+    uint32_t *s_off = sm.off;
+    int32_t *s_row = sm.row;
+    float *s_du = sm.du;
+    BlockQueue &bq = sm.bq;
+    if (threadIdx.x == 0) bq.n = 0;
+    __syncthreads();
     Ctrl *c = a.f.ctrl;
     const int cur = c->cur, nxt = cur ^ 1;
     const uint64_t q = c->q[cur];
     const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
     const int32_t sv = c->step + 1;
-    const int32_t *qv = a.f.qv[cur];
-    const uint32_t *qo = a.f.qo[cur];
-    const int32_t *tf = a.f.tf[cur];
+    // near-far: relaxations to >= thresh go to the far pile
+    const float thresh = c->p.delta > 0.f ? c->thresh : 3.0e38f;
+    const int32_t *qv = pick(a.f.qv, cur);
+    const uint32_t *qo = pick(a.f.qo, cur);
+    const int32_t *tf = pick(a.f.tf, cur);
     const uint32_t tiles = (m + kTile - 1) / kTile;
     uint32_t cn = 0;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
@@ -81,28 +118,50 @@ __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
             s_du[j] = ld_dist(a, u);
         }
         __syncthreads();
+        // all loads of the thread's kTileItems edges first, then the relaxations
+        int32_t v[kTileItems];
+        float nd[kTileItems], dv[kTileItems];
+        bool ok[kTileItems];
 #pragma unroll
         for (int r = 0; r < kTileItems; r++) {
             const uint32_t e_idx = c0 + r * kPushThreads + threadIdx.x;
-            bool own = false;
-            int32_t v = 0;
-            uint32_t deg = 0;
-            if (e_idx < c1) {
+            ok[r] = e_idx < c1;
+            v[r] = 0;
+            nd[r] = 0.f;
+            if (ok[r]) {
                 const int j = upper_bound_minus1(s_off, k, e_idx);
                 const int32_t e = s_row[j] + (int32_t)(e_idx - s_off[j]);
-                v = a.col[e];
-                if (relax(a, v, s_du[j] + a.wt[e], sv)) {
-                    deg = (uint32_t)a.f.outdeg[v];
+                v[r] = __ldg(&a.col[e]);
+                nd[r] = s_du[j] + __ldg(&a.wt[e]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kTileItems; r++) dv[r] = ok[r] ? ld_dist(a, v[r]) : 0.f;
+#pragma unroll
+        for (int r = 0; r < kTileItems; r++) {
+            bool own = false, to_far = false;
+            uint32_t deg = 0;
+            if (ok[r] && nd[r] < dv[r] && lower(a, v[r], nd[r])) {
+                if (nd[r] >= thresh) {
+                    to_far = true;
+                } else if (mark(a, v[r], sv)) {
+                    deg = (uint32_t)a.f.outdeg[v[r]];
                     own = true;
                     cn++;
                 }
             }
-            enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], a.f.qv[nxt], a.f.qo[nxt], a.f.tf[nxt]);
+            bq_push(bq, own && deg > 0, v[r], deg);
+            far_push(a, c, to_far, v[r]);
         }
-        __syncthreads();
+        bq_flush(bq, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt), pick(a.f.tf, nxt));
     }
     flush_counts(c, cn, 0);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+}
+
+__global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
+    __shared__ PushSmem sm;
+    count_launch(a.f.ctrl);
+    work_push_edge_q(a, sm);
 }
 
 // schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
@@ -112,7 +171,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
     const int cur = c->cur, nxt = cur ^ 1;
     const uint32_t n = (uint32_t)(c->q[cur] >> 32);
     const int32_t sv = c->step + 1;
-    const int32_t *qv = a.f.qv[cur];
+    const int32_t *qv = pick(a.f.qv, cur);
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     uint32_t cn = 0;
@@ -128,7 +187,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
                 cn++;
             }
         }
-        enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], a.f.qv[nxt], a.f.qo[nxt], a.f.tf[nxt]);
+        enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt), pick(a.f.tf, nxt));
     };
     for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n;
          base += warps * 32) {
@@ -160,7 +219,6 @@ __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
         });
     }
     flush_counts(c, cn, 0);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
 }
 
 // an improved vertex joins the bitmap frontier of the next superstep
@@ -178,8 +236,8 @@ template <bool kEdgeBalanced>
 __global__ void __launch_bounds__(kPushThreads) k_push_bm(SsspArgs a) {
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
-    const uint32_t *front = a.f.bm[c->bcur];
-    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const uint32_t *front = pick(a.f.bm, c->bcur);
+    uint32_t *next = pick(a.f.bm, c->bcur ^ 1);
     const int32_t sv = c->step + 1;
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -215,7 +273,6 @@ __global__ void __launch_bounds__(kPushThreads) k_push_bm(SsspArgs a) {
         }
     }
     flush_counts(c, cn, cm);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
 }
 
 // Pull epilogue of one word: lanes whose `found` is set lowered their vertex
@@ -233,54 +290,62 @@ __device__ __forceinline__ void pull_commit(const SsspArgs &a, uint32_t *next, i
     }
 }
 
-constexpr int kPullLaneCap = 64;
-
-// schedule 4: pull, thread-per-vertex with a warp-cooperative tail
-__global__ void __launch_bounds__(256) k_pull_thread(SsspArgs a) {
-    count_launch(a.f.ctrl);
+// schedules 4 and 7: pull, edge-streamed.  A warp owns 32 consecutive
+// vertices, whose in-edges are contiguous in the reverse CSR; it streams them
+// 32 at a time (coalesced rcol/rwt loads), keeps the candidates dist[u]+w of
+// frontier sources (schedule 7: every source), and min-combines each into its
+// destination's slot with a shared-memory atomicMin on the float bits
+// (non-negative floats order like uint32).  The owner of an edge is found by
+// binary search over the group's 33 offsets.  Hubs stream at full warp width.
+template <bool kAllEdges>
+__device__ __forceinline__ void work_pull_stream(const SsspArgs &a) {
+    constexpr int kWarps = 256 / 32;
+    __shared__ uint32_t s_best[kWarps][32];
+    __shared__ int32_t s_off[kWarps][33];
     Ctrl *c = a.f.ctrl;
-    const uint32_t *front = a.f.bm[c->bcur];
-    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const uint32_t *front = pick(a.f.bm, c->bcur);
+    uint32_t *next = pick(a.f.bm, c->bcur ^ 1);
     const int32_t sv = c->step + 1;
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t *best = s_best[wid];
+    int32_t *off = s_off[wid];
+    const int64_t warps = (int64_t)gridDim.x * kWarps;
     uint32_t cn = 0;
     uint64_t cm = 0;
     for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
-        const int32_t v = (int32_t)(w * 32 + lane);
+        const int32_t vb = (int32_t)(w * 32);
+        const int32_t v = vb + lane;
         const bool valid = v < a.f.V;
-        int32_t j = 0, je = 0;
-        float cur_d = 0.f, best = 0.f;
-        if (valid) {
-            j = a.rrow[v];
-            je = a.rrow[v + 1];
-            cur_d = ld_dist(a, v);
-            best = cur_d;
-            const int32_t jcap = min(je, j + kPullLaneCap);
-            for (; j < jcap; j++) {
-                const int32_t u = a.rcol[j];
-                if (test_bit(front, u)) best = fminf(best, ld_dist(a, u) + a.rwt[j]);
+        off[lane] = a.rrow[min(v, a.f.V)];
+        if (lane == 0) off[32] = a.rrow[min(vb + 32, a.f.V)];
+        const float cur_d = valid ? ld_dist(a, v) : 0.f;
+        best[lane] = __float_as_uint(valid ? cur_d : 3.0e38f);
+        __syncwarp();
+        const int32_t g0 = off[0], g1 = off[32];
+        for (int32_t j = g0 + lane; j < g1; j += 32) {
+            const int32_t u = a.rcol[j];
+            if (kAllEdges || test_bit(front, u)) {
+                const float cand = ld_dist(a, u) + a.rwt[j];
+                int lo = 0, hi = 32;  // last slot whose offset <= j
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (off[mid] <= j) lo = mid; else hi = mid;
+                }
+                atomicMin(&best[lo], __float_as_uint(cand));
             }
         }
-        unsigned pend = __ballot_sync(0xffffffffu, j < je);
-        while (pend) {
-            const int l = __ffs(pend) - 1;
-            pend &= pend - 1;
-            const int32_t pj = __shfl_sync(0xffffffffu, j, l);
-            const int32_t pje = __shfl_sync(0xffffffffu, je, l);
-            float m = 3.0e38f;
-            for (int32_t b = pj + lane; b < pje; b += 32) {
-                const int32_t u = a.rcol[b];
-                if (test_bit(front, u)) m = fminf(m, ld_dist(a, u) + a.rwt[b]);
-            }
-#pragma unroll
-            for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (lane == l) best = fminf(best, m);
-        }
-        pull_commit(a, next, w, v, valid && best < cur_d, best, sv, cn, cm);
+        __syncwarp();
+        const float b = __uint_as_float(best[lane]);
+        pull_commit(a, next, w, v, valid && b < cur_d, b, sv, cn, cm);
+        __syncwarp();
     }
     flush_counts(c, cn, cm);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+template <bool kAllEdges>
+__global__ void __launch_bounds__(256) k_pull_stream(SsspArgs a) {
+    count_launch(a.f.ctrl);
+    work_pull_stream<kAllEdges>(a);
 }
 
 // schedule 5: pull, warp-per-vertex.  mode 1: full Bellman-Ford over every
@@ -289,8 +354,8 @@ template <bool kAllEdges>
 __global__ void __launch_bounds__(256) k_pull_warp(SsspArgs a) {
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
-    const uint32_t *front = a.f.bm[c->bcur];
-    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    const uint32_t *front = pick(a.f.bm, c->bcur);
+    uint32_t *next = pick(a.f.bm, c->bcur ^ 1);
     const int32_t sv = c->step + 1;
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -319,7 +384,6 @@ __global__ void __launch_bounds__(256) k_pull_warp(SsspArgs a) {
         pull_commit(a, next, w, v, ((valid >> lane) & 1u) && mybest < mycur, mybest, sv, cn, cm);
     }
     flush_counts(c, cn, cm);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
 }
 
 // schedule 6, step 1 (InitMessageBuffer, SSSP/InitMessage.h:4-9): msg[] = FLT_MAX
@@ -348,7 +412,7 @@ __global__ void k_msg_send(SsspArgs a) {
 __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
-    uint32_t *next = a.f.bm[c->bcur ^ 1];
+    uint32_t *next = pick(a.f.bm, c->bcur ^ 1);
     const int32_t sv = c->step + 1;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     uint32_t cn = 0;
@@ -365,7 +429,160 @@ __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
         pull_commit(a, next, w, v, found, m, sv, cn, cm);
     }
     flush_counts(c, cn, cm);
-    if (last_block(c)) finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_BITMAP);
+}
+
+// Persistent small-frontier tail (schedule 0 in one CTA): consecutive
+// supersteps in one launch while the queue frontier stays within the tail
+// limits; the CTA does each superstep's bookkeeping itself.  Counters that
+// other threads bump with atomics are read through L2 (ldg2).
+__global__ void __launch_bounds__(kTailThreads) k_tail(SsspArgs a, int cap) {
+    count_launch(a.f.ctrl);
+    __shared__ uint32_t s_off[kTailEntries];
+    __shared__ int32_t s_row[kTailEntries];
+    __shared__ float s_du[kTailEntries];
+    __shared__ int s_go;
+    Ctrl *c = a.f.ctrl;
+    for (;;) {
+        const int cur = ldg2(&c->cur), nxt = cur ^ 1;
+        const unsigned long long q = ldg2(&c->q[cur]);
+        const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
+        const int32_t sv = ldg2(&c->step) + 1;
+        const float delta = c->p.delta;
+        const float thresh = delta > 0.f ? ldg2(&c->thresh) : 3.0e38f;
+        const int32_t *qv = pick(a.f.qv, cur);
+        const uint32_t *qo = pick(a.f.qo, cur);
+        for (uint32_t j = threadIdx.x; j < n; j += kTailThreads) {
+            const int32_t u = qv[j];
+            s_off[j] = qo[j];
+            s_row[j] = a.row[u];
+            s_du[j] = ld_dist(a, u);
+        }
+        __syncthreads();
+        uint32_t cn = 0;
+        for (uint32_t base = 0; base < m; base += kTailThreads) {
+            const uint32_t e_idx = base + threadIdx.x;
+            bool own = false, to_far = false;
+            int32_t v = 0;
+            uint32_t deg = 0;
+            if (e_idx < m) {
+                const int j = upper_bound_minus1(s_off, (int)n, e_idx);
+                const int32_t e = s_row[j] + (int32_t)(e_idx - s_off[j]);
+                v = __ldg(&a.col[e]);
+                const float nd = s_du[j] + __ldg(&a.wt[e]);
+                if (lower(a, v, nd)) {
+                    if (nd >= thresh) {
+                        to_far = true;
+                    } else if (mark(a, v, sv)) {
+                        deg = (uint32_t)a.f.outdeg[v];
+                        own = true;
+                        cn++;
+                    }
+                }
+            }
+            enqueue_warp(own && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
+                         pick(a.f.tf, nxt));
+            far_push(a, c, to_far, v);
+        }
+        flush_counts(c, cn, 0);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+            c->iter++;
+            if (c->iter > cap && !c->done) {
+                c->err |= ERR_STEP_CAP;
+                c->done = 1;
+            }
+            s_go = !c->done && c->branch == kBranchTail;
+            __threadfence();
+        }
+        __syncthreads();
+        if (!s_go) break;
+    }
+    // every superstep this kernel ran is finished already
+    if (threadIdx.x == 0) c->pending = 0;
+}
+
+// Near-far split: the threshold was just raised by delta; every far-pile
+// vertex now below it joins the near queue, the rest move to the other pile.
+__device__ __forceinline__ void work_far_split(const SsspArgs &a) {
+    Ctrl *c = a.f.ctrl;
+    const int f = c->fcur;
+    const uint32_t n = c->far_n[f];
+    const int32_t *src = pick(a.far, f);
+    const float thresh = c->thresh, thresh_prev = c->thresh - c->p.delta;
+    const int nxt = c->cur ^ 1;
+    const int32_t sv = c->step + 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n;
+         base += warps * 32) {
+        const int64_t i = base + lane;
+        bool near = false, keep = false;
+        int32_t v = 0;
+        uint32_t deg = 0;
+        if (i < n) {
+            v = src[i];
+            const float d = ld_dist(a, v);
+            if (d < thresh) {
+                // leaves the piles; a kept vertex keeps its bit, the pile it
+                // moves to becomes the one being filled.  Below the previous
+                // threshold it was expanded at this distance already (it got
+                // there through the near queue), so it is dropped.
+                atomicAnd(&a.farbm[v >> 5], ~(1u << (v & 31)));
+                if (d >= thresh_prev && mark(a, v, sv)) {
+                    deg = (uint32_t)a.f.outdeg[v];
+                    near = true;
+                    cn++;
+                }
+            } else {
+                keep = true;
+            }
+        }
+        enqueue_warp(near && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
+                     pick(a.f.tf, nxt));
+        // the kept ones go to the other pile
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            uint32_t b = 0;
+            if (lane == leader) b = atomicAdd(&c->far_n[f ^ 1], (uint32_t)__popc(mask));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (keep) pick(a.far, f ^ 1)[b + __popc(mask & lanemask_lt())] = v;
+        }
+    }
+    flush_counts(c, cn, 0);
+}
+
+__global__ void __launch_bounds__(256) k_far_split(SsspArgs a) {
+    count_launch(a.f.ctrl);
+    work_far_split(a);
+}
+
+// Persistent BSP kernel (cooperative launch, all blocks resident): runs
+// consecutive supersteps of schedules 0 and 4 (with their frontier
+// conversions) and near-far splits, separated by grid barriers; block 0 does
+// each superstep's bookkeeping between two barriers.  Leaves when the next
+// superstep needs another schedule, the run is done, or a barrier gives up.
+__global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
+    __shared__ PushSmem sm;
+    Ctrl *c = a.f.ctrl;
+    count_launch(c);
+    for (;;) {
+        const int s = ldg2(&c->sched), mode = ldg2(&c->mode);
+        if (s == kSchedSplit) {
+            work_far_split(a);
+        } else {
+            if (!persist_convert(a.f, s, mode)) break;
+            if (s == MB_SCHED_PULL_THREAD) work_pull_stream<false>(a);
+            else work_push_edge_q(a, sm);
+        }
+        if (!grid_sync(c)) break;
+        persist_bookkeep(a.f, APP_SSSP, cap);
+        if (!grid_sync(c)) break;
+        if (!ldg2(&c->persist_go)) break;
+    }
 }
 
 __global__ void k_sssp_init(SsspArgs a) {
@@ -391,18 +608,26 @@ __global__ void k_sssp_init(SsspArgs a) {
         c->prev_nf = 1;
         c->reached = 0;
         c->edges_reached = 0;
+        c->work = 0;
+        c->pending = 0;
+        c->thresh = c->p.delta;
+        c->far_n[0] = 0;
+        c->far_n[1] = 0;
+        c->fcur = 0;
+        c->splits = 0;
+        c->bar_count = 0;
         c->q[1] = 0ull;
         c->m_unvisited = a.f.E - deg;
         c->n_unvisited = a.f.V - 1;
         if (deg > 0) {
-            a.f.qv[0][0] = source;
-            a.f.qo[0][0] = 0;
+            pick(a.f.qv, 0)[0] = source;
+            pick(a.f.qo, 0)[0] = 0;
             c->q[0] = (1ull << 32) | (uint32_t)deg;
         } else {
             c->q[0] = 0ull;
         }
     }
-    for (int32_t t = threadIdx.x; deg > 0 && t * kTile < deg; t += blockDim.x) a.f.tf[0][t] = 0;
+    for (int32_t t = threadIdx.x; deg > 0 && t * kTile < deg; t += blockDim.x) pick(a.f.tf, 0)[t] = 0;
     __syncthreads();
     if (threadIdx.x == 0) choose_next(c, APP_SSSP, a.f.V, a.f.E);
 }
@@ -435,7 +660,31 @@ __global__ void k_stats(SsspArgs a) {
     }
 }
 
+__global__ void k_weight_sum(const float *w, int64_t E, double *out) {
+    double t = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < E;
+         i += (int64_t)gridDim.x * blockDim.x)
+        t += w[i];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, t);
+}
+
 }  // namespace
+
+float sssp_default_delta(const Graph &g) {
+    if (g.E == 0) return 0.f;
+    DevBuf acc;
+    acc.reserve(sizeof(double));
+    MB_CUDA(cudaMemset(acc.p, 0, sizeof(double)));
+    k_weight_sum<<<grid_for(g.E, 256, 1184), 256>>>(g.wt.as<float>(), g.E, acc.as<double>());
+    MB_CHECK_LAUNCH();
+    double sum = 0;
+    MB_CUDA(cudaMemcpy(&sum, acc.p, sizeof(double), cudaMemcpyDeviceToHost));
+    acc.release();
+    const double mean_w = sum / (double)g.E, mean_deg = (double)g.E / (double)g.V;
+    constexpr double kDeltaWarps = 32.0;
+    return (float)(mean_w * kDeltaWarps / std::max(1.0, mean_deg));
+}
 
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats) {
     st.ensure(g);
@@ -451,23 +700,45 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.dist = st.dist.as<float>();
     a.stamp = st.stamp.as<int32_t>();
     a.msg = st.msg.as<float>();
-    upload_params(ctx, st.ctrl.p, source);
+    a.far[0] = st.far[0].as<int32_t>();
+    a.far[1] = st.far[1].as<int32_t>();
+    a.farbm = st.farbm.as<uint32_t>();
+    // near-far bucket width: the context's, or a per-graph default
+    const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
+    upload_params(ctx, st.ctrl.p, source, delta);
 
-    const int grid_push = ctx.num_sms * 4, grid_vtx = ctx.num_sms * 8, grid_edge = ctx.num_sms * 8;
+    const int grid_push = ctx.num_sms * 8, grid_vtx = ctx.num_sms * 8, grid_edge = ctx.num_sms * 8;
+    const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
     LoopSpec sp;
     sp.st = &st;
     sp.fa = a.f;
     // each superstep lowers some distance; with integer distances below 2^24
     // a run cannot need more supersteps than this
+    sp.app = APP_SSSP;
     sp.cap = (int)std::min<int64_t>((int64_t)g.V * 4 + 16, 1 << 30);
     sp.name = "sssp";
     sp.prologue = [&](cudaStream_t s) {
         k_fill_dist<<<grid_vtx, 256, 0, s>>>(a);
         MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
+        MB_CUDA(cudaMemsetAsync(a.farbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
         k_sssp_init<<<1, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();
     };
     sp.branch = [&](int branch, cudaStream_t s) {
+        if (branch == kBranchSplit) {
+            k_far_split<<<grid_vtx, 256, 0, s>>>(a);
+            MB_CHECK_LAUNCH();
+            return;
+        }
+        if (branch == kBranchTail) {
+            k_tail<<<1, kTailThreads, 0, s>>>(a, sp.cap);
+            MB_CHECK_LAUNCH();
+            return;
+        }
+        if (branch == kBranchPersist) {
+            launch_cooperative((const void *)k_persist, persist_grid, kPushThreads, s, a, sp.cap);
+            return;
+        }
         const int sched = branch % MB_NUM_SCHEDULES;
         if (branch >= MB_NUM_SCHEDULES) {
             if (sched_input(sched) == FMT_BITMAP) {
@@ -489,14 +760,14 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
                 k_bm_clear<<<grid_vtx, 256, 0, s>>>(a.f, 1);
                 k_push_bm<false><<<grid_push, kPushThreads, 0, s>>>(a);
                 break;
-            case MB_SCHED_PULL_THREAD: k_pull_thread<<<grid_vtx, 256, 0, s>>>(a); break;
+            case MB_SCHED_PULL_THREAD: k_pull_stream<false><<<grid_vtx, 256, 0, s>>>(a); break;
             case MB_SCHED_PULL_WARP: k_pull_warp<false><<<grid_vtx, 256, 0, s>>>(a); break;
             case MB_SCHED_PUSH_UNFUSED:
                 k_msg_fill<<<grid_edge, 256, 0, s>>>(a);
                 k_msg_send<<<grid_vtx, 256, 0, s>>>(a);
                 k_msg_combine_update<<<grid_vtx, 256, 0, s>>>(a);
                 break;
-            default: k_pull_warp<true><<<grid_vtx, 256, 0, s>>>(a); break;
+            default: k_pull_stream<true><<<grid_vtx, 256, 0, s>>>(a); break;
         }
         MB_CHECK_LAUNCH();
     };

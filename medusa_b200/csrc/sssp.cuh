@@ -4,14 +4,22 @@
 
 namespace mb {
 
+// Default near-far bucket width of a graph: kDeltaWarps warps' worth of
+// edges per bucket at the mean degree, times the mean weight.
+float sssp_default_delta(const Graph &g);
+
 struct SsspState : FrontierState {
-    DevBuf dist, stamp, msg;
+    DevBuf dist, stamp, msg, far[2], farbm;
+    float default_delta = 0.f;
     ~SsspState() { release(); }
     void release() {
         release_frontier();
         dist.release();
         stamp.release();
         msg.release();
+        far[0].release();
+        far[1].release();
+        farbm.release();
     }
     void ensure(const Graph &g) {
         if (ensure_frontier(g)) {
@@ -23,6 +31,10 @@ struct SsspState : FrontierState {
             // E-slot message array of the unfused schedule (the reference's
             // MessageArray, MultipleGPU/MultiPublicAPI.h:178-199)
             msg.reserve(sizeof(float) * (size_t)std::max<int64_t>(g.E, 1));
+            far[0].reserve(sizeof(int32_t) * (size_t)g.V);
+            far[1].reserve(sizeof(int32_t) * (size_t)g.V);
+            farbm.reserve(sizeof(uint32_t) * (size_t)W);
+            default_delta = sssp_default_delta(g);
         }
     }
 };

@@ -110,6 +110,41 @@ def test_every_schedule_bit_identical(gpu_ctx, api, name):
         g.close()
 
 
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "uniform_2k"])
+def test_persistent_tail_and_grid_on_off_identical(gpu_ctx, api, name):
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        for tail, grid in ((False, False), (True, False), (False, True), (True, True)):
+            gpu_ctx.set_persistent_tail(tail)
+            gpu_ctx.set_persistent_grid(grid)
+            for i, s in enumerate(c["sources"]):
+                lv, _ = g.bfs([s])
+                np.testing.assert_array_equal(lv[0], c["bfs_level"][i])
+                d, _ = g.sssp([s])
+                np.testing.assert_array_equal(d[0], c["sssp_dist"][i])
+    finally:
+        gpu_ctx.set_persistent_tail(True)
+        gpu_ctx.set_persistent_grid(False)
+        g.close()
+
+
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "tiny"])
+def test_sssp_every_delta_identical(gpu_ctx, api, name):
+    """Near-far bucket widths (and plain Bellman-Ford) give the same distances."""
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        for delta in (0.0, 1.0, 37.0, 500.0, 5000.0, -1.0):
+            gpu_ctx.set_sssp_delta(delta)
+            for i, s in enumerate(c["sources"]):
+                d, _ = g.sssp([s])
+                np.testing.assert_array_equal(d[0], c["sssp_dist"][i], err_msg="delta %g" % delta)
+    finally:
+        gpu_ctx.set_sssp_delta(0.0)
+        g.close()
+
+
 def test_oracle_replay_policy(gpu_ctx, api):
     """A per-superstep schedule list (alternating push/pull) gives the same levels."""
     c = load_golden("rmat_s10")
