@@ -76,18 +76,23 @@ __device__ __forceinline__ void work_push_edge_q(const BfsArgs &a, PushSmem &sm)
             s_row[j] = a.row[qv[i0 + j]];
         }
         __syncthreads();
-        // all the thread's edge loads first, then the claims
+        // the thread's kTileItems CONSECUTIVE edges: one binary search for the
+        // first, then walk; all loads first, then the claims
         int32_t v[kTileItems];
         uint32_t vw[kTileItems];
         bool ok[kTileItems];
+        {
+            const uint32_t e0 = c0 + threadIdx.x * kTileItems;
+            int j = e0 < c1 ? upper_bound_minus1(s_off, k, e0) : 0;
 #pragma unroll
-        for (int r = 0; r < kTileItems; r++) {
-            const uint32_t e_idx = c0 + r * kPushThreads + threadIdx.x;
-            ok[r] = e_idx < c1;
-            v[r] = 0;
-            if (ok[r]) {
-                const int j = upper_bound_minus1(s_off, k, e_idx);
-                v[r] = __ldg(&a.col[s_row[j] + (int32_t)(e_idx - s_off[j])]);
+            for (int r = 0; r < kTileItems; r++) {
+                const uint32_t e_idx = e0 + r;
+                ok[r] = e_idx < c1;
+                v[r] = 0;
+                if (ok[r]) {
+                    while (j + 1 < k && s_off[j + 1] <= e_idx) j++;
+                    v[r] = __ldg(&a.col[s_row[j] + (int32_t)(e_idx - s_off[j])]);
+                }
             }
         }
 #pragma unroll

@@ -118,21 +118,26 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
             s_du[j] = ld_dist(a, u);
         }
         __syncthreads();
-        // all loads of the thread's kTileItems edges first, then the relaxations
+        // the thread's kTileItems CONSECUTIVE edges: one binary search for the
+        // first, then walk; all loads first, then the relaxations
         int32_t v[kTileItems];
         float nd[kTileItems], dv[kTileItems];
         bool ok[kTileItems];
+        {
+            const uint32_t e0 = c0 + threadIdx.x * kTileItems;
+            int j = e0 < c1 ? upper_bound_minus1(s_off, k, e0) : 0;
 #pragma unroll
-        for (int r = 0; r < kTileItems; r++) {
-            const uint32_t e_idx = c0 + r * kPushThreads + threadIdx.x;
-            ok[r] = e_idx < c1;
-            v[r] = 0;
-            nd[r] = 0.f;
-            if (ok[r]) {
-                const int j = upper_bound_minus1(s_off, k, e_idx);
-                const int32_t e = s_row[j] + (int32_t)(e_idx - s_off[j]);
-                v[r] = __ldg(&a.col[e]);
-                nd[r] = s_du[j] + __ldg(&a.wt[e]);
+            for (int r = 0; r < kTileItems; r++) {
+                const uint32_t e_idx = e0 + r;
+                ok[r] = e_idx < c1;
+                v[r] = 0;
+                nd[r] = 0.f;
+                if (ok[r]) {
+                    while (j + 1 < k && s_off[j + 1] <= e_idx) j++;
+                    const int32_t e = s_row[j] + (int32_t)(e_idx - s_off[j]);
+                    v[r] = __ldg(&a.col[e]);
+                    nd[r] = s_du[j] + __ldg(&a.wt[e]);
+                }
             }
         }
 #pragma unroll
@@ -141,7 +146,11 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
         for (int r = 0; r < kTileItems; r++) {
             bool own = false, to_far = false;
             uint32_t deg = 0;
-            if (ok[r] && nd[r] < dv[r] && lower(a, v[r], nd[r])) {
+            if (ok[r] && nd[r] < dv[r]) {
+                // fire-and-forget minimum; v is queued whenever this candidate
+                // beat the distance just read -- if another thread lowered it
+                // further meanwhile, v is queued anyway, which is harmless
+                atomicMin((unsigned *)&a.dist[v[r]], __float_as_uint(nd[r]));
                 if (nd[r] >= thresh) {
                     to_far = true;
                 } else if (mark(a, v[r], sv)) {
