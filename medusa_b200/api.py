@@ -74,6 +74,7 @@ def _load():
         "mb_set_sssp_delta": (ctypes.c_int, [P, F32]),
         "mb_set_persistent_tail": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_set_persistent_grid": (ctypes.c_int, [P, ctypes.c_int]),
+        "mb_set_batching": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_graph_from_edges": (ctypes.c_int, [P, I32, I64, P, P, P, U32, ctypes.POINTER(P)]),
         "mb_graph_generate": (ctypes.c_int, [P, ctypes.POINTER(GenParams), U32,
                                              ctypes.POINTER(P)]),
@@ -276,6 +277,9 @@ class Context:
 
     def set_persistent_grid(self, enable):
         _check(lib.mb_set_persistent_grid(self.h, 1 if enable else 0), self.h)
+
+    def set_batching(self, enable):
+        _check(lib.mb_set_batching(self.h, 1 if enable else 0), self.h)
 
     def set_graph_capture(self, enable):
         _check(lib.mb_set_graph_capture(self.h, 1 if enable else 0), self.h)

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include "bfs.cuh"
+#include "msbfs.cuh"
 #include "pagerank.cuh"
 #include "sched.cuh"
 #include "sssp.cuh"
@@ -13,6 +14,7 @@
 namespace mb {
 struct AppStates {
     BfsState bfs;
+    MsBfsState msbfs;
     SsspState sssp;
     PrState pr;
 };
@@ -177,6 +179,12 @@ int mb_set_persistent_grid(mb_ctx *ctx, int enable) {
     return MB_OK;
 }
 
+int mb_set_batching(mb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    ctx->c.batching = enable != 0;
+    return MB_OK;
+}
+
 int mb_set_graph_capture(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.use_graphs = enable != 0;
@@ -299,6 +307,32 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
         for (int32_t s : src)
             if (s < 0 || s >= V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
         mb_stats total{};
+        if (nsrc > 1 && ctx->c.batching) {
+            // batches of up to 64 sources, one masked traversal each
+            mb::MsBfsState &ms = apps(g).msbfs;
+            ms.ensure(g->g);  // before reserving ms.out (a rebuild releases it)
+            const bool dev_out = mb::is_device_ptr(levels_out);
+            for (int32_t b0 = 0; b0 < nsrc; b0 += 64) {
+                const int32_t nb = std::min<int32_t>(64, nsrc - b0);
+                int32_t *dst = levels_out + (size_t)b0 * V;
+                int32_t *dev = dst;
+                if (!dev_out) dev = (int32_t *)ms.out.reserve(sizeof(int32_t) * (size_t)nb * V);
+                mb_stats st{};
+                mb::run_msbfs(ctx->c, g->g, ms, src.data() + b0, nb, dev, &st);
+                if (!dev_out)
+                    MB_CUDA(cudaMemcpyAsync(dst, dev, sizeof(int32_t) * (size_t)nb * V,
+                                            cudaMemcpyDeviceToHost, ctx->c.stream));
+                total.supersteps = std::max(total.supersteps, st.supersteps);
+                total.edges_traversed += st.edges_traversed;
+                total.vertices_reached += st.vertices_reached;
+                total.device_ms += st.device_ms;
+                total.kernel_launches += st.kernel_launches;
+                for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+            }
+            MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+            if (stats) *stats = total;
+            return;
+        }
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};
             mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st);

@@ -124,6 +124,7 @@ struct Context {
     float sssp_delta = 0.f;        // near-far bucket width (0: off); < 0: chosen per graph
     bool tail = true;              // persistent single-CTA tail for small frontiers
     bool persist = false;          // persistent cooperative grid for schedules 0/4
+    bool batching = true;          // several BFS sources: one masked traversal per 64
     void *ctrl_readback() { return pinned_small + kCtrlOff; }
     void *pinned_reserve(size_t n) {
         if (n <= pinned_bytes && pinned) return pinned;

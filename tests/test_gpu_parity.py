@@ -268,3 +268,44 @@ def test_full_size_pagerank_c1_against_oracle(gpu_ctx, api):
     # in-degrees are far below the hub threshold: same order as the oracle
     np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
     g.close()
+
+
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "tiny", "empty"])
+def test_batched_bfs_equals_single_source_runs(gpu_ctx, api, name):
+    """64-bit-mask batched BFS: levels of every source equal the oracle's."""
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    rng = np.random.default_rng(3)
+    srcs = list(rng.integers(0, c["V"], size=min(70, 3 * c["V"])))
+    srcs[:len(c["sources"])] = list(c["sources"])
+    if len(srcs) > 2:
+        srcs[2] = srcs[1]  # a repeated source
+    lv, st = g.bfs(srcs)
+    aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+    outdeg = aa.out_degree()
+    er = 0
+    for i, s in enumerate(srcs):
+        want, _ = O.bfs(c["V"], aa, None, [s])
+        np.testing.assert_array_equal(lv[i], want, err_msg="source %d (#%d)" % (s, i))
+        er += int(outdeg[want >= 0].sum())
+    assert st["edges_traversed"] == er
+    gpu_ctx.set_batching(False)
+    lv2, _ = g.bfs(srcs)
+    gpu_ctx.set_batching(True)
+    np.testing.assert_array_equal(lv, lv2)
+    g.close()
+
+
+def test_batched_bfs_c4_size_certificates(gpu_ctx, api):
+    """64 sources on a 2^20-vertex R-MAT: each source's levels pass the BFS certificate."""
+    p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=2)
+    V, s_, d_, _ = api.generate_edges_host(p)
+    g = gpu_ctx.generate(p)
+    srcs = list(range(64))
+    lv, st = g.bfs(srcs)
+    for i in (0, 1, 17, 63):
+        bfs_certificate(V, s_, d_, lv[i], srcs[i])
+    single, _ = g.bfs([17])
+    gpu_ctx.set_batching(True)
+    np.testing.assert_array_equal(lv[17], single[0])
+    g.close()
