@@ -133,10 +133,10 @@ int mb_set_persistent_tail(mb_ctx *ctx, int enable);
  * grid barriers between them (bounded waits: MB_ERR_TIMEOUT if one gives up);
  * 0 (the default): one launch per superstep.  Identical results either way. */
 int mb_set_persistent_grid(mb_ctx *ctx, int enable);
-/* 1 (default): BFS with several sources runs them batched, 64 per traversal
- * with 64-bit per-vertex source masks (one edge scan serves every source
- * whose frontier holds its tail); 0: one traversal per source.  Identical
- * levels either way.  No reference counterpart. */
+/* 1 (default): BFS (SSSP) with several sources runs them batched, 64 (32)
+ * per traversal with per-vertex source masks -- one edge scan serves every
+ * source whose frontier holds its tail; 0: one traversal per source.
+ * Identical results either way.  No reference counterpart. */
 int mb_set_batching(mb_ctx *ctx, int enable);
 /* 1: run whole iteration loops as CUDA graphs with device-side convergence
  * (no host round trip per superstep); 0: host-driven loop, one flag read per

@@ -7,6 +7,7 @@
 #include <new>
 #include "bfs.cuh"
 #include "msbfs.cuh"
+#include "mssssp.cuh"
 #include "pagerank.cuh"
 #include "sched.cuh"
 #include "sssp.cuh"
@@ -16,6 +17,7 @@ struct AppStates {
     BfsState bfs;
     MsBfsState msbfs;
     SsspState sssp;
+    MsSsspState mssssp;
     PrState pr;
 };
 int64_t generate_edges_host(const mb_gen_params &p, int32_t *src, int32_t *dst, float *w);
@@ -364,6 +366,33 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
         for (int32_t s : src)
             if (s < 0 || s >= V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
         mb_stats total{};
+        if (nsrc > 1 && ctx->c.batching) {
+            // batches of up to 32 sources, one masked traversal each
+            mb::MsSsspState &ms = apps(g).mssssp;
+            ms.ensure(g->g);  // before reserving ms.out (a rebuild releases it)
+            const bool dev_out = mb::is_device_ptr(dist_out);
+            for (int32_t b0 = 0; b0 < nsrc; b0 += 32) {
+                const int32_t nb = std::min<int32_t>(32, nsrc - b0);
+                float *dst = dist_out + (size_t)b0 * V;
+                float *dev = dst;
+                if (!dev_out) dev = (float *)ms.out.reserve(sizeof(float) * (size_t)nb * V);
+                mb_stats st{};
+                mb::run_mssssp(ctx->c, g->g, ms, src.data() + b0, nb, dev, &st);
+                if (!dev_out)
+                    MB_CUDA(cudaMemcpyAsync(dst, dev, sizeof(float) * (size_t)nb * V,
+                                            cudaMemcpyDeviceToHost, ctx->c.stream));
+                total.supersteps = std::max(total.supersteps, st.supersteps);
+                total.edges_traversed += st.edges_traversed;
+                total.vertices_reached += st.vertices_reached;
+                total.device_ms += st.device_ms;
+                total.kernel_launches += st.kernel_launches;
+                total.edges_scanned += st.edges_scanned;
+                for (int k = 0; k < MB_NUM_SCHEDULES; k++) total.schedule_count[k] += st.schedule_count[k];
+            }
+            MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+            if (stats) *stats = total;
+            return;
+        }
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};
             mb::run_sssp(ctx->c, g->g, apps(g).sssp, src[i], &st);

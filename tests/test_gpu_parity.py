@@ -309,3 +309,21 @@ def test_batched_bfs_c4_size_certificates(gpu_ctx, api):
     gpu_ctx.set_batching(True)
     np.testing.assert_array_equal(lv[17], single[0])
     g.close()
+
+
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "tiny", "empty"])
+def test_batched_sssp_equals_single_source_runs(gpu_ctx, api, name):
+    """32-source batched SSSP: distances of every source equal the oracle's."""
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    rng = np.random.default_rng(5)
+    srcs = list(rng.integers(0, c["V"], size=min(40, 3 * c["V"])))
+    srcs[:len(c["sources"])] = list(c["sources"])
+    if len(srcs) > 2:
+        srcs[2] = srcs[1]
+    d, st = g.sssp(srcs)
+    aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+    for i, s in enumerate(srcs):
+        want, _ = O.sssp(c["V"], aa, None, None, s)
+        np.testing.assert_array_equal(d[i], want, err_msg="source %d (#%d)" % (s, i))
+    g.close()
