@@ -194,6 +194,37 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
+/* ---- learned scheduler (no reference counterpart) ------------------------ */
+/* Timing traces for the learned scheduler.  app: 0 BFS, 1 SSSP.  For every
+ * superstep of a fixed-rule traversal from `source`, the traversal is replayed
+ * with each of the 8 schedules at that superstep (same choices before it) and
+ * that superstep is timed alone.  Writes up to max_samples rows of
+ * features[6] (the scheduler inputs) and times[8] (ms; -1: not measured) to
+ * host arrays, and (nullable) fixed_sched[1] = the schedule the fixed rule
+ * chose there; *n_out = rows written. */
+int mb_scheduler_collect(mb_ctx *ctx, const mb_graph *g, int32_t app, int32_t source,
+                         float *features, float *times, int32_t *fixed_sched,
+                         int32_t max_samples, int32_t *n_out);
+/* Train the scheduler MLP (6-32-32-8, FP32) on the GPU: seeded init, `epochs`
+ * full-batch Adam steps at learning rate lr, loss = cross-entropy against a
+ * softmax of the negated relative times.  Arrays may be host or device.
+ * *final_loss (nullable) gets the loss after training.  The weights then
+ * serve MB_POLICY_LEARNED. */
+int mb_scheduler_train(mb_ctx *ctx, const float *features, const float *times, int32_t n,
+                       int32_t epochs, float lr, uint64_t seed, float *final_loss);
+/* Number of MLP parameters (row-major w1[32][6], b1[32], w2[32][32], b2[32],
+ * w3[8][32], b3[8]). */
+int32_t mb_scheduler_num_params(void);
+int mb_scheduler_get_weights(mb_ctx *ctx, float *weights);
+int mb_scheduler_set_weights(mb_ctx *ctx, const float *weights);
+/* Mean loss and its gradient (mean over the n samples) for given weights,
+ * computed by the training kernels (for checking them against an FP64 CPU
+ * implementation). */
+int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features,
+                      const float *times, int32_t n, float *grad_out, float *loss_out);
+/* The schedule the current weights pick for each of n feature rows. */
+int mb_scheduler_pick(mb_ctx *ctx, const float *features, int32_t n, int32_t *out);
+
 /* PageRank that allocates no memory, for callers that cannot call cudaMalloc
  * (a host application that owns all GPU memory through its own pool, or a
  * latency-bound caller that cannot accept cudaMalloc/cudaFree's device

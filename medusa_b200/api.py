@@ -87,6 +87,14 @@ def _load():
         "mb_sssp": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank_noalloc": (ctypes.c_int, [P, P, P, I32, I64, I32, F32, P, P]),
+        "mb_scheduler_collect": (ctypes.c_int, [P, P, I32, I32, P, P, P, I32, ctypes.POINTER(I32)]),
+        "mb_scheduler_train": (ctypes.c_int, [P, P, P, I32, I32, F32, ctypes.c_uint64,
+                                              ctypes.POINTER(F32)]),
+        "mb_scheduler_num_params": (I32, []),
+        "mb_scheduler_get_weights": (ctypes.c_int, [P, P]),
+        "mb_scheduler_set_weights": (ctypes.c_int, [P, P]),
+        "mb_scheduler_grad": (ctypes.c_int, [P, P, P, P, I32, P, ctypes.POINTER(F32)]),
+        "mb_scheduler_pick": (ctypes.c_int, [P, P, I32, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -277,6 +285,55 @@ class Context:
 
     def set_persistent_grid(self, enable):
         _check(lib.mb_set_persistent_grid(self.h, 1 if enable else 0), self.h)
+
+    # ---- learned scheduler ----
+    def scheduler_collect(self, g, app, source, max_samples=4096):
+        """Timing traces of one run (app 0 BFS, 1 SSSP): features [n,6],
+        per-schedule superstep times [n,8] (ms, -1 unmeasured) and the
+        schedule the fixed rule chose at each superstep [n]."""
+        X = np.zeros((max_samples, 6), np.float32)
+        T = np.zeros((max_samples, 8), np.float32)
+        S = np.zeros(max_samples, np.int32)
+        n = ctypes.c_int32(0)
+        _check(lib.mb_scheduler_collect(self.h, g.h, int(app), int(source), X.ctypes.data,
+                                        T.ctypes.data, S.ctypes.data, max_samples,
+                                        ctypes.byref(n)), self.h)
+        k = n.value
+        return X[:k].copy(), T[:k].copy(), S[:k].copy()
+
+    def scheduler_train(self, X, T, epochs=1500, lr=3e-3, seed=1):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        loss = ctypes.c_float(0)
+        _check(lib.mb_scheduler_train(self.h, X.ctypes.data, T.ctypes.data, len(X), int(epochs),
+                                      float(lr), int(seed), ctypes.byref(loss)), self.h)
+        return loss.value
+
+    def scheduler_weights(self):
+        w = np.zeros(lib.mb_scheduler_num_params(), np.float32)
+        _check(lib.mb_scheduler_get_weights(self.h, w.ctypes.data), self.h)
+        return w
+
+    def scheduler_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        assert len(w) == lib.mb_scheduler_num_params()
+        _check(lib.mb_scheduler_set_weights(self.h, w.ctypes.data), self.h)
+
+    def scheduler_grad(self, w, X, T):
+        w = np.ascontiguousarray(w, np.float32)
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        g = np.zeros(lib.mb_scheduler_num_params(), np.float32)
+        loss = ctypes.c_float(0)
+        _check(lib.mb_scheduler_grad(self.h, w.ctypes.data, X.ctypes.data, T.ctypes.data, len(X),
+                                     g.ctypes.data, ctypes.byref(loss)), self.h)
+        return g, loss.value
+
+    def scheduler_pick(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        out = np.zeros(len(X), np.int32)
+        _check(lib.mb_scheduler_pick(self.h, X.ctypes.data, len(X), out.ctypes.data), self.h)
+        return out
 
     def set_batching(self, enable):
         _check(lib.mb_set_batching(self.h, 1 if enable else 0), self.h)

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include "bfs.cuh"
+#include "learn.cuh"
 #include "msbfs.cuh"
 #include "mssssp.cuh"
 #include "pagerank.cuh"
@@ -191,6 +192,101 @@ int mb_set_graph_capture(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.use_graphs = enable != 0;
     return MB_OK;
+}
+
+namespace {
+// n*k floats from host or device memory into a temporary device buffer
+void to_device(mb::DevBuf &b, const float *p, size_t count) {
+    b.reserve(sizeof(float) * std::max<size_t>(count, 1));
+    if (count) MB_CUDA(cudaMemcpy(b.p, p, sizeof(float) * count, cudaMemcpyDefault));
+}
+}  // namespace
+
+int mb_scheduler_collect(mb_ctx *ctx, const mb_graph *gc, int32_t app, int32_t source,
+                         float *features, float *times, int32_t *fixed_sched,
+                         int32_t max_samples, int32_t *n_out) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (app != 0 && app != 1) mb::fail(MB_ERR_INVALID, "app must be 0 (BFS) or 1 (SSSP)");
+        if (!features || !times || !n_out || max_samples < 0) mb::fail(MB_ERR_INVALID, "bad output");
+        if (source < 0 || source >= gc->g.V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        *n_out = mb::collect_traces(ctx->c, g->g, apps(g).bfs, apps(g).sssp,
+                                    app == 0 ? mb::APP_BFS : mb::APP_SSSP, source, features, times,
+                                    fixed_sched, max_samples);
+    });
+}
+
+int mb_scheduler_train(mb_ctx *ctx, const float *features, const float *times, int32_t n,
+                       int32_t epochs, float lr, uint64_t seed, float *final_loss) {
+    return guarded(ctx, [&] {
+        if (!ctx) mb::fail(MB_ERR_INVALID, "null context");
+        if (n < 1 || !features || !times || epochs < 0 || !(lr > 0.f))
+            mb::fail(MB_ERR_INVALID, "bad training arguments");
+        use_device(ctx);
+        mb::DevBuf X, T;
+        to_device(X, features, (size_t)n * mb::kFeat);
+        to_device(T, times, (size_t)n * mb::kOut);
+        const float loss = mb::mlp_train(ctx->c, X.as<float>(), T.as<float>(), n, epochs, lr, seed);
+        if (final_loss) *final_loss = loss;
+        X.release();
+        T.release();
+    });
+}
+
+int32_t mb_scheduler_num_params(void) { return mb::kMlpParams; }
+
+int mb_scheduler_get_weights(mb_ctx *ctx, float *w) {
+    return guarded(ctx, [&] {
+        if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
+        use_device(ctx);
+        MB_CUDA(cudaMemcpy(w, ctx->c.mlp.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+    });
+}
+
+int mb_scheduler_set_weights(mb_ctx *ctx, const float *w) {
+    return guarded(ctx, [&] {
+        if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
+        use_device(ctx);
+        MB_CUDA(cudaMemcpy(ctx->c.mlp.p, w, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        ctx->c.mlp_ready = true;
+    });
+}
+
+int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features, const float *times,
+                      int32_t n, float *grad_out, float *loss_out) {
+    return guarded(ctx, [&] {
+        if (!ctx || !weights || !features || !times || !grad_out || n < 1)
+            mb::fail(MB_ERR_INVALID, "null argument");
+        use_device(ctx);
+        mb::DevBuf P, X, T, G, L;
+        to_device(P, weights, mb::kMlpParams);
+        to_device(X, features, (size_t)n * mb::kFeat);
+        to_device(T, times, (size_t)n * mb::kOut);
+        G.reserve(sizeof(float) * mb::kMlpParams);
+        L.reserve(sizeof(float));
+        mb::mlp_grad(ctx->c, P.as<float>(), X.as<float>(), T.as<float>(), n, G.as<float>(), L.as<float>());
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        MB_CUDA(cudaMemcpy(grad_out, G.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        if (loss_out) MB_CUDA(cudaMemcpy(loss_out, L.p, sizeof(float), cudaMemcpyDefault));
+        P.release(); X.release(); T.release(); G.release(); L.release();
+    });
+}
+
+int mb_scheduler_pick(mb_ctx *ctx, const float *features, int32_t n, int32_t *out) {
+    return guarded(ctx, [&] {
+        if (!ctx || !features || !out || n < 0) mb::fail(MB_ERR_INVALID, "null argument");
+        use_device(ctx);
+        mb::DevBuf X, O;
+        to_device(X, features, (size_t)n * mb::kFeat);
+        O.reserve(sizeof(int32_t) * std::max(n, 1));
+        mb::mlp_pick(ctx->c, X.as<float>(), n, O.as<int32_t>());
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        if (n) MB_CUDA(cudaMemcpy(out, O.p, sizeof(int32_t) * n, cudaMemcpyDefault));
+        X.release();
+        O.release();
+    });
 }
 
 int mb_graph_from_edges(mb_ctx *ctx, int32_t V, int64_t E, const int32_t *src, const int32_t *dst,

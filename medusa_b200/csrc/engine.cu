@@ -16,6 +16,8 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta) {
     p->delta = delta;
     p->tail = ctx.tail ? 1 : 0;
     p->persist = ctx.persist ? 1 : 0;
+    p->replay_then_fixed = ctx.replay_then_fixed ? 1 : 0;
+    p->max_step = ctx.max_step;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));
@@ -58,14 +60,37 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
             MB_CUDA(cudaEventRecord(e0, s));
             sp.prologue(s);
             Ctrl *hc = (Ctrl *)ctx.ctrl_readback();
+            cudaEvent_t t0 = nullptr, t1 = nullptr;
+            if (ctx.tracing) {
+                MB_CUDA(cudaEventCreate(&t0));
+                MB_CUDA(cudaEventCreate(&t1));
+            }
             for (;;) {
                 k_select<<<1, 32, 0, s>>>(fa, sp.app, sp.cap, 0, 0, nbranch, 0);
                 MB_CHECK_LAUNCH();
                 MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
                 MB_CUDA(cudaStreamSynchronize(s));
                 if (hc->done) break;
-                sp.branch(hc->branch, s);
+                if (ctx.tracing) {
+                    // time this superstep alone (its branch, conversion included)
+                    Context::TraceRec r;
+                    r.app = sp.app;
+                    r.step = hc->step;
+                    r.sched = hc->sched;
+                    r.branch = hc->branch;
+                    for (int i = 0; i < 8; i++) r.feat[i] = hc->feat[i];
+                    MB_CUDA(cudaEventRecord(t0, s));
+                    sp.branch(hc->branch, s);
+                    MB_CUDA(cudaEventRecord(t1, s));
+                    MB_CUDA(cudaEventSynchronize(t1));
+                    MB_CUDA(cudaEventElapsedTime(&r.ms, t0, t1));
+                    ctx.trace.push_back(r);
+                } else {
+                    sp.branch(hc->branch, s);
+                }
             }
+            if (t0) cudaEventDestroy(t0);
+            if (t1) cudaEventDestroy(t1);
             if (sp.epilogue) sp.epilogue(s);
             MB_CUDA(cudaEventRecord(e1, s));
         }

@@ -49,6 +49,8 @@ struct RunParams {
     float delta;                // SSSP near-far bucket width (0: plain frontier Bellman-Ford)
     int32_t tail;               // 1: small frontiers run in the persistent single-CTA tail
     int32_t persist;            // 1: schedules 0/4 and splits run in the persistent grid
+    int32_t replay_then_fixed;  // replay policy: past the list use the fixed rule (else repeat)
+    int32_t max_step;           // >= 0: stop after this superstep (trace collection)
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 
@@ -171,6 +173,10 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     }
     c->front_n = n;
     c->front_m = m;
+    if (c->p.max_step >= 0 && c->step > c->p.max_step) {  // trace collection: stop here
+        c->done = 1;
+        return;
+    }
     if (n == 0 || m == 0) {  // nothing left to expand
         if (app == APP_SSSP && ldg2(&c->far_n[c->fcur]) > 0) {
             // near-far: next bucket
@@ -186,7 +192,8 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     switch (c->p.policy) {
         case MB_POLICY_FORCED: s = c->p.forced; break;
         case MB_POLICY_ORACLE_BEST:
-            s = c->step < c->p.nreplay ? c->p.replay[c->step] : c->p.forced;
+            if (c->step < c->p.nreplay) s = c->p.replay[c->step];
+            else s = c->p.replay_then_fixed ? fixed_rule(c, app, V, E, n, m) : c->p.forced;
             break;
         default: s = fixed_rule(c, app, V, E, n, m); break;
     }

@@ -125,6 +125,16 @@ struct Context {
     bool tail = true;              // persistent single-CTA tail for small frontiers
     bool persist = false;          // persistent cooperative grid for schedules 0/4
     bool batching = true;          // several BFS sources: one masked traversal per 64
+    bool replay_then_fixed = false;  // replay policy: fixed rule after the list
+    int32_t max_step = -1;           // >= 0: runs stop after this superstep
+    // superstep trace (host-loop runs): one record per superstep
+    bool tracing = false;
+    struct TraceRec {
+        int32_t app, step, sched, branch;
+        float feat[8];
+        float ms;
+    };
+    std::vector<TraceRec> trace;
     void *ctrl_readback() { return pinned_small + kCtrlOff; }
     void *pinned_reserve(size_t n) {
         if (n <= pinned_bytes && pinned) return pinned;

@@ -1,0 +1,76 @@
+"""FP64 CPU restatement of the learned scheduler's MLP and training loss.
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA training kernels in
+medusa_b200/csrc/learn.cu (k_mlp_grad) and the inference in
+medusa_b200/csrc/sched.cuh (mlp_pick_warp).  No reference counterpart: the
+reference has one fixed schedule.
+
+Layout of the parameter vector (row-major): w1[32][6], b1[32], w2[32][32],
+b2[32], w3[8][32], b3[8].  Loss per sample: cross-entropy between the
+softmax of the outputs and the target q_s ~ exp(-(t_s - t_min)/(0.25 t_min))
+over the measured schedules (t_s > 0); the batch loss and gradient are means.
+"""
+import numpy as np
+
+F, H, O = 6, 32, 8
+TAU = 0.25
+SIZES = [("w1", (H, F)), ("b1", (H,)), ("w2", (H, H)), ("b2", (H,)), ("w3", (O, H)), ("b3", (O,))]
+NUM_PARAMS = sum(int(np.prod(s)) for _, s in SIZES)
+
+
+def unpack(P):
+    out, i = {}, 0
+    for name, shape in SIZES:
+        n = int(np.prod(shape))
+        out[name] = np.asarray(P[i:i + n], np.float64).reshape(shape)
+        i += n
+    return out
+
+
+def pack(d):
+    return np.concatenate([d[name].reshape(-1) for name, _ in SIZES])
+
+
+def targets(T):
+    T = np.asarray(T, np.float64)
+    valid = T > 0
+    tmin = np.where(valid, T, np.inf).min(axis=1, keepdims=True)
+    q = np.where(valid, np.exp(-(T - tmin) / (TAU * tmin)), 0.0)
+    z = q.sum(axis=1, keepdims=True)
+    return np.where(z > 0, q / np.where(z > 0, z, 1), 0.0)
+
+
+def forward(P, X):
+    w = unpack(P)
+    X = np.asarray(X, np.float64)
+    z1 = X @ w["w1"].T + w["b1"]
+    h1 = np.maximum(z1, 0)
+    z2 = h1 @ w["w2"].T + w["b2"]
+    h2 = np.maximum(z2, 0)
+    o = h2 @ w["w3"].T + w["b3"]
+    return z1, h1, z2, h2, o
+
+
+def loss_and_grad(P, X, T):
+    w = unpack(P)
+    X = np.asarray(X, np.float64)
+    n = len(X)
+    z1, h1, z2, h2, o = forward(P, X)
+    o = o - o.max(axis=1, keepdims=True)
+    p = np.exp(o)
+    p /= p.sum(axis=1, keepdims=True)
+    q = targets(T)
+    loss = -(q * np.log(np.maximum(p, 1e-30))).sum() / n
+    do = (p - q) / n
+    g = {"w3": do.T @ h2, "b3": do.sum(0)}
+    dz2 = (do @ w["w3"]) * (z2 > 0)
+    g["w2"] = dz2.T @ h1
+    g["b2"] = dz2.sum(0)
+    dz1 = (dz2 @ w["w2"]) * (z1 > 0)
+    g["w1"] = dz1.T @ X
+    g["b1"] = dz1.sum(0)
+    return loss, pack(g)
+
+
+def pick(P, X):
+    return forward(P, X)[4].argmax(axis=1)
