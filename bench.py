@@ -17,6 +17,16 @@ distances come back device->host inside the timed region.
 `pagerank`: PageRank on the reference's CPU-runnable configuration (uniform,
 2^18 vertices, 2^22 edges, 10 supersteps from 1/N), edges/s per superstep.
 
+`forms`: the same graph, 64 BFS sources (vertices 0..63) and 32 SSSP
+sources (0..31) under four forms -- plain (fixed schedule rule, one loop per
+source), learned (the trained MLP scheduler picks each superstep's
+schedule), batched (64-bit / 32-lane source masks, one traversal per batch)
+and learned+batched -- each form's GTEPS, its ratio to plain, and a check
+that all four return identical levels and distances.  The scheduler is
+trained first, on the GPU, from timing traces of the uniform / R-MAT / grid
+generator families at 2^14, 2^17 and 2^20 vertices with seeds other than
+the workload's.
+
 Multi-GPU (torchrun): the path does not shard (one graph per GPU, as the
 reference's single-GPU path); every rank runs the full workload on its own
 replica, `value` sums all ranks' traversed edges over the max device time.
@@ -41,6 +51,8 @@ SEED = 1
 C2 = dict(scale=20, num_edges=1 << 24, a=0.45, b=0.15, c=0.15, wmin=1, wmax=1000)
 C1 = dict(num_vertices=1 << 18, num_edges=1 << 22)
 PR_ITERS = 10
+TRAIN_SCALES = (14, 17, 20)  # log2 vertices of the scheduler's trace graphs
+TRAIN_ROUNDS = 3  # trace collections: fixed-rule trajectories, then the learned policy's
 METRIC = "BFS/SSSP GTEPS (R-MAT 2^20 V / 2^24 E, source 0)"
 WORKLOAD = ("R-MAT 2^20 vertices, 2^24 edges, (a,b,c,d)=(0.45,0.15,0.15,0.25), seed 1, "
             "weights int [1,1000] as f32; one step = BFS + SSSP from source 0")
@@ -247,6 +259,8 @@ def run_medusa(args):
         "wall_s": round(wall, 3),
         "clocks": clk.summary(),
     }
+    if not args.no_forms:
+        out["forms"] = bench_forms(ctx, api, args, flush, g)
     if not args.no_pagerank:
         out["pagerank"] = bench_pagerank(ctx, api, args, flush)
     g.close()
@@ -258,6 +272,79 @@ def run_medusa(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def bench_forms(ctx, api, args, flush, g):
+    """plain / learned / batched / learned+batched on the workload graph."""
+    import torch
+    from medusa_b200 import scheduler
+    t0 = time.perf_counter()
+    trained = scheduler.train(ctx, seeds=(101, 102), scales=TRAIN_SCALES, rounds=TRAIN_ROUNDS)
+    MODELS = (("bfs", api.MB_MODEL_BFS), ("sssp", api.MB_MODEL_SSSP),
+              ("batched_bfs", api.MB_MODEL_BATCHED))
+    train_s = time.perf_counter() - t0
+    V = g.V
+    bsrc, ssrc = list(range(64)), list(range(32))
+    lv = torch.empty((64, V), dtype=torch.int32, device="cuda")
+    dd = torch.empty((32, V), dtype=torch.float32, device="cuda")
+    forms = {"plain": (api.MB_POLICY_FIXED, False), "learned": (api.MB_POLICY_LEARNED, False),
+             "batched": (api.MB_POLICY_FIXED, True),
+             "learned_batched": (api.MB_POLICY_LEARNED, True)}
+    reps = max(1, min(args.steps, 3))
+    res, ref_out, launches = {}, None, 0
+    for name, (policy, batching) in forms.items():
+        ctx.set_policy(policy)
+        ctx.set_batching(batching)
+        for _ in range(max(1, args.warmup // 3)):
+            g.bfs(bsrc, out=lv)
+            g.sssp(ssrc, out=dd)
+        ms_b = ms_s = 0.0
+        e_b = e_s = 0
+        for _ in range(reps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            _, sb = g.bfs(bsrc, out=lv)
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            _, ss = g.sssp(ssrc, out=dd)
+            ms_b += sb["device_ms"]
+            ms_s += ss["device_ms"]
+            e_b += sb["edges_traversed"]
+            e_s += ss["edges_traversed"]
+            launches += sb["kernel_launches"] + ss["kernel_launches"]
+        outs = (lv.cpu().numpy().copy(), dd.cpu().numpy().view(np.uint32).copy())
+        if ref_out is None:
+            ref_out = outs
+        same = bool(np.array_equal(outs[0], ref_out[0]) and np.array_equal(outs[1], ref_out[1]))
+        res[name] = {"gteps": round((e_b + e_s) / ((ms_b + ms_s) / 1e3) / 1e9, 3),
+                     "bfs_gteps": round(e_b / (ms_b / 1e3) / 1e9, 3),
+                     "sssp_gteps": round(e_s / (ms_s / 1e3) / 1e9, 3),
+                     "bfs_ms": round(ms_b / reps, 3), "sssp_ms": round(ms_s / reps, 3),
+                     "identical_to_plain": same}
+    ctx.set_policy(api.MB_POLICY_FIXED)
+    ctx.set_batching(True)
+    base = res["plain"]["gteps"]
+    for name in res:
+        res[name]["vs_plain"] = round(res[name]["gteps"] / base, 3)
+    res["sources"] = {"bfs": "vertices 0..63", "sssp": "vertices 0..31"}
+    res["scheduler_training"] = {
+        "seconds": round(train_s, 1),
+        "samples": {k: trained[m][1] for k, m in MODELS},
+        "final_loss": {k: round(trained[m][0], 4) for k, m in MODELS},
+        "traces": "uniform / R-MAT / grid families, 2^%s vertices, seeds 101 and 102"
+                  % "/".join(str(x) for x in TRAIN_SCALES)}
+    # per superstep on this graph (source 0): the fixed rule's choice, the
+    # model's choice and the best of all schedules, each choice costed as
+    # that superstep plus the 3 after it under the fixed rule
+    per_step = {}
+    for app, name, model in ((0, "bfs", api.MB_MODEL_BFS), (1, "sssp", api.MB_MODEL_SSSP),
+                             (2, "batched_bfs", api.MB_MODEL_BATCHED)):
+        X, T, F = ctx.scheduler_collect(g, app, 0)
+        r = scheduler.evaluate(ctx, X, T, F, model)
+        per_step[name] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+    res["per_superstep"] = per_step
+    res["gpu_launches"] = launches
+    return res
 
 
 def bench_pagerank(ctx, api, args, flush):
@@ -356,6 +443,8 @@ def main():
     ap.add_argument("--impl", default="medusa", choices=["medusa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pagerank", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the plain / learned / batched / learned+batched comparison")
     ap.add_argument("--hostloop", action="store_true",
                     help="host-driven superstep loop instead of one CUDA graph per loop")
     args = ap.parse_args()

@@ -195,35 +195,53 @@ int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
 /* ---- learned scheduler (no reference counterpart) ------------------------ */
-/* Timing traces for the learned scheduler.  app: 0 BFS, 1 SSSP.  For every
- * superstep of a fixed-rule traversal from `source`, the traversal is replayed
- * with each of the 8 schedules at that superstep (same choices before it) and
- * that superstep is timed alone.  Writes up to max_samples rows of
+/* One model per loop kind: single-source BFS and SSSP (8 schedules each;
+ * the two apps see the same frontier features but rank the schedules
+ * differently) and the batched BFS traversal (push 0 vs pull 4).  Under
+ * MB_POLICY_LEARNED each loop uses its model; a loop whose model is
+ * untrained stays on the fixed rule. */
+#define MB_MODEL_BFS 0
+#define MB_MODEL_BATCHED 1
+#define MB_MODEL_SSSP 2
+/* Timing traces for the learned scheduler.  app: 0 BFS, 1 SSSP, 2 batched
+ * BFS from `source` and the 63 vertices after it (mod V).  For every
+ * superstep of a fixed-rule traversal, the traversal is replayed with each
+ * schedule at that superstep (same choices before it; batched: push and
+ * pull only) and timed over that superstep and the 3 after it (fixed rule
+ * after the choice), since a choice also sets the next frontier's format.  Writes up to max_samples rows of
  * features[6] (the scheduler inputs) and times[8] (ms; -1: not measured) to
- * host arrays, and (nullable) fixed_sched[1] = the schedule the fixed rule
- * chose there; *n_out = rows written. */
+ * host arrays, and (nullable) fixed_sched[1] = the schedule the base run
+ * chose there; *n_out = rows written.  The base run follows the fixed rule,
+ * or the learned policy when that is the context's policy (traces of the
+ * states the trained scheduler itself reaches). */
 int mb_scheduler_collect(mb_ctx *ctx, const mb_graph *g, int32_t app, int32_t source,
                          float *features, float *times, int32_t *fixed_sched,
                          int32_t max_samples, int32_t *n_out);
 /* Train the scheduler MLP (6-32-32-8, FP32) on the GPU: seeded init, `epochs`
  * full-batch Adam steps at learning rate lr, loss = cross-entropy against a
- * softmax of the negated relative times.  Arrays may be host or device.
+ * softmax of the negated relative times, each sample weighted by its best
+ * time.  Arrays may be host or device.
  * *final_loss (nullable) gets the loss after training.  The weights then
  * serve MB_POLICY_LEARNED. */
-int mb_scheduler_train(mb_ctx *ctx, const float *features, const float *times, int32_t n,
-                       int32_t epochs, float lr, uint64_t seed, float *final_loss);
+int mb_scheduler_train(mb_ctx *ctx, int32_t model, const float *features, const float *times,
+                       int32_t n, int32_t epochs, float lr, uint64_t seed, float *final_loss);
 /* Number of MLP parameters (row-major w1[32][6], b1[32], w2[32][32], b2[32],
  * w3[8][32], b3[8]). */
 int32_t mb_scheduler_num_params(void);
-int mb_scheduler_get_weights(mb_ctx *ctx, float *weights);
-int mb_scheduler_set_weights(mb_ctx *ctx, const float *weights);
-/* Mean loss and its gradient (mean over the n samples) for given weights,
+int mb_scheduler_get_weights(mb_ctx *ctx, int32_t model, float *weights);
+int mb_scheduler_set_weights(mb_ctx *ctx, int32_t model, const float *weights);
+/* Loss and its gradient (means over the n samples, each weighted by its
+ * best measured time) for given weights,
  * computed by the training kernels (for checking them against an FP64 CPU
  * implementation). */
 int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features,
                       const float *times, int32_t n, float *grad_out, float *loss_out);
-/* The schedule the current weights pick for each of n feature rows. */
-int mb_scheduler_pick(mb_ctx *ctx, const float *features, int32_t n, int32_t *out);
+/* The schedule the model's weights pick for each of n feature rows (host
+ * arrays).  fallback (nullable, host): the rule a run applies, keep
+ * fallback[i] (the fixed rule's choice) unless the network's best output
+ * beats that schedule's output by more than 1.0. */
+int mb_scheduler_pick(mb_ctx *ctx, int32_t model, const float *features,
+                      const int32_t *fallback, int32_t n, int32_t *out);
 
 /* PageRank that allocates no memory, for callers that cannot call cudaMalloc
  * (a host application that owns all GPU memory through its own pool, or a

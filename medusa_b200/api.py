@@ -20,6 +20,7 @@ MB_ERR_INVALID, MB_ERR_CUDA, MB_ERR_OOM, MB_ERR_TIMEOUT, MB_ERR_UNSUPPORTED = 1,
 MB_ORDER_INPUT, MB_ORDER_REFERENCE = 0, 1
 MB_POLICY_FIXED, MB_POLICY_LEARNED, MB_POLICY_FORCED, MB_POLICY_ORACLE_BEST = 0, 1, 2, 3
 MB_GEN_RMAT, MB_GEN_UNIFORM, MB_GEN_GRID = 0, 1, 2
+MB_MODEL_BFS, MB_MODEL_BATCHED, MB_MODEL_SSSP = 0, 1, 2
 NUM_SCHEDULES = 8
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
@@ -88,13 +89,13 @@ def _load():
         "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank_noalloc": (ctypes.c_int, [P, P, P, I32, I64, I32, F32, P, P]),
         "mb_scheduler_collect": (ctypes.c_int, [P, P, I32, I32, P, P, P, I32, ctypes.POINTER(I32)]),
-        "mb_scheduler_train": (ctypes.c_int, [P, P, P, I32, I32, F32, ctypes.c_uint64,
+        "mb_scheduler_train": (ctypes.c_int, [P, I32, P, P, I32, I32, F32, ctypes.c_uint64,
                                               ctypes.POINTER(F32)]),
         "mb_scheduler_num_params": (I32, []),
-        "mb_scheduler_get_weights": (ctypes.c_int, [P, P]),
-        "mb_scheduler_set_weights": (ctypes.c_int, [P, P]),
+        "mb_scheduler_get_weights": (ctypes.c_int, [P, I32, P]),
+        "mb_scheduler_set_weights": (ctypes.c_int, [P, I32, P]),
         "mb_scheduler_grad": (ctypes.c_int, [P, P, P, P, I32, P, ctypes.POINTER(F32)]),
-        "mb_scheduler_pick": (ctypes.c_int, [P, P, I32, P]),
+        "mb_scheduler_pick": (ctypes.c_int, [P, I32, P, P, I32, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -257,6 +258,7 @@ class Context:
         h = ctypes.c_void_p()
         _check(lib.mb_create(int(device), ctypes.byref(h)))
         self.h = h
+        self.policy = (MB_POLICY_FIXED, 0)
 
     def close(self):
         if self.h:
@@ -271,6 +273,7 @@ class Context:
 
     def set_policy(self, policy, schedule=0):
         _check(lib.mb_set_schedule_policy(self.h, int(policy), int(schedule)), self.h)
+        self.policy = (int(policy), int(schedule))
 
     def set_replay(self, schedules):
         arr = np.ascontiguousarray(schedules, dtype=np.int8)
@@ -288,7 +291,8 @@ class Context:
 
     # ---- learned scheduler ----
     def scheduler_collect(self, g, app, source, max_samples=4096):
-        """Timing traces of one run (app 0 BFS, 1 SSSP): features [n,6],
+        """Timing traces of one run (app 0 BFS, 1 SSSP, 2 batched BFS from
+        `source` and the 63 vertices after it): features [n,6],
         per-schedule superstep times [n,8] (ms, -1 unmeasured) and the
         schedule the fixed rule chose at each superstep [n]."""
         X = np.zeros((max_samples, 6), np.float32)
@@ -301,23 +305,24 @@ class Context:
         k = n.value
         return X[:k].copy(), T[:k].copy(), S[:k].copy()
 
-    def scheduler_train(self, X, T, epochs=1500, lr=3e-3, seed=1):
+    def scheduler_train(self, X, T, epochs=1500, lr=3e-3, seed=1, model=MB_MODEL_BFS):
         X = np.ascontiguousarray(X, np.float32)
         T = np.ascontiguousarray(T, np.float32)
         loss = ctypes.c_float(0)
-        _check(lib.mb_scheduler_train(self.h, X.ctypes.data, T.ctypes.data, len(X), int(epochs),
-                                      float(lr), int(seed), ctypes.byref(loss)), self.h)
+        _check(lib.mb_scheduler_train(self.h, int(model), X.ctypes.data, T.ctypes.data, len(X),
+                                      int(epochs), float(lr), int(seed), ctypes.byref(loss)),
+               self.h)
         return loss.value
 
-    def scheduler_weights(self):
+    def scheduler_weights(self, model=MB_MODEL_BFS):
         w = np.zeros(lib.mb_scheduler_num_params(), np.float32)
-        _check(lib.mb_scheduler_get_weights(self.h, w.ctypes.data), self.h)
+        _check(lib.mb_scheduler_get_weights(self.h, int(model), w.ctypes.data), self.h)
         return w
 
-    def scheduler_set_weights(self, w):
+    def scheduler_set_weights(self, w, model=MB_MODEL_BFS):
         w = np.ascontiguousarray(w, np.float32)
         assert len(w) == lib.mb_scheduler_num_params()
-        _check(lib.mb_scheduler_set_weights(self.h, w.ctypes.data), self.h)
+        _check(lib.mb_scheduler_set_weights(self.h, int(model), w.ctypes.data), self.h)
 
     def scheduler_grad(self, w, X, T):
         w = np.ascontiguousarray(w, np.float32)
@@ -329,10 +334,18 @@ class Context:
                                      g.ctypes.data, ctypes.byref(loss)), self.h)
         return g, loss.value
 
-    def scheduler_pick(self, X):
+    def scheduler_pick(self, X, model=MB_MODEL_BFS, fallback=None):
+        """The model's choice per feature row; with `fallback` (the fixed
+        rule's choices), the in-run rule that overrides them only by a margin."""
         X = np.ascontiguousarray(X, np.float32)
         out = np.zeros(len(X), np.int32)
-        _check(lib.mb_scheduler_pick(self.h, X.ctypes.data, len(X), out.ctypes.data), self.h)
+        fb = None
+        if fallback is not None:
+            fb = np.ascontiguousarray(fallback, np.int32)
+            assert len(fb) == len(X)
+        _check(lib.mb_scheduler_pick(self.h, int(model), X.ctypes.data,
+                                     fb.ctypes.data if fb is not None else None, len(X),
+                                     out.ctypes.data), self.h)
         return out
 
     def set_batching(self, enable):

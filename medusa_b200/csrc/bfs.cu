@@ -544,7 +544,7 @@ __global__ void k_bfs_init(BfsArgs a) {
 void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats) {
     st.ensure(g);
     BfsArgs a;
-    a.f = st.frontier_args(g, ctx.mlp_ready ? ctx.mlp.as<float>() : nullptr);
+    a.f = st.frontier_args(g, ctx.model(MB_MODEL_BFS));
     a.row = g.row.as<int32_t>();
     a.col = g.col.as<int32_t>();
     a.esrc = g.esrc.as<int32_t>();

@@ -108,8 +108,10 @@ int mb_create(int device, mb_ctx **out) {
         ctx->c.num_sms = prop.multiProcessorCount;
         MB_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         MB_CUDA(cudaMallocHost((void **)&ctx->c.pinned_small, mb::Context::kSmallBytes));
-        ctx->c.mlp.reserve(sizeof(float) * mb::kMlpParams);
-        MB_CUDA(cudaMemset(ctx->c.mlp.p, 0, sizeof(float) * mb::kMlpParams));
+        for (mb::DevBuf &b : ctx->c.mlp) {
+            b.reserve(sizeof(float) * mb::kMlpParams);
+            MB_CUDA(cudaMemset(b.p, 0, sizeof(float) * mb::kMlpParams));
+        }
     });
     if (rc != MB_OK) {
         t_last_error = ctx->c.last_error;
@@ -125,7 +127,7 @@ int mb_destroy(mb_ctx *ctx) {
     cudaSetDevice(ctx->c.device);
     if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
     for (auto &b : ctx->c.scratch) b.release();
-    ctx->c.mlp.release();
+    for (mb::DevBuf &b : ctx->c.mlp) b.release();
     if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
     if (ctx->c.pinned_small) cudaFreeHost(ctx->c.pinned_small);
     if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
@@ -143,7 +145,8 @@ int mb_set_schedule_policy(mb_ctx *ctx, int policy, int schedule) {
         return set_error(ctx, MB_ERR_INVALID, "unknown policy");
     if (policy == MB_POLICY_FORCED && (schedule < 0 || schedule >= MB_NUM_SCHEDULES))
         return set_error(ctx, MB_ERR_INVALID, "schedule id out of range");
-    if (policy == MB_POLICY_LEARNED && !ctx->c.mlp_ready)
+    if (policy == MB_POLICY_LEARNED && !ctx->c.mlp_ready[MB_MODEL_BFS] &&
+        !ctx->c.mlp_ready[MB_MODEL_BATCHED] && !ctx->c.mlp_ready[MB_MODEL_SSSP])
         return set_error(ctx, MB_ERR_INVALID, "the learned scheduler has no weights yet");
     ctx->c.schedule_policy = policy;
     ctx->c.fixed_schedule = schedule;
@@ -195,6 +198,12 @@ int mb_set_graph_capture(mb_ctx *ctx, int enable) {
 }
 
 namespace {
+// weights of scheduler model m (MB_MODEL_BFS / MB_MODEL_BATCHED / MB_MODEL_SSSP)
+mb::DevBuf &model_weights(mb_ctx *ctx, int32_t m) {
+    if (m < 0 || m >= mb::Context::kModels) mb::fail(MB_ERR_INVALID, "unknown scheduler model");
+    return ctx->c.mlp[m];
+}
+bool &model_ready(mb_ctx *ctx, int32_t m) { return ctx->c.mlp_ready[m]; }
 // n*k floats from host or device memory into a temporary device buffer
 void to_device(mb::DevBuf &b, const float *p, size_t count) {
     b.reserve(sizeof(float) * std::max<size_t>(count, 1));
@@ -207,28 +216,32 @@ int mb_scheduler_collect(mb_ctx *ctx, const mb_graph *gc, int32_t app, int32_t s
                          int32_t max_samples, int32_t *n_out) {
     return guarded(ctx, [&] {
         check_graph(ctx, gc);
-        if (app != 0 && app != 1) mb::fail(MB_ERR_INVALID, "app must be 0 (BFS) or 1 (SSSP)");
+        if (app < 0 || app > 2)
+            mb::fail(MB_ERR_INVALID, "app must be 0 (BFS), 1 (SSSP) or 2 (batched BFS)");
         if (!features || !times || !n_out || max_samples < 0) mb::fail(MB_ERR_INVALID, "bad output");
         if (source < 0 || source >= gc->g.V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
         use_device(ctx);
         mb_graph *g = const_cast<mb_graph *>(gc);
-        *n_out = mb::collect_traces(ctx->c, g->g, apps(g).bfs, apps(g).sssp,
-                                    app == 0 ? mb::APP_BFS : mb::APP_SSSP, source, features, times,
-                                    fixed_sched, max_samples);
+        const int a = app == 0 ? mb::APP_BFS : app == 1 ? mb::APP_SSSP : mb::APP_MSBFS;
+        *n_out = mb::collect_traces(ctx->c, g->g, apps(g).bfs, apps(g).sssp, apps(g).msbfs, a,
+                                    source, features, times, fixed_sched, max_samples);
     });
 }
 
-int mb_scheduler_train(mb_ctx *ctx, const float *features, const float *times, int32_t n,
-                       int32_t epochs, float lr, uint64_t seed, float *final_loss) {
+int mb_scheduler_train(mb_ctx *ctx, int32_t model, const float *features, const float *times,
+                       int32_t n, int32_t epochs, float lr, uint64_t seed, float *final_loss) {
     return guarded(ctx, [&] {
         if (!ctx) mb::fail(MB_ERR_INVALID, "null context");
+        mb::DevBuf &W = model_weights(ctx, model);
         if (n < 1 || !features || !times || epochs < 0 || !(lr > 0.f))
             mb::fail(MB_ERR_INVALID, "bad training arguments");
         use_device(ctx);
         mb::DevBuf X, T;
         to_device(X, features, (size_t)n * mb::kFeat);
         to_device(T, times, (size_t)n * mb::kOut);
-        const float loss = mb::mlp_train(ctx->c, X.as<float>(), T.as<float>(), n, epochs, lr, seed);
+        const float loss =
+            mb::mlp_train(ctx->c, W.as<float>(), X.as<float>(), T.as<float>(), n, epochs, lr, seed);
+        model_ready(ctx, model) = true;
         if (final_loss) *final_loss = loss;
         X.release();
         T.release();
@@ -237,20 +250,22 @@ int mb_scheduler_train(mb_ctx *ctx, const float *features, const float *times, i
 
 int32_t mb_scheduler_num_params(void) { return mb::kMlpParams; }
 
-int mb_scheduler_get_weights(mb_ctx *ctx, float *w) {
+int mb_scheduler_get_weights(mb_ctx *ctx, int32_t model, float *w) {
     return guarded(ctx, [&] {
         if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
-        MB_CUDA(cudaMemcpy(w, ctx->c.mlp.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        mb::DevBuf &W = model_weights(ctx, model);
+        MB_CUDA(cudaMemcpy(w, W.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
     });
 }
 
-int mb_scheduler_set_weights(mb_ctx *ctx, const float *w) {
+int mb_scheduler_set_weights(mb_ctx *ctx, int32_t model, const float *w) {
     return guarded(ctx, [&] {
         if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
-        MB_CUDA(cudaMemcpy(ctx->c.mlp.p, w, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
-        ctx->c.mlp_ready = true;
+        mb::DevBuf &W = model_weights(ctx, model);
+        MB_CUDA(cudaMemcpy(W.p, w, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        model_ready(ctx, model) = true;
     });
 }
 
@@ -265,7 +280,7 @@ int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features, 
         to_device(X, features, (size_t)n * mb::kFeat);
         to_device(T, times, (size_t)n * mb::kOut);
         G.reserve(sizeof(float) * mb::kMlpParams);
-        L.reserve(sizeof(float));
+        L.reserve(2 * sizeof(float));
         mb::mlp_grad(ctx->c, P.as<float>(), X.as<float>(), T.as<float>(), n, G.as<float>(), L.as<float>());
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         MB_CUDA(cudaMemcpy(grad_out, G.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
@@ -274,18 +289,29 @@ int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features, 
     });
 }
 
-int mb_scheduler_pick(mb_ctx *ctx, const float *features, int32_t n, int32_t *out) {
+int mb_scheduler_pick(mb_ctx *ctx, int32_t model, const float *features, const int32_t *fallback,
+                      int32_t n, int32_t *out) {
     return guarded(ctx, [&] {
         if (!ctx || !features || !out || n < 0) mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
-        mb::DevBuf X, O;
+        mb::DevBuf &W = model_weights(ctx, model);
+        mb::DevBuf X, O, F;
         to_device(X, features, (size_t)n * mb::kFeat);
         O.reserve(sizeof(int32_t) * std::max(n, 1));
-        mb::mlp_pick(ctx->c, X.as<float>(), n, O.as<int32_t>());
+        if (fallback) {
+            F.reserve(sizeof(int32_t) * std::max(n, 1));
+            for (int32_t i = 0; i < n; i++)
+                if (fallback[i] < 0 || fallback[i] >= MB_NUM_SCHEDULES)
+                    mb::fail(MB_ERR_INVALID, "fallback schedule out of range");
+            if (n) MB_CUDA(cudaMemcpy(F.p, fallback, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+        }
+        mb::mlp_pick(ctx->c, W.as<float>(), X.as<float>(), fallback ? F.as<int32_t>() : nullptr, n,
+                     O.as<int32_t>());
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         if (n) MB_CUDA(cudaMemcpy(out, O.p, sizeof(int32_t) * n, cudaMemcpyDefault));
         X.release();
         O.release();
+        F.release();
     });
 }
 

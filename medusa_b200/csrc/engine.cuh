@@ -13,6 +13,7 @@
 #include <cstddef>
 #include "frontier.cuh"
 #include "loopgraph.cuh"
+#include "runparams.cuh"
 #include "sched.cuh"
 
 namespace mb {
@@ -20,8 +21,6 @@ namespace mb {
 constexpr int FMT_QUEUE = 0, FMT_BITMAP = 1, FMT_NONE = 2;
 constexpr int ERR_STEP_CAP = 1;
 constexpr int ERR_BARRIER = 2;     // a grid barrier of the persistent kernel gave up
-constexpr int kMaxReplay = 4096;
-constexpr int APP_BFS = 0, APP_SSSP = 1;
 // Internal step of near-far SSSP (not a user schedule): raise the distance
 // threshold and move far-pile vertices below it into the near queue.
 constexpr int kSchedSplit = MB_NUM_SCHEDULES;
@@ -37,22 +36,6 @@ constexpr int kBranchPersist = kBranchTail + 1;
 constexpr int kNumBranches = kBranchPersist + 1;
 constexpr int kTailThreads = 1024;
 constexpr uint32_t kTailEntries = 2048, kTailEdges = 16384;
-
-// Per-run parameters, written by the host before each run (one small copy),
-// so an instantiated loop graph serves every source and policy.
-struct RunParams {
-    int32_t source;
-    int32_t policy;
-    int32_t forced;
-    int32_t nreplay;
-    uint32_t launches;          // kernels launched by this run (device-counted)
-    float delta;                // SSSP near-far bucket width (0: plain frontier Bellman-Ford)
-    int32_t tail;               // 1: small frontiers run in the persistent single-CTA tail
-    int32_t persist;            // 1: schedules 0/4 and splits run in the persistent grid
-    int32_t replay_then_fixed;  // replay policy: past the list use the fixed rule (else repeat)
-    int32_t max_step;           // >= 0: stop after this superstep (trace collection)
-    int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
-};
 
 // Device-resident control block of one run.
 struct Ctrl {
@@ -118,11 +101,6 @@ __host__ __device__ inline int branch_of(int s, int mode) {
     const int in = sched_input(s);
     return s + ((in != FMT_NONE && in != mode) ? MB_NUM_SCHEDULES : 0);
 }
-
-// Loads that bypass L1: counters other threads update with atomics (at L2)
-// are read this way by code that may run inside the same kernel.
-template <class T>
-__device__ __forceinline__ T ldg2(const T *p) { return __ldcg(p); }
 
 // The branch that runs schedule s from the current frontier: the persistent
 // tail for a small queue frontier under schedule 0.
@@ -326,18 +304,21 @@ __device__ __forceinline__ uint32_t tail_mask(int64_t w, int32_t V) {
 // MLP on the features it left.
 __device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
     Ctrl *c = a.ctrl;
+    const bool use_mlp = a.mlp && c->p.policy == MB_POLICY_LEARNED;  // warp-uniform
+    MlpRegs r;
+    if (use_mlp) mlp_load_warp(a.mlp, r);  // in flight during the bookkeeping
     if ((threadIdx.x & 31) == 0 && c->pending) {
         c->pending = 0;
         finish_superstep(c, app, a.V, a.E, sched_output(c->sched));
     }
     __syncwarp();
-    const bool learned = c->p.policy == MB_POLICY_LEARNED && !c->done && a.mlp &&
-                         c->sched != kSchedSplit;
+    const bool learned = use_mlp && !c->done && c->sched != kSchedSplit;
     if (learned) {  // warp-uniform
         float f[kFeat];
 #pragma unroll
         for (int i = 0; i < kFeat; i++) f[i] = c->feat[i];
-        const int s = mlp_pick_warp(a.mlp, f, 0xffu);
+        // c->sched holds the fixed rule's choice (choose_next)
+        const int s = mlp_decide_warp(r, f, 0xffu, c->sched, kOverrideMargin);
         if ((threadIdx.x & 31) == 0) {
             c->sched = s;
             c->branch = route(c, s);
@@ -564,9 +545,6 @@ struct FrontierState {
     }
 };
 
-// Write this run's RunParams (policy, forced schedule, replay list, source,
-// SSSP bucket width) to the control block (RunParams is its first member).
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f);
 
 // Run a loop (graph mode or host-driven mode) and time it; fills the common
 // part of stats from the control block.

@@ -17,6 +17,12 @@
 
 namespace mb {
 
+// Loads that bypass L1: counters other threads update with atomics (at L2)
+// are read this way by code that may run inside the same kernel.
+template <class T>
+__device__ __forceinline__ T ldg2(const T *p) { return __ldcg(p); }
+
+
 constexpr int kTile = 1024;          // edges per merge-path tile
 constexpr int kPushThreads = 256;    // threads per push CTA
 constexpr int kTileItems = kTile / kPushThreads;

@@ -111,8 +111,13 @@ struct Context {
     std::string last_error;
     // scratch buffers, grown on demand
     DevBuf scratch[8];
-    DevBuf mlp;   // learned-scheduler weights (kMlpParams floats)
-    bool mlp_ready = false;
+    // learned-scheduler weights (kMlpParams floats each), one model per loop
+    // kind: MB_MODEL_BFS, MB_MODEL_BATCHED (batched BFS: push vs pull),
+    // MB_MODEL_SSSP.  An untrained model leaves its loops on the fixed rule.
+    static constexpr int kModels = 3;
+    DevBuf mlp[kModels];
+    bool mlp_ready[kModels] = {false, false, false};
+    const float *model(int m) const { return mlp_ready[m] ? mlp[m].as<float>() : nullptr; }
     void *pinned = nullptr;        // staging for caller host buffers (grown)
     size_t pinned_bytes = 0;
     char *pinned_small = nullptr;  // fixed 64 KiB: run parameters + control readback

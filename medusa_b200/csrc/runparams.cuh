@@ -1,0 +1,31 @@
+// runparams.cuh -- per-run scheduling parameters shared by every BSP loop
+// (single-source engine and batched traversals): written by the host into
+// the first bytes of a run's device control block before the run.
+#pragma once
+#include "mb_internal.cuh"
+
+namespace mb {
+
+constexpr int kMaxReplay = 4096;
+// Apps of a run (trace records, scheduler features).
+constexpr int APP_BFS = 0, APP_SSSP = 1, APP_MSBFS = 2;
+
+struct RunParams {
+    int32_t source;
+    int32_t policy;
+    int32_t forced;
+    int32_t nreplay;
+    uint32_t launches;          // kernels launched by this run (device-counted)
+    float delta;                // SSSP near-far bucket width (0: plain frontier Bellman-Ford)
+    int32_t tail;               // 1: small frontiers run in the persistent single-CTA tail
+    int32_t persist;            // 1: schedules 0/4 and splits run in the persistent grid
+    int32_t replay_then_fixed;  // replay policy: past the list use the fixed rule (else repeat)
+    int32_t max_step;           // >= 0: stop after this superstep (trace collection)
+    int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
+};
+
+// Write this run's RunParams (policy, forced schedule, replay list, source,
+// SSSP bucket width) to a control block whose first member is RunParams.
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f);
+
+}  // namespace mb

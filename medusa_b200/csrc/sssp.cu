@@ -698,7 +698,7 @@ float sssp_default_delta(const Graph &g) {
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats) {
     st.ensure(g);
     SsspArgs a;
-    a.f = st.frontier_args(g, ctx.mlp_ready ? ctx.mlp.as<float>() : nullptr);
+    a.f = st.frontier_args(g, ctx.model(MB_MODEL_SSSP));
     a.row = g.row.as<int32_t>();
     a.col = g.col.as<int32_t>();
     a.rrow = g.rrow.as<int32_t>();

@@ -8,7 +8,11 @@ reference has one fixed schedule.
 Layout of the parameter vector (row-major): w1[32][6], b1[32], w2[32][32],
 b2[32], w3[8][32], b3[8].  Loss per sample: cross-entropy between the
 softmax of the outputs and the target q_s ~ exp(-(t_s - t_min)/(0.25 t_min))
-over the measured schedules (t_s > 0); the batch loss and gradient are means.
+over the measured schedules (t_s > 0); the batch loss and gradient are
+means weighted by each sample's best time, w_i = t_min,i / sum_j t_min,j.
+Features (sched.cuh make_features): log2(1+count)/32 for frontier vertices,
+frontier out-edges, unvisited vertices and unvisited out-edges; degree skew
+log2(max/mean out-degree)/16 (capped at 1); frontier format 0/1.
 """
 import numpy as np
 
@@ -40,6 +44,19 @@ def targets(T):
     return np.where(z > 0, q / np.where(z > 0, z, 1), 0.0)
 
 
+def features(n, m, nu, mu, skew, mode):
+    f = np.log2(1.0 + np.array([n, m, max(nu, 0), max(mu, 0)], np.float64)) / 32
+    return np.concatenate([f, [min(skew, 16.0) / 16.0, float(mode)]])
+
+
+def weights(T):
+    T = np.asarray(T, np.float64)
+    tmin = np.where(T > 0, T, np.inf).min(axis=1)
+    w = np.where(np.isfinite(tmin), tmin, 0.0)
+    s = w.sum()
+    return w / s if s > 0 else w
+
+
 def forward(P, X):
     w = unpack(P)
     X = np.asarray(X, np.float64)
@@ -54,14 +71,14 @@ def forward(P, X):
 def loss_and_grad(P, X, T):
     w = unpack(P)
     X = np.asarray(X, np.float64)
-    n = len(X)
     z1, h1, z2, h2, o = forward(P, X)
     o = o - o.max(axis=1, keepdims=True)
     p = np.exp(o)
     p /= p.sum(axis=1, keepdims=True)
     q = targets(T)
-    loss = -(q * np.log(np.maximum(p, 1e-30))).sum() / n
-    do = (p - q) / n
+    sw = weights(T)[:, None]
+    loss = -(sw * q * np.log(np.maximum(p, 1e-30))).sum()
+    do = (p - q) * sw
     g = {"w3": do.T @ h2, "b3": do.sum(0)}
     dz2 = (do @ w["w3"]) * (z2 > 0)
     g["w2"] = dz2.T @ h1
@@ -72,5 +89,16 @@ def loss_and_grad(P, X, T):
     return loss, pack(g)
 
 
-def pick(P, X):
-    return forward(P, X)[4].argmax(axis=1)
+OVERRIDE_MARGIN = 1.0
+
+
+def pick(P, X, fallback=None):
+    """argmax of the outputs; with fallback, keep fallback[i] unless the
+    best output beats its output by more than OVERRIDE_MARGIN."""
+    o = forward(P, X)[4]
+    best = o.argmax(axis=1)
+    if fallback is None:
+        return best
+    fb = np.asarray(fallback)
+    idx = np.arange(len(o))
+    return np.where(o[idx, best] - o[idx, fb] > OVERRIDE_MARGIN, best, fb)

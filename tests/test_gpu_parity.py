@@ -270,9 +270,12 @@ def test_full_size_pagerank_c1_against_oracle(gpu_ctx, api):
     g.close()
 
 
+@pytest.mark.parametrize("direction", [None, 0, 4], ids=["fixed", "push", "pull"])
 @pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "tiny", "empty"])
-def test_batched_bfs_equals_single_source_runs(gpu_ctx, api, name):
-    """64-bit-mask batched BFS: levels of every source equal the oracle's."""
+def test_batched_bfs_equals_single_source_runs(ctx, api, name, direction):
+    """64-bit-mask batched BFS (fixed rule, all-push, all-pull; CUDA graph
+    and host loop): levels of every source equal the oracle's."""
+    gpu_ctx = ctx
     c = load_golden(name)
     g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
     rng = np.random.default_rng(3)
@@ -280,7 +283,14 @@ def test_batched_bfs_equals_single_source_runs(gpu_ctx, api, name):
     srcs[:len(c["sources"])] = list(c["sources"])
     if len(srcs) > 2:
         srcs[2] = srcs[1]  # a repeated source
+    if direction is not None:
+        gpu_ctx.set_policy(api.MB_POLICY_FORCED, direction)
     lv, st = g.bfs(srcs)
+    gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    if direction == 0:
+        assert st["schedule_count"][4] == 0
+    elif direction == 4:
+        assert st["schedule_count"][0] == 0
     aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
     outdeg = aa.out_degree()
     er = 0
