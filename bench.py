@@ -17,6 +17,12 @@ distances come back device->host inside the timed region.
 `pagerank`: PageRank on the reference's CPU-runnable configuration (uniform,
 2^18 vertices, 2^22 edges, 10 supersteps from 1/N), edges/s per superstep.
 
+`configs`: C3 (1448x1448 road-like grid, BFS + SSSP from the corner), C4a
+(64 BFS + 32 SSSP sources on R-MAT 2^22/2^26, batched vs one loop per
+source, identical outputs) and C5 (R-MAT 2^24/2^28, (0.57,0.19,0.19,0.05):
+BFS, SSSP and 20 PageRank supersteps, fixed vs learned schedule with HBM
+roofline fractions, plus per-superstep fixed / learned / oracle-best costs).
+
 `forms`: the same graph, 64 BFS sources (vertices 0..63) and 32 SSSP
 sources (0..31) under four forms -- plain (fixed schedule rule, one loop per
 source), learned (the trained MLP scheduler picks each superstep's
@@ -264,6 +270,8 @@ def run_medusa(args):
     if not args.no_pagerank:
         out["pagerank"] = bench_pagerank(ctx, api, args, flush)
     g.close()
+    if not args.no_configs and not args.no_forms:  # C5's learned arm needs the trained models
+        out["configs"] = bench_configs(ctx, api, args, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(api, args)
     ctx.close()
@@ -345,6 +353,119 @@ def bench_forms(ctx, api, args, flush, g):
     res["per_superstep"] = per_step
     res["gpu_launches"] = launches
     return res
+
+
+def _timed(fn, reps, flush):
+    """Median device ms (library stats) of fn() over reps runs, L2 flushed before each."""
+    import torch
+    ms, st = [], None
+    for _ in range(reps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        st = fn()
+        ms.append(st["device_ms"])
+    return float(np.median(ms)), st
+
+
+def _trav(st, ms, nbytes, pk):
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"gteps": round(st["edges_traversed"] / (ms / 1e3) / 1e9, 3), "ms": round(ms, 4),
+            "supersteps": st["supersteps"], "edges_traversed": st["edges_traversed"],
+            "schedule_count": st["schedule_count"],
+            "roofline": {"achieved_gbs": round(ach, 1), "frac": round(ach / pk, 4)}}
+
+
+def bench_configs(ctx, api, args, flush):
+    """The other configurations: C3 road-like grid, C4a batched sources on a
+    2^22-vertex R-MAT, C5 2^24-vertex R-MAT at scale (fixed vs learned)."""
+    import torch
+    from medusa_b200 import scheduler
+    pk, _ = peaks()
+    reps = max(1, min(args.steps, 3))
+    out = {}
+    # C3: 1448x1448 grid, 10% of the edges dropped, 0.5% shortcuts, weights [1,100]
+    g = ctx.generate(api.grid_params(1448, 1448, 0.1, 0.005, seed=SEED, wmin=1, wmax=100))
+    V = g.V
+    lv = torch.empty(V, dtype=torch.int32, device="cuda")
+    dd = torch.empty(V, dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        g.bfs([0], out=lv)
+        g.sssp([0], out=dd)
+    mb, sb = _timed(lambda: g.bfs([0], out=lv)[1], reps, flush)
+    ms_, ss = _timed(lambda: g.sssp([0], out=dd)[1], reps, flush)
+    out["c3_grid"] = {"workload": "grid 1448x1448, 10% edges dropped, 0.5% shortcuts, weights "
+                                  "int [1,100], seed 1, source 0 (corner)",
+                      "vertices": V, "edges": g.E,
+                      "bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
+                      "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk)}
+    g.close()
+    del lv, dd
+    # C4a: 64 BFS + 32 SSSP sources on R-MAT 2^22 / 2^26, batched vs one loop per source
+    g = ctx.generate(api.rmat_params(22, 1 << 26, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000))
+    V = g.V
+    lv = torch.empty((64, V), dtype=torch.int32, device="cuda")
+    dd = torch.empty((32, V), dtype=torch.float32, device="cuda")
+    c4 = {"workload": "R-MAT 2^22 vertices, 2^26 edges, (0.45,0.15,0.15,0.25), seed 1; "
+                      "BFS sources 0..63, SSSP sources 0..31", "vertices": V, "edges": g.E}
+    outs = {}
+    for name, batching in (("plain", False), ("batched", True)):
+        ctx.set_batching(batching)
+        g.bfs(list(range(64)), out=lv)
+        g.sssp(list(range(32)), out=dd)
+        mb, sb = _timed(lambda: g.bfs(list(range(64)), out=lv)[1], 1, flush)
+        ms_, ss = _timed(lambda: g.sssp(list(range(32)), out=dd)[1], 1, flush)
+        outs[name] = (lv.cpu().numpy().copy(), dd.cpu().numpy().view(np.uint32).copy())
+        c4[name] = {"bfs_gteps": round(sb["edges_traversed"] / (mb / 1e3) / 1e9, 3),
+                    "sssp_gteps": round(ss["edges_traversed"] / (ms_ / 1e3) / 1e9, 3),
+                    "gteps": round((sb["edges_traversed"] + ss["edges_traversed"])
+                                   / ((mb + ms_) / 1e3) / 1e9, 3),
+                    "bfs_ms": round(mb, 3), "sssp_ms": round(ms_, 3)}
+    ctx.set_batching(True)
+    c4["batched"]["vs_plain"] = round(c4["batched"]["gteps"] / c4["plain"]["gteps"], 3)
+    c4["identical"] = bool(np.array_equal(outs["plain"][0], outs["batched"][0]) and
+                           np.array_equal(outs["plain"][1], outs["batched"][1]))
+    out["c4a_batched"] = c4
+    g.close()
+    del lv, dd, outs
+    # C5: R-MAT 2^24 / 2^28, (0.57,0.19,0.19,0.05), weights [1,1000]; fixed vs learned
+    g = ctx.generate(api.rmat_params(24, 1 << 28, 0.57, 0.19, 0.19, seed=SEED, wmin=1, wmax=1000))
+    V, E = g.V, g.E
+    lv = torch.empty(V, dtype=torch.int32, device="cuda")
+    dd = torch.empty(V, dtype=torch.float32, device="cuda")
+    rk = torch.empty(V, dtype=torch.float32, device="cuda")
+    c5 = {"workload": "R-MAT 2^24 vertices, 2^28 edges, (0.57,0.19,0.19,0.05), seed 1, weights "
+                      "int [1,1000]; BFS and SSSP from 0, PageRank 20 supersteps from 1/N",
+          "vertices": V, "edges": E}
+    res = {}
+    for name, policy in (("fixed", api.MB_POLICY_FIXED), ("learned", api.MB_POLICY_LEARNED)):
+        ctx.set_policy(policy)
+        g.bfs([0], out=lv)
+        g.sssp([0], out=dd)
+        mb, sb = _timed(lambda: g.bfs([0], out=lv)[1], reps, flush)
+        ms_, ss = _timed(lambda: g.sssp([0], out=dd)[1], reps, flush)
+        res[name] = (lv.cpu().numpy().copy(), dd.cpu().numpy().view(np.uint32).copy())
+        c5[name] = {"bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
+                    "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk)}
+    ctx.set_policy(api.MB_POLICY_FIXED)
+    c5["learned_identical"] = bool(np.array_equal(res["fixed"][0], res["learned"][0]) and
+                                   np.array_equal(res["fixed"][1], res["learned"][1]))
+    per_step = {}
+    for app, name, model in ((0, "bfs", api.MB_MODEL_BFS), (1, "sssp", api.MB_MODEL_SSSP)):
+        X, T, F = ctx.scheduler_collect(g, app, 0, max_samples=32)
+        r = scheduler.evaluate(ctx, X, T, F, model)
+        per_step[name] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+    c5["per_superstep"] = per_step
+    g.pagerank(20, 1.0 / V, out=rk)
+    mp, sp = _timed(lambda: g.pagerank(20, 1.0 / V, out=rk)[1], reps, flush)
+    per = mp / 20
+    b = 8 * E + 16 * V + 4
+    c5["pagerank"] = {"ms_per_superstep": round(per, 4),
+                      "edges_per_s": round(E / (per / 1e3), 1),
+                      "roofline": {"achieved_gbs": round(b / (per / 1e3) / 1e9, 1),
+                                   "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}}
+    out["c5_scale"] = c5
+    g.close()
+    return out
 
 
 def bench_pagerank(ctx, api, args, flush):
@@ -443,6 +564,8 @@ def main():
     ap.add_argument("--impl", default="medusa", choices=["medusa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pagerank", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the C3 grid, C4a batched and C5 at-scale measurements")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the plain / learned / batched / learned+batched comparison")
     ap.add_argument("--hostloop", action="store_true",

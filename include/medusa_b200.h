@@ -194,6 +194,23 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
+/* ---- tunables (no reference counterpart) --------------------------------- */
+/* Launch and routing parameters that change speed, never results; set by
+ * the autotuner (medusa_b200/autotune.py) or by hand.  value -1 restores
+ * the built-in default. */
+#define MB_TUNE_SSSP_BM_PUSH_MIN 0 /* SSSP: frontier out-edges from which schedule 0
+                                      writes a bitmap compacted afterwards (0: never);
+                                      default max(2^20, E/8) */
+#define MB_TUNE_PUSH_BLOCKS_PER_SM 1 /* CTAs per SM of the edge-balanced push kernels
+                                        (default 8) */
+#define MB_TUNE_VERTEX_BLOCKS_PER_SM 2 /* CTAs per SM of the per-vertex / per-word
+                                          kernels (default 8) */
+#define MB_TUNE_TAIL_EDGES 3 /* frontier out-edges up to which schedule 0 runs in the
+                                persistent single-CTA tail (default 16384, at most 16384) */
+#define MB_NUM_TUNABLES 4
+int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
+int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
+
 /* ---- learned scheduler (no reference counterpart) ------------------------ */
 /* One model per loop kind: single-source BFS and SSSP (8 schedules each;
  * the two apps see the same frontier features but rank the schedules

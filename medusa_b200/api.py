@@ -21,6 +21,10 @@ MB_ORDER_INPUT, MB_ORDER_REFERENCE = 0, 1
 MB_POLICY_FIXED, MB_POLICY_LEARNED, MB_POLICY_FORCED, MB_POLICY_ORACLE_BEST = 0, 1, 2, 3
 MB_GEN_RMAT, MB_GEN_UNIFORM, MB_GEN_GRID = 0, 1, 2
 MB_MODEL_BFS, MB_MODEL_BATCHED, MB_MODEL_SSSP = 0, 1, 2
+MB_TUNE_SSSP_BM_PUSH_MIN, MB_TUNE_PUSH_BLOCKS_PER_SM, MB_TUNE_VERTEX_BLOCKS_PER_SM, \
+    MB_TUNE_TAIL_EDGES = 0, 1, 2, 3
+TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_sm": 2,
+            "tail_edges": 3}
 NUM_SCHEDULES = 8
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
@@ -92,6 +96,8 @@ def _load():
         "mb_scheduler_train": (ctypes.c_int, [P, I32, P, P, I32, I32, F32, ctypes.c_uint64,
                                               ctypes.POINTER(F32)]),
         "mb_scheduler_num_params": (I32, []),
+        "mb_set_tunable": (ctypes.c_int, [P, I32, ctypes.c_int64]),
+        "mb_get_tunable": (ctypes.c_int, [P, I32, ctypes.POINTER(ctypes.c_int64)]),
         "mb_scheduler_get_weights": (ctypes.c_int, [P, I32, P]),
         "mb_scheduler_set_weights": (ctypes.c_int, [P, I32, P]),
         "mb_scheduler_grad": (ctypes.c_int, [P, P, P, P, I32, P, ctypes.POINTER(F32)]),
@@ -347,6 +353,17 @@ class Context:
                                      fb.ctypes.data if fb is not None else None, len(X),
                                      out.ctypes.data), self.h)
         return out
+
+    def set_tunable(self, which, value):
+        """Launch/routing parameter (name from TUNABLES or MB_TUNE_* id); -1: default."""
+        w = TUNABLES[which] if isinstance(which, str) else int(which)
+        _check(lib.mb_set_tunable(self.h, w, int(value)), self.h)
+
+    def get_tunable(self, which):
+        w = TUNABLES[which] if isinstance(which, str) else int(which)
+        v = ctypes.c_int64(0)
+        _check(lib.mb_get_tunable(self.h, w, ctypes.byref(v)), self.h)
+        return v.value
 
     def set_batching(self, enable):
         _check(lib.mb_set_batching(self.h, 1 if enable else 0), self.h)

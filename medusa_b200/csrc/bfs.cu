@@ -554,7 +554,9 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
     a.vis = st.vis.as<uint32_t>();
     upload_params(ctx, st.ctrl.p, source);
 
-    const int grid_push = ctx.num_sms * 8, grid_vtx = ctx.num_sms * 8, grid_edge = ctx.num_sms * 8;
+    const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
+    const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
+    const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
     LoopSpec sp;
     sp.st = &st;
@@ -569,6 +571,8 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
         MB_CHECK_LAUNCH();
     };
     sp.branch = [&](int branch, cudaStream_t s) {
+        // BFS never routes to the bitmap-output push (bm_push_min is 0)
+        if (branch == kBranchPushBm) branch = MB_SCHED_PUSH_EDGE_QUEUE;
         if (branch == kBranchTail) {
             k_tail<<<1, kTailThreads, 0, s>>>(a, sp.cap);
             MB_CHECK_LAUNCH();

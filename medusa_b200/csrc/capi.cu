@@ -197,6 +197,27 @@ int mb_set_graph_capture(mb_ctx *ctx, int enable) {
     return MB_OK;
 }
 
+int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    if (which < 0 || which >= MB_NUM_TUNABLES) return set_error(ctx, MB_ERR_INVALID, "unknown tunable");
+    if (value < -1) return set_error(ctx, MB_ERR_INVALID, "tunable value must be >= -1");
+    if ((which == MB_TUNE_PUSH_BLOCKS_PER_SM || which == MB_TUNE_VERTEX_BLOCKS_PER_SM) &&
+        (value == 0 || value > 32))
+        return set_error(ctx, MB_ERR_INVALID, "blocks per SM must be 1..32");
+    if (which == MB_TUNE_TAIL_EDGES && value > (1 << 24))
+        return set_error(ctx, MB_ERR_INVALID, "tail edges must be <= 2^24");
+    ctx->c.tunable[which] = value;
+    ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
+    return MB_OK;
+}
+
+int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value) {
+    if (!ctx || !value) return set_error(nullptr, MB_ERR_INVALID, "null argument");
+    if (which < 0 || which >= MB_NUM_TUNABLES) return MB_ERR_INVALID;
+    *value = ctx->c.tunable[which];
+    return MB_OK;
+}
+
 namespace {
 // weights of scheduler model m (MB_MODEL_BFS / MB_MODEL_BATCHED / MB_MODEL_SSSP)
 mb::DevBuf &model_weights(mb_ctx *ctx, int32_t m) {

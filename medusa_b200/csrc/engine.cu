@@ -4,7 +4,7 @@
 
 namespace mb {
 
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta) {
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, uint32_t bm_push_min) {
     static_assert(sizeof(RunParams) <= Context::kCtrlOff, "params staging too small");
     static_assert(sizeof(Ctrl) <= Context::kSmallBytes - Context::kCtrlOff, "ctrl readback too small");
     RunParams *p = (RunParams *)(ctx.pinned_small + Context::kParamsOff);
@@ -18,6 +18,9 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta) {
     p->persist = ctx.persist ? 1 : 0;
     p->replay_then_fixed = ctx.replay_then_fixed ? 1 : 0;
     p->max_step = ctx.max_step;
+    p->bm_push_min = bm_push_min;
+    p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0 ? (uint32_t)ctx.tunable[MB_TUNE_TAIL_EDGES]
+                                                        : kTailEdges;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));
@@ -40,7 +43,8 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
     MB_CUDA(cudaEventCreate(&e1));
     try {
         if (ctx.use_graphs) {
-            if (!st.lg.exec || st.owner != (const void *)&ctx || st.owner_mlp != (const void *)fa.mlp) {
+            if (!st.lg.exec || st.owner != (const void *)&ctx || st.owner_mlp != (const void *)fa.mlp ||
+                st.owner_gen != ctx.tune_gen) {
                 const int cap = sp.cap, app = sp.app;
                 build_loop_graph(
                     st.lg, s, nbranch, sp.prologue,
@@ -52,6 +56,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
                     sp.branch, sp.epilogue);
                 st.owner = &ctx;
                 st.owner_mlp = fa.mlp;
+                st.owner_gen = ctx.tune_gen;
             }
             MB_CUDA(cudaEventRecord(e0, s));
             MB_CUDA(cudaGraphLaunch(st.lg.exec, s));

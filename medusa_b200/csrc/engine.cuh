@@ -33,7 +33,11 @@ constexpr int kBranchTail = kBranchSplit + 1;
 // schedules 0 and 4 (with their frontier conversions) and near-far splits,
 // separated by grid barriers, until a superstep needs anything else.
 constexpr int kBranchPersist = kBranchTail + 1;
-constexpr int kNumBranches = kBranchPersist + 1;
+// Schedule 0 of SSSP on a large queue frontier: the relaxations set bits of
+// a next-frontier bitmap with fire-and-forget atomics (no per-vertex claim
+// round trip), and a compaction pass turns the bitmap into the next queue.
+constexpr int kBranchPushBm = kBranchPersist + 1;
+constexpr int kNumBranches = kBranchPushBm + 1;
 constexpr int kTailThreads = 1024;
 constexpr uint32_t kTailEntries = 2048, kTailEdges = 16384;
 
@@ -132,8 +136,11 @@ __host__ __device__ inline bool persist_supported(int s) {
 __device__ inline int route(const Ctrl *c, int s) {
     if (c->p.persist && persist_supported(s)) return kBranchPersist;
     if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.tail &&
-        c->front_n <= kTailEntries && c->front_m <= kTailEdges)
+        c->front_n <= kTailEntries && c->front_m <= c->p.tail_edges)
         return kBranchTail;
+    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.bm_push_min &&
+        c->front_m >= c->p.bm_push_min)
+        return kBranchPushBm;
     return branch_of(s, c->mode);
 }
 
@@ -486,6 +493,7 @@ struct FrontierState {
     int64_t E = 0, W = 0;
     const void *owner = nullptr;      // context the loop graph was built for
     const void *owner_mlp = nullptr;  // scheduler weights it was built with
+    uint64_t owner_gen = ~0ull;       // tunables generation it was built with
     DevBuf bm[2], qv[2], qo[2], tf[2], ctrl;
     LoopGraph lg;
     void release_frontier() {

@@ -13,14 +13,14 @@
 // process exits.  Graphs with more than kNoAllocMaxVertices vertices are
 // rejected.
 //
-// The arithmetic is the same as mb_pagerank's fused pull (pagerank.cu), so
-// the two give identical bits: per vertex, a sequential fold of the in-edge
-// contributions in reverse-CSR order, and for in-degrees above 2048 a
-// sequential fold of the sequential folds of consecutive 2048-edge blocks --
-// here computed by the lane that owns the vertex instead of by a separate
-// block kernel, because the block partial sums would need more scratch.
+// The arithmetic is the same as mb_pagerank's (the order of pr_order.cuh),
+// so the two give identical bits.  Heavier vertices' blocks are summed by
+// the warp that owns the vertex's 32-vertex group, one vertex after the
+// other, instead of by a separate block kernel: the block sums would need
+// more scratch.
 #include <mutex>
 #include "mb_internal.cuh"
+#include "pr_order.cuh"
 
 namespace mb {
 void record_thread_error(const std::string &msg);  // capi.cu
@@ -29,7 +29,6 @@ void record_thread_error(const std::string &msg);  // capi.cu
 namespace {
 
 constexpr int32_t kNoAllocMaxVertices = 1 << 20;  // 2 x 4 MiB of scratch
-constexpr int kNaHubBlock = 2048;
 constexpr int kNaWin = 1024;
 constexpr int kNaWarps = 8;
 constexpr int kMaxDevices = 64;
@@ -52,8 +51,7 @@ __device__ __forceinline__ int32_t na_outdeg(const NaArgs &a, int32_t v) {
 }
 
 __device__ __forceinline__ void na_write(const NaArgs &a, int32_t v, float sum) {
-    const float s = (float)((double)sum * 0.85);  // MPG/UserOperators.h:22-23
-    const float r = (float)(0.15 + (double)s);
+    const float r = mb::pr_update(sum);
     a.rank[v] = r;
     const int32_t d = na_outdeg(a, v);
     a.cout[v] = d > 0 ? r / (float)d : 0.0f;
@@ -73,8 +71,8 @@ __global__ void k_na_fill(float *x, int32_t n, float v) {
         x[i] = v;
 }
 
-// One warp per 32 consecutive vertices, in-edges streamed through a shared
-// window; the owner lane of a vertex above the hub threshold folds it alone.
+// One warp per 32 consecutive vertices, light in-edge lists streamed through
+// a shared window; then the warp sums each heavier vertex's blocks in turn.
 __global__ void __launch_bounds__(kNaWarps * 32) k_na_pull(NaArgs a) {
     __shared__ float win[kNaWarps][kNaWin];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -91,7 +89,7 @@ __global__ void __launch_bounds__(kNaWarps * 32) k_na_pull(NaArgs a) {
             b = a.rrow[v];
             e = a.rrow[v + 1];
         }
-        const bool hub = valid && (e - b) > kNaHubBlock;
+        const bool hub = valid && (e - b) > mb::kPrLight;
         const int64_t g0 = a.rrow[vb], g1 = a.rrow[ve];
         float sum = 0.f;
         for (int64_t w0 = g0; w0 < g1; w0 += kNaWin) {
@@ -109,14 +107,16 @@ __global__ void __launch_bounds__(kNaWarps * 32) k_na_pull(NaArgs a) {
             }
             __syncwarp();
         }
-        if (hub) {
-            sum = 0.f;
-            for (int64_t j0 = b; j0 < e; j0 += kNaHubBlock) {
-                const int64_t j1 = min(e, j0 + kNaHubBlock);
-                float s = 0.f;
-                for (int64_t j = j0; j < j1; j++) s += __ldg(&a.cin[a.rcol[j]]);
-                sum += s;
+        for (unsigned hm = __ballot_sync(0xffffffffu, hub); hm; hm &= hm - 1) {
+            const int owner = __ffs(hm) - 1;
+            const int64_t hb = __shfl_sync(0xffffffffu, b, owner);
+            const int64_t he = __shfl_sync(0xffffffffu, e, owner);
+            float tot = 0.f;
+            for (int64_t j0 = hb; j0 < he; j0 += mb::kPrBlock) {
+                const int64_t j1 = min(he, j0 + (int64_t)mb::kPrBlock);
+                tot += mb::pr_warp_block_sum(j0, j1, [&](int64_t j) { return __ldg(&a.cin[a.rcol[j]]); });
             }
+            if (lane == owner) sum = tot;
         }
         if (valid) na_write(a, v, sum);
     }

@@ -9,25 +9,29 @@
 //           0.15 + sum a double add rounded to float.
 // No dangling-rank redistribution; a vertex with no in-edges gets 0.15.
 //
-// The sum runs in a fixed order, the same for every schedule, so schedules
-// never change a bit of the result:
-//   in-degree <= kHubBlock: a sequential fold over the in-edges in reverse-CSR
-//     order -- the order the reference's msgDstID hands out message slots, so
-//     these vertices match a sequential CPU sum bit for bit;
-//   larger in-degrees ("hubs"): sequential folds over consecutive blocks of
-//     kHubBlock in-edges, then a sequential fold of the block sums.
-// Schedules: 0 fused pull (gather rank/outdeg through shared memory, fold,
-// update, write the next contribution -- one kernel per superstep); 6 the
-// reference's split: send into the E-slot message array at msgDstID, then
-// the same combine+update reading the messages.
+// The sum runs in the fixed order of pr_order.cuh, the same for every
+// schedule, so schedules never change a bit of the result.  Work mapping:
+//   light vertices (in-degree <= kPrLight): one warp per 32 consecutive
+//     vertices streams their in-edges through a shared-memory window
+//     (coalesced) and each lane folds its own vertex;
+//   heavier vertices: their kPrBlock-edge blocks form a work list built once
+//     per graph, one 16-byte item per block (edge range, vertex, slot); one
+//     warp per item (k_heavy_blocks).  A vertex with a single block is
+//     finished there (update and next contribution); a hub's blocks write
+//     block sums that k_hub_finalize folds in order -- so hubs and the long
+//     tail of R-MAT's hundreds-to-thousands in-degrees spread over every SM
+//     instead of serialising in one lane.
+// Schedules: 0 fused pull (gather rank/outdeg, fold, update, write the next
+// contribution); 6 the reference's split: send into the E-slot message
+// array at msgDstID, then the same combine+update reading the messages.
 #include <algorithm>
 #include <vector>
 #include "pagerank.cuh"
+#include "pr_order.cuh"
 
 namespace mb {
 namespace {
 
-constexpr int kHubBlock = 2048;          // in-edges per hub block
 constexpr int kWin = 1024;               // edges staged per warp per window
 constexpr int kPrWarps = 8;              // warps per CTA
 constexpr int kPrThreads = kPrWarps * 32;
@@ -40,18 +44,13 @@ struct PrArgs {
     float *contrib_out;
     float *rank_out;
     float *msg;                // E-slot message array (schedule 6)
-    const int32_t *hub_v;      // hub vertices
-    const int32_t *hub_first;  // first block of each hub (nhub+1 entries)
-    const int32_t *blk_v;      // hub of each block
-    int32_t nhub, nblk;
-    float *blk_sum;            // per-block partial sums
+    const int4 *items;           // heavy blocks: {j0, j1, vertex, hub slot or -1}
+    int32_t nitems;
+    const int32_t *hub_v;        // vertices with more than one block
+    const int32_t *hub_first;    // first slot of each hub (nhub+1 entries)
+    int32_t nhub;
+    float *blk_sum;              // per-slot block sums of the hubs
 };
-
-__device__ __forceinline__ float pr_update(float sum) {
-    // MPG/UserOperators.h:22-23: "msg_sum *= 0.85; set_level(0.15 + msg_sum)"
-    const float s = (float)((double)sum * 0.85);
-    return (float)(0.15 + (double)s);
-}
 
 __device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) {
     const float r = pr_update(sum);
@@ -66,17 +65,28 @@ __device__ __forceinline__ float edge_val(const PrArgs &a, int64_t j) {
     return __ldg(&a.contrib_in[a.rcol[j]]);
 }
 
-// Hub blocks: thread per block, sequential fold of its kHubBlock edges.
+// Heavy-vertex blocks: one warp per work item (a block of <= kPrBlock
+// in-edges).  A single-block vertex is finished here.
 template <bool kFromMsg>
-__global__ void k_hub_blocks(PrArgs a) {
-    for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < a.nblk; b += gridDim.x * blockDim.x) {
-        const int32_t h = a.blk_v[b];
-        const int32_t v = a.hub_v[h];
-        const int64_t j0 = (int64_t)a.rrow[v] + (int64_t)(b - a.hub_first[h]) * kHubBlock;
-        const int64_t j1 = min((int64_t)a.rrow[v + 1], j0 + kHubBlock);
-        float s = 0.f;
-        for (int64_t j = j0; j < j1; j++) s += edge_val<kFromMsg>(a, j);
-        a.blk_sum[b] = s;
+__global__ void __launch_bounds__(256) k_heavy_blocks(PrArgs a) {
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; b < a.nitems; b += warps) {
+        const int4 it = __ldg(&a.items[b]);
+        const float s = pr_warp_block_sum((int64_t)it.x, (int64_t)it.y,
+                                          [&](int64_t j) { return edge_val<kFromMsg>(a, j); });
+        if ((threadIdx.x & 31) == 0) {
+            if (it.w < 0) pr_write(a, it.z, 0.f + s);  // the fold of one block sum from 0
+            else a.blk_sum[it.w] = s;
+        }
+    }
+}
+
+// Hubs (more than one block): fold the block sums in order, then update.
+__global__ void k_hub_finalize(PrArgs a) {
+    for (int32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < a.nhub; h += gridDim.x * blockDim.x) {
+        float sum = 0.f;
+        for (int32_t k = a.hub_first[h]; k < a.hub_first[h + 1]; k++) sum += a.blk_sum[k];
+        pr_write(a, a.hub_v[h], sum);
     }
 }
 
@@ -101,21 +111,24 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
             b = a.rrow[v];
             e = a.rrow[v + 1];
         }
-        const bool hub = valid && (e - b) > kHubBlock;
+        const bool heavy = valid && (e - b) > kPrLight;
         const int64_t g0 = a.rrow[vb], g1 = a.rrow[ve];
         float sum = 0.f;
-        // hub vertices are excluded from the window pass
-        const unsigned hubmask = __ballot_sync(0xffffffffu, hub);
+        // heavy vertices are finished by k_heavy_blocks / k_hub_finalize
         for (int64_t w0 = g0; w0 < g1; w0 += kWin) {
             const int64_t w1 = min(w0 + (int64_t)kWin, g1);
-            // skip windows that lie entirely inside hub ranges
-            const bool mine = !hub && b < w1 && e > w0;
+            // skip windows that lie entirely inside heavy ranges
+            const bool mine = !heavy && b < w1 && e > w0;
             if (!__any_sync(0xffffffffu, mine)) continue;
-#pragma unroll 8
-            for (int k = lane; k < kWin; k += 32) {
-                const int64_t j = w0 + k;
-                if (j < w1) wv[k] = edge_val<kFromMsg>(a, j);
+            // every load of the window in flight at once
+            float vals[kWin / 32];
+#pragma unroll
+            for (int r = 0; r < kWin / 32; r++) {
+                const int64_t j = w0 + lane + 32 * r;
+                vals[r] = j < w1 ? edge_val<kFromMsg>(a, j) : 0.f;
             }
+#pragma unroll
+            for (int r = 0; r < kWin / 32; r++) wv[lane + 32 * r] = vals[r];
             __syncwarp();
             if (mine) {
                 const int64_t lo = max(b, w0), hi = min(e, w1);
@@ -123,18 +136,7 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
             }
             __syncwarp();
         }
-        if (hubmask && hub) {
-            // fold this hub's block sums in order (k_hub_blocks ran before)
-            int32_t h = 0, lo = 0, hi = a.nhub;  // binary search hub id
-            while (lo < hi) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (a.hub_v[mid] < v) lo = mid + 1; else hi = mid;
-            }
-            h = lo;
-            sum = 0.f;
-            for (int32_t k = a.hub_first[h]; k < a.hub_first[h + 1]; k++) sum += a.blk_sum[k];
-        }
-        if (valid) pr_write(a, v, sum);
+        if (valid && !heavy) pr_write(a, v, sum);
     }
 }
 
@@ -173,29 +175,36 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     contrib[0].reserve(sizeof(float) * (size_t)V);
     contrib[1].reserve(sizeof(float) * (size_t)V);
     msg.reserve(sizeof(float) * (size_t)std::max<int64_t>(E, 1));
-    // hub table, built once per graph from the in-degree offsets
+    // heavy-vertex work list, built once per graph from the in-degree offsets:
+    // one item per block; hubs (more than one block) get block-sum slots
     std::vector<int32_t> rrow(V + 1);
     MB_CUDA(cudaMemcpy(rrow.data(), g.rrow.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost));
-    std::vector<int32_t> hv, hf, bv;
+    std::vector<int4> it;
+    std::vector<int32_t> hv, hf;
+    int32_t slots = 0;
     for (int32_t v = 0; v < V; v++) {
         const int64_t d = (int64_t)rrow[v + 1] - rrow[v];
-        if (d > kHubBlock) {
-            hf.push_back((int32_t)bv.size());
-            const int32_t nb = (int32_t)((d + kHubBlock - 1) / kHubBlock);
-            for (int32_t k = 0; k < nb; k++) bv.push_back((int32_t)hv.size());
-            hv.push_back(v);
+        if (d <= kPrLight) continue;
+        if (d <= kPrBlock) {
+            it.push_back(make_int4(rrow[v], rrow[v + 1], v, -1));
+            continue;
         }
+        hv.push_back(v);
+        hf.push_back(slots);
+        for (int64_t j0 = rrow[v]; j0 < rrow[v + 1]; j0 += kPrBlock)
+            it.push_back(make_int4((int32_t)j0, (int32_t)std::min<int64_t>(rrow[v + 1], j0 + kPrBlock),
+                                   v, slots++));
     }
-    hf.push_back((int32_t)bv.size());
+    hf.push_back(slots);
+    nitems = (int32_t)it.size();
     nhub = (int32_t)hv.size();
-    nblk = (int32_t)bv.size();
+    items.reserve(sizeof(int4) * std::max<size_t>(it.size(), 1));
     hub_v.reserve(sizeof(int32_t) * std::max<size_t>(hv.size(), 1));
     hub_first.reserve(sizeof(int32_t) * hf.size());
-    blk_v.reserve(sizeof(int32_t) * std::max<size_t>(bv.size(), 1));
-    blk_sum.reserve(sizeof(float) * std::max<size_t>(bv.size(), 1));
+    blk_sum.reserve(sizeof(float) * std::max<int32_t>(slots, 1));
+    if (nitems) MB_CUDA(cudaMemcpy(items.p, it.data(), sizeof(int4) * it.size(), cudaMemcpyHostToDevice));
     if (nhub) MB_CUDA(cudaMemcpy(hub_v.p, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice));
     MB_CUDA(cudaMemcpy(hub_first.p, hf.data(), 4 * hf.size(), cudaMemcpyHostToDevice));
-    if (nblk) MB_CUDA(cudaMemcpy(blk_v.p, bv.data(), 4 * bv.size(), cudaMemcpyHostToDevice));
     built = true;
     (void)ctx;
 }
@@ -218,15 +227,22 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         a.contrib_out = st.contrib[parity ^ 1].as<float>();
         a.rank_out = st.rank.as<float>();
         a.msg = st.msg.as<float>();
+        a.items = st.items.as<int4>();
+        a.nitems = st.nitems;
         a.hub_v = st.hub_v.as<int32_t>();
         a.hub_first = st.hub_first.as<int32_t>();
-        a.blk_v = st.blk_v.as<int32_t>();
         a.nhub = st.nhub;
-        a.nblk = st.nblk;
         a.blk_sum = st.blk_sum.as<float>();
         return a;
     };
-    const int grid_pull = ctx.num_sms * 8;
+    // grids of exactly the resident blocks (grid-stride loops: no tail wave)
+    auto resident = [&](const void *k, int threads) {
+        int per_sm = 0;
+        MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0));
+        return ctx.num_sms * std::max(per_sm, 1);
+    };
+    const int grid_pull = resident((const void *)k_pr_pull<false>, kPrThreads);
+    const int grid_heavy = resident((const void *)k_heavy_blocks<false>, 256);
     const int grid_vtx = ctx.num_sms * 8;
     auto emit = [&](cudaStream_t cs) {
         k_pr_init<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init, st.contrib[0].as<float>());
@@ -235,12 +251,13 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             PrArgs a = args(it & 1);
             if (unfused) {
                 k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
-                if (a.nblk) k_hub_blocks<true><<<grid_for(a.nblk, 128, 4096), 128, 0, cs>>>(a);
+                if (a.nitems) k_heavy_blocks<true><<<grid_for((int64_t)a.nitems * 32, 256, grid_heavy), 256, 0, cs>>>(a);
                 k_pr_pull<true><<<grid_pull, kPrThreads, 0, cs>>>(a);
             } else {
-                if (a.nblk) k_hub_blocks<false><<<grid_for(a.nblk, 128, 4096), 128, 0, cs>>>(a);
+                if (a.nitems) k_heavy_blocks<false><<<grid_for((int64_t)a.nitems * 32, 256, grid_heavy), 256, 0, cs>>>(a);
                 k_pr_pull<false><<<grid_pull, kPrThreads, 0, cs>>>(a);
             }
+            if (a.nhub) k_hub_finalize<<<grid_for(a.nhub, 128, ctx.num_sms * 4), 128, 0, cs>>>(a);
             MB_CHECK_LAUNCH();
         }
         if (iters == 0) {  // no superstep: the ranks are the initial ranks
@@ -291,7 +308,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             stats->device_ms = ms;
             stats->schedule_count[unfused ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE] = iters;
             stats->edges_scanned = (int64_t)iters * g.E;
-            stats->kernel_launches = 1 + (int64_t)iters * (1 + (st.nblk > 0) + unfused) + (iters == 0);
+            stats->kernel_launches =
+                1 + (int64_t)iters * (1 + (st.nitems > 0) + (st.nhub > 0) + unfused) + (iters == 0);
         }
     } catch (...) {
         cudaEventDestroy(e0);

@@ -8,8 +8,8 @@ struct PrState {
     bool built = false;
     int32_t V = 0;
     int64_t E = 0;
-    DevBuf rank, contrib[2], msg, hub_v, hub_first, blk_v, blk_sum;
-    int32_t nhub = 0, nblk = 0;
+    DevBuf rank, contrib[2], msg, items, hub_v, hub_first, blk_sum;
+    int32_t nitems = 0, nhub = 0;
     cudaGraphExec_t exec = nullptr;  // captured run (init + iters supersteps)
     int32_t g_iters = -1, g_sched = -1;
     float g_init = 0.f;
@@ -19,7 +19,7 @@ struct PrState {
         exec = nullptr;
         g_iters = -1;
         rank.release(); contrib[0].release(); contrib[1].release(); msg.release();
-        hub_v.release(); hub_first.release(); blk_v.release(); blk_sum.release();
+        items.release(); hub_v.release(); hub_first.release(); blk_sum.release();
         built = false;
     }
     void ensure(Context &ctx, const Graph &g);

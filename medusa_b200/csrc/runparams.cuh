@@ -21,11 +21,15 @@ struct RunParams {
     int32_t persist;            // 1: schedules 0/4 and splits run in the persistent grid
     int32_t replay_then_fixed;  // replay policy: past the list use the fixed rule (else repeat)
     int32_t max_step;           // >= 0: stop after this superstep (trace collection)
+    uint32_t tail_edges;        // schedule 0 frontiers up to this many out-edges run in the tail
+    uint32_t bm_push_min;       // SSSP: schedule 0 on a queue frontier with at least this many
+                                // out-edges writes a bitmap compacted after (0: never)
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 
 // Write this run's RunParams (policy, forced schedule, replay list, source,
 // SSSP bucket width) to a control block whose first member is RunParams.
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f);
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f,
+                   uint32_t bm_push_min = 0);
 
 }  // namespace mb

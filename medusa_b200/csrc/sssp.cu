@@ -41,6 +41,7 @@ struct SsspArgs {
     float *msg;
     int32_t *far[2];  // near-far piles (vertices whose distance is >= the threshold)
     uint32_t *farbm;  // membership bitmap of the pile being filled
+    uint32_t *nbm;    // next-frontier bitmap of the bitmap-output push (all zero between uses)
 };
 
 __device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
@@ -87,6 +88,10 @@ struct PushSmem {
     BlockQueue bq;
 };
 
+// kBmOut: instead of claiming each improved vertex (an atomic with a
+// result) and appending it to the next queue, set its bit in a.nbm with a
+// fire-and-forget atomicOr; k_nbm2q then builds the next queue.
+template <bool kBmOut>
 __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm) {
     uint32_t *s_off = sm.off;
     int32_t *s_row = sm.row;
@@ -142,6 +147,20 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
         }
 #pragma unroll
         for (int r = 0; r < kTileItems; r++) dv[r] = ok[r] ? ld_dist(a, v[r]) : 0.f;
+        if (kBmOut) {
+#pragma unroll
+            for (int r = 0; r < kTileItems; r++) {
+                bool to_far = false;
+                if (ok[r] && nd[r] < dv[r]) {
+                    atomicMin((unsigned *)&a.dist[v[r]], __float_as_uint(nd[r]));
+                    if (nd[r] >= thresh) to_far = true;
+                    else atomicOr(&a.nbm[v[r] >> 5], 1u << (v[r] & 31));
+                }
+                far_push(a, c, to_far, v[r]);
+            }
+            __syncthreads();  // the tile's shared entries are reloaded next
+            continue;
+        }
 #pragma unroll
         for (int r = 0; r < kTileItems; r++) {
             bool own = false, to_far = false;
@@ -170,7 +189,36 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
 __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
     __shared__ PushSmem sm;
     count_launch(a.f.ctrl);
-    work_push_edge_q(a, sm);
+    work_push_edge_q<false>(a, sm);
+}
+
+__global__ void __launch_bounds__(kPushThreads) k_push_edge_bm(SsspArgs a) {
+    __shared__ PushSmem sm;
+    count_launch(a.f.ctrl);
+    work_push_edge_q<true>(a, sm);
+}
+
+// After k_push_edge_bm: next-frontier bitmap -> next queue (with the
+// claimed-vertex count), clearing the bitmap; one warp per word.
+__global__ void __launch_bounds__(256) k_nbm2q(SsspArgs a) {
+    count_launch(a.f.ctrl);
+    Ctrl *c = a.f.ctrl;
+    const int nxt = c->cur ^ 1;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    uint32_t cn = 0;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
+        const uint32_t word = a.nbm[w];
+        if (!word) continue;  // warp-uniform
+        if (lane == 0) a.nbm[w] = 0u;
+        const int32_t v = (int32_t)(w * 32 + lane);
+        const bool in = (word >> lane) & 1u;
+        const uint32_t deg = in ? (uint32_t)a.f.outdeg[v] : 0u;
+        cn += in;
+        enqueue_warp(in && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
+                     pick(a.f.tf, nxt));
+    }
+    flush_counts(c, cn, 0);
 }
 
 // schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
@@ -585,7 +633,7 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
         } else {
             if (!persist_convert(a.f, s, mode)) break;
             if (s == MB_SCHED_PULL_THREAD) work_pull_stream<false>(a);
-            else work_push_edge_q(a, sm);
+            else work_push_edge_q<false>(a, sm);
         }
         if (!grid_sync(c)) break;
         persist_bookkeep(a.f, APP_SSSP, cap);
@@ -680,6 +728,12 @@ __global__ void k_weight_sum(const float *w, int64_t E, double *out) {
 
 }  // namespace
 
+uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g) {
+    const int64_t t = ctx.tunable[MB_TUNE_SSSP_BM_PUSH_MIN];
+    if (t >= 0) return (uint32_t)std::min<int64_t>(t, 0xffffffffll);
+    return (uint32_t)std::min<int64_t>(std::max<int64_t>(1 << 20, g.E / 8), 0xffffffffll);
+}
+
 float sssp_default_delta(const Graph &g) {
     if (g.E == 0) return 0.f;
     DevBuf acc;
@@ -712,11 +766,14 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.far[0] = st.far[0].as<int32_t>();
     a.far[1] = st.far[1].as<int32_t>();
     a.farbm = st.farbm.as<uint32_t>();
+    a.nbm = st.nbm.as<uint32_t>();
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
-    upload_params(ctx, st.ctrl.p, source, delta);
+    upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
 
-    const int grid_push = ctx.num_sms * 8, grid_vtx = ctx.num_sms * 8, grid_edge = ctx.num_sms * 8;
+    const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
+    const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
+    const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
     LoopSpec sp;
     sp.st = &st;
@@ -730,6 +787,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         k_fill_dist<<<grid_vtx, 256, 0, s>>>(a);
         MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
         MB_CUDA(cudaMemsetAsync(a.farbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
+        MB_CUDA(cudaMemsetAsync(a.nbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
         k_sssp_init<<<1, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();
     };
@@ -746,6 +804,12 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         }
         if (branch == kBranchPersist) {
             launch_cooperative((const void *)k_persist, persist_grid, kPushThreads, s, a, sp.cap);
+            return;
+        }
+        if (branch == kBranchPushBm) {
+            k_push_edge_bm<<<grid_push, kPushThreads, 0, s>>>(a);
+            k_nbm2q<<<grid_vtx, 256, 0, s>>>(a);
+            MB_CHECK_LAUNCH();
             return;
         }
         const int sched = branch % MB_NUM_SCHEDULES;

@@ -9,7 +9,7 @@ namespace mb {
 float sssp_default_delta(const Graph &g);
 
 struct SsspState : FrontierState {
-    DevBuf dist, stamp, msg, far[2], farbm;
+    DevBuf dist, stamp, msg, far[2], farbm, nbm;
     float default_delta = 0.f;
     ~SsspState() { release(); }
     void release() {
@@ -20,6 +20,7 @@ struct SsspState : FrontierState {
         far[0].release();
         far[1].release();
         farbm.release();
+        nbm.release();
     }
     void ensure(const Graph &g) {
         if (ensure_frontier(g)) {
@@ -34,10 +35,16 @@ struct SsspState : FrontierState {
             far[0].reserve(sizeof(int32_t) * (size_t)g.V);
             far[1].reserve(sizeof(int32_t) * (size_t)g.V);
             farbm.reserve(sizeof(uint32_t) * (size_t)W);
+            nbm.reserve(sizeof(uint32_t) * (size_t)W);
             default_delta = sssp_default_delta(g);
         }
     }
 };
+
+// Frontier out-edges from which schedule 0 writes a next-frontier bitmap
+// (compacted afterwards) instead of claiming vertices one by one.
+// MB_TUNE_SSSP_BM_PUSH_MIN when set, else max(2^20, E/8); 0 turns it off.
+uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g);
 
 // One SSSP from `source`; distances are left in st.dist (device).
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats);

@@ -1,0 +1,63 @@
+"""One measured case per invocation, for profilers (ncu launch lists and
+single-kernel captures) and quick timings:
+
+    python -m medusa_b200.profile_cases CASE [--reps N] [--hostloop]
+
+CASE: c2-bfs, c2-sssp (R-MAT 2^20 / 2^24, source 0), c1-pr (uniform
+2^18 / 2^22, 10 supersteps), c5-bfs, c5-sssp (R-MAT 2^24 / 2^28,
+(0.57,0.19,0.19,0.05)), c5-pr (20 supersteps), c3-bfs, c3-sssp (1448^2
+grid), c5s-bfs, c5s-sssp, c5s-pr (the C5 generator at 2^21 / 2^25: a case
+small enough for full ncu captures).  Prints one line per repetition with
+the library's device time.  --hostloop runs the host-driven loop (kernels in
+conditional-node graphs are invisible to ncu)."""
+import argparse
+import sys
+
+from . import api
+
+SEED = 1
+
+
+def params(case):
+    if case.startswith("c2"):
+        return api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000)
+    if case.startswith("c1"):
+        return api.uniform_params(1 << 18, 1 << 22, seed=SEED)
+    if case.startswith("c5s"):
+        return api.rmat_params(21, 1 << 25, 0.57, 0.19, 0.19, seed=SEED, wmin=1, wmax=1000)
+    if case.startswith("c5"):
+        return api.rmat_params(24, 1 << 28, 0.57, 0.19, 0.19, seed=SEED, wmin=1, wmax=1000)
+    if case.startswith("c3"):
+        return api.grid_params(1448, 1448, 0.1, 0.005, seed=SEED, wmin=1, wmax=100)
+    raise SystemExit("unknown case " + case)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--hostloop", action="store_true")
+    args = ap.parse_args(argv)
+    ctx = api.Context(0)
+    if args.hostloop:
+        ctx.set_graph_capture(False)
+    g = ctx.generate(params(args.case))
+    kind = args.case.split("-")[1]
+    for i in range(args.reps):
+        if kind == "bfs":
+            _, st = g.bfs([0])
+        elif kind == "sssp":
+            _, st = g.sssp([0])
+        elif kind == "pr":
+            _, st = g.pagerank(20 if args.case.startswith("c5") else 10, 1.0 / g.V)
+        else:
+            raise SystemExit("unknown case " + args.case)
+        print("%s rep %d: %.4f ms, %d supersteps, %d launches" %
+              (args.case, i, st["device_ms"], st["supersteps"], st["kernel_launches"]), flush=True)
+    g.close()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -147,16 +147,52 @@ int orc_sssp(int32_t V, int64_t E, const int32_t *e_src, const float *e_w,
 }
 
 /*
+ * The GPU's fixed summation order for a vertex's n messages m[0..n) (slot
+ * order): n <= 64, a sequential fold; else blocks of 4096 messages, each the
+ * 32-lane strided fold (lane l: m[l], m[l+32], ... in order) reduced by an
+ * xor butterfly (each step t[l] = s[l] + s[l ^ off], off = 16, 8, 4, 2, 1),
+ * the block results folded sequentially.  Not the reference's order: the
+ * reference folds sequentially (MPG/CPUFunctorHoster.cpp:21-26); this order
+ * is what the CUDA kernels compute, so they can be checked bit for bit.
+ */
+#define ORC_PR_LIGHT 64
+#define ORC_PR_BLOCK 4096
+static float orc_fold_blocked(const float *m, int32_t n)
+{
+    float total = 0.0f;
+    if (n <= ORC_PR_LIGHT) {
+        for (int32_t i = 0; i < n; i++) total += m[i];
+        return total;
+    }
+    for (int32_t b0 = 0; b0 < n; b0 += ORC_PR_BLOCK) {
+        int32_t b1 = n < b0 + ORC_PR_BLOCK ? n : b0 + ORC_PR_BLOCK;
+        float lane[32], t[32];
+        for (int l = 0; l < 32; l++) {
+            lane[l] = 0.0f;
+            for (int32_t j = b0 + l; j < b1; j += 32) lane[l] += m[j];
+        }
+        for (int off = 16; off; off >>= 1) {
+            for (int l = 0; l < 32; l++) t[l] = lane[l] + lane[l ^ off];
+            for (int l = 0; l < 32; l++) lane[l] = t[l];
+        }
+        total += lane[0];
+    }
+    return total;
+}
+
+/*
  * PageRank in the reference's non-normalised form, FP32, with the reference's
  * mixed-precision update: sum is float, "sum *= 0.85" multiplies by a double
  * literal and rounds back to float, "0.15 + sum" adds in double and rounds to
  * float (MPG/CPUFunctorHoster.cpp:21-29).  msg = rank/out_degree in float
- * (:80-82).  Each vertex sums its slots in msg_index order.  iters supersteps,
- * rank[] holds the initial ranks on entry.
+ * (:80-82).  order 0: each vertex sums its slots sequentially in msg_index
+ * order (the reference's fold); order 1: the GPU's fixed order
+ * (orc_fold_blocked).  iters supersteps, rank[] holds the initial ranks on
+ * entry.
  */
 int orc_pagerank_f32(int32_t V, int64_t E, const int32_t *e_src,
                      const int32_t *msg_dst, const int32_t *msg_index,
-                     const int32_t *edge_index, int iters, float *rank)
+                     const int32_t *edge_index, int iters, float *rank, int order)
 {
     float *msg = (float *)malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
     if (!msg) return -1;
@@ -169,7 +205,11 @@ int orc_pagerank_f32(int32_t V, int64_t E, const int32_t *e_src,
         }
         for (int32_t v = 0; v < V; v++) {
             float sum = 0.0f;
-            for (int32_t i = msg_index[v]; i < msg_index[v + 1]; i++) sum += msg[i];
+            if (order == 1) {
+                sum = orc_fold_blocked(msg + msg_index[v], msg_index[v + 1] - msg_index[v]);
+            } else {
+                for (int32_t i = msg_index[v]; i < msg_index[v + 1]; i++) sum += msg[i];
+            }
             sum = (float)((double)sum * 0.85);
             rank[v] = (float)(0.15 + (double)sum);
         }

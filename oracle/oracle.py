@@ -47,8 +47,7 @@ _lib = None
 def _oracle():
     global _lib
     if _lib is None:
-        if not os.path.exists(ORACLE_SO):
-            build_oracle()
+        build_oracle()  # rebuilds when the source is newer than the library
         lib = ctypes.CDLL(ORACLE_SO)
         lib.orc_build_aa.restype = ctypes.c_int
         lib.orc_build_aa.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p,
@@ -61,7 +60,7 @@ def _oracle():
                                  _i32p, _f32p]
         lib.orc_pagerank_f32.restype = ctypes.c_int
         lib.orc_pagerank_f32.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p,
-                                         _i32p, _i32p, ctypes.c_int, _f32p]
+                                         _i32p, _i32p, ctypes.c_int, _f32p, ctypes.c_int]
         lib.orc_pagerank_f64.restype = ctypes.c_int
         lib.orc_pagerank_f64.argtypes = [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p,
                                          _i32p, _i32p, ctypes.c_int, _f64p]
@@ -120,8 +119,12 @@ def sssp(V, src, dst, w, source):
     return dist, steps
 
 
-def pagerank(V, src, dst, iters, init, fp64=False):
-    """Ranks after `iters` supersteps of the reference's PageRank."""
+def pagerank(V, src, dst, iters, init, fp64=False, order="reference"):
+    """Ranks after `iters` supersteps of the reference's PageRank.  order
+    "reference": each vertex folds its messages sequentially in slot order
+    (MPG/CPUFunctorHoster.cpp:21-26); "device": the CUDA kernels' fixed
+    order (sequential up to 64 in-edges, else 4096-edge blocks of 32-lane
+    strided folds reduced by an xor butterfly, folded in order)."""
     g = src if isinstance(src, AAGraph) else AAGraph(V, src, dst)
     if fp64:
         rank = np.full(g.V, float(init), np.float64)
@@ -130,7 +133,8 @@ def pagerank(V, src, dst, iters, init, fp64=False):
     else:
         rank = np.full(g.V, np.float32(init), np.float32)
         rc = _oracle().orc_pagerank_f32(g.V, g.E, g.e_src, g.msg_dst, g.msg_index,
-                                        g.edge_index, iters, rank)
+                                        g.edge_index, iters, rank,
+                                        {"reference": 0, "device": 1}[order])
     if rc < 0:
         raise MemoryError("orc_pagerank")
     return rank

@@ -81,10 +81,9 @@ def test_pagerank_matches_reference(ctx, name):
     indeg = np.diff(aa.msg_index)
     r64 = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], fp64=True)
     check_pagerank(r, c["pr_rank"], r64, indeg)
-    # same summation order as the oracle for in-degree <= 2048 and no hubs
-    if indeg.max(initial=0) <= 2048:
-        ro = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"])
-        np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
+    # bit for bit against the oracle run in the kernels' summation order
+    ro = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], order="device")
+    np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
     g.close()
 
 
@@ -265,9 +264,42 @@ def test_full_size_pagerank_c1_against_oracle(gpu_ctx, api):
     r, st = g.pagerank(10, 1.0 / V)
     aa = O.AAGraph(V, s_, d_)
     ro = O.pagerank(V, aa, None, 10, 1.0 / V)
-    # in-degrees are far below the hub threshold: same order as the oracle
+    # in-degrees are all <= 64: the kernels' order is the reference's fold
+    assert np.diff(aa.msg_index).max() <= 64
     np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
     g.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_sssp_bitmap_output_push(ctx, api, name):
+    """Every schedule-0 superstep through the bitmap-output push (threshold
+    1, persistent tail off): distances equal the reference's."""
+    c = load_golden(name)
+    if c["w"] is None:
+        pytest.skip("unweighted")
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    ctx.set_tunable("sssp_bm_push_min", 1)
+    ctx.set_tunable("tail_edges", 0)
+    try:
+        for i, s in enumerate(c["sources"]):
+            d, st = g.sssp([int(s)])
+            np.testing.assert_array_equal(d[0], c["sssp_dist"][i])
+    finally:
+        ctx.set_tunable("sssp_bm_push_min", -1)
+        ctx.set_tunable("tail_edges", -1)
+        g.close()
+
+
+def test_tunables_validate_and_reset(gpu_ctx, api):
+    assert gpu_ctx.get_tunable("push_blocks_per_sm") == -1
+    gpu_ctx.set_tunable("push_blocks_per_sm", 4)
+    assert gpu_ctx.get_tunable("push_blocks_per_sm") == 4
+    with pytest.raises(api.MedusaError):
+        gpu_ctx.set_tunable("push_blocks_per_sm", 0)
+    with pytest.raises(api.MedusaError):
+        gpu_ctx.set_tunable(99, 1)
+    gpu_ctx.set_tunable("push_blocks_per_sm", -1)
+    assert gpu_ctx.get_tunable("push_blocks_per_sm") == -1
 
 
 @pytest.mark.parametrize("direction", [None, 0, 4], ids=["fixed", "push", "pull"])

@@ -47,6 +47,58 @@ def check_pagerank(got, ref, r64, indeg, tol=1e-5, hub=2048):
     assert (np.abs(ref - r64) / r64).max() <= bound
 
 
+def _butterfly_fold(m):
+    """numpy emulation of the kernels' order for one vertex's messages."""
+    m = np.asarray(m, np.float32)
+    if len(m) <= 64:
+        t = np.float32(0)
+        for x in m:
+            t = np.float32(t + x)
+        return t
+    total = np.float32(0)
+    for b0 in range(0, len(m), 4096):
+        blk = m[b0:b0 + 4096]
+        lane = np.zeros(32, np.float32)
+        for l in range(32):
+            for x in blk[l::32]:
+                lane[l] = np.float32(lane[l] + x)
+        for off in (16, 8, 4, 2, 1):
+            lane = (lane + lane[np.arange(32) ^ off]).astype(np.float32)
+        total = np.float32(total + lane[0])
+    return total
+
+
+@pytest.mark.parametrize("n", [5, 64, 65, 4096, 4097, 9000])
+def test_oracle_device_order_on_a_star(n):
+    """Device-order PageRank of a star (n leaves -> hub, one superstep):
+    the hub's sum equals the numpy emulation of the kernels' fold."""
+    rng = np.random.default_rng(n)
+    V = n + 1
+    # leaf i has out-degree k_i (edges to the hub, plus extra edges to leaf 1
+    # so messages differ: rank/outdeg)
+    src, dst = [], []
+    for i in range(1, V):
+        src.append(i); dst.append(0)
+        for _ in range(int(rng.integers(0, 3))):
+            src.append(i); dst.append(1 if i != 1 else 2)
+    src = np.array(src, np.int32); dst = np.array(dst, np.int32)
+    init = np.float32(1.0 / V)
+    g = O.AAGraph(V, src, dst)
+    r = O.pagerank(V, g, None, 1, init, order="device")
+    # messages of the hub in slot order
+    outdeg = g.out_degree()
+    slots = np.empty(g.E, np.float32)
+    for e in range(g.E):
+        s_ = g.e_src[e]
+        slots[g.msg_dst[e]] = np.float32(init / np.float32(outdeg[s_]))
+    m = slots[g.msg_index[0]:g.msg_index[1]]
+    sm = _butterfly_fold(m)
+    want = np.float32(0.15 + np.float64(np.float32(np.float64(sm) * 0.85)))
+    assert r[0] == want
+    if n <= 64:
+        assert r[0] == O.pagerank(V, g, None, 1, init)[0]
+
+
 def test_oracle_layout_matches_reference_builders():
     # msg_index is the prefix of in-degrees; msg_dst hands out slots per
     # destination in AA edge order (SSSP/EdgeDataType.cu:181-182)
