@@ -21,7 +21,10 @@ distances come back device->host inside the timed region.
 (64 BFS + 32 SSSP sources on R-MAT 2^22/2^26, batched vs one loop per
 source, identical outputs) and C5 (R-MAT 2^24/2^28, (0.57,0.19,0.19,0.05):
 BFS, SSSP and 20 PageRank supersteps, fixed vs learned schedule with HBM
-roofline fractions, plus per-superstep fixed / learned / oracle-best costs).
+roofline fractions, plus per-superstep fixed / learned / oracle-best costs)
+and C4b (256 R-MAT graphs of uneven sizes, 20 PageRank supersteps + one BFS
+each, in one persistent launch vs one library call per graph, identical
+outputs).
 
 `forms`: the same graph, 64 BFS sources (vertices 0..63) and 32 SSSP
 sources (0..31) under four forms -- plain (fixed schedule rule, one loop per
@@ -465,7 +468,53 @@ def bench_configs(ctx, api, args, flush):
                                    "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}}
     out["c5_scale"] = c5
     g.close()
+    del lv, dd, rk
+    out["c4b_many_graphs"] = bench_many_graphs(ctx, api, reps)
     return out
+
+
+def bench_many_graphs(ctx, api, reps):
+    """C4b: 256 R-MAT graphs of uneven sizes, 20 PageRank supersteps + one
+    BFS each, in ONE persistent launch vs one library call per graph."""
+    import torch
+    ps = api.c4b_params(256, seed=SEED)
+    b = ctx.batch_generate(ps)
+    ranks = torch.empty(b.total_V, dtype=torch.float32, device="cuda")
+    levels = torch.empty(b.total_V, dtype=torch.int32, device="cuda")
+    b.run(20, None, ranks, levels)
+    ms = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        _, _, st = b.run(20, None, ranks, levels)
+        ms.append(st["device_ms"])
+    one = float(np.median(ms))
+    r_all = ranks.cpu().numpy()
+    l_all = levels.cpu().numpy()
+    # the same work one graph at a time through mb_pagerank / mb_bfs
+    seq_ms, same = 0.0, True
+    for i, p in enumerate(ps):
+        g = ctx.generate(p)
+        r, s1 = g.pagerank(20, 1.0 / g.V)
+        lv, s2 = g.bfs([0])
+        seq_ms += s1["device_ms"] + s2["device_ms"]
+        same &= bool(np.array_equal(r.view(np.uint32), r_all[b.vbase[i]:b.vbase[i + 1]].view(np.uint32))
+                     and np.array_equal(lv[0], l_all[b.vbase[i]:b.vbase[i + 1]]))
+        g.close()
+    edges = st["edges_traversed"]
+    res = {"workload": "256 R-MAT graphs, (0.45,0.15,0.15,0.25), vertices 2^10..2^18 log-uniform, "
+                       "average degree uniform [4,32], seed 1; 20 PageRank supersteps + one BFS "
+                       "from vertex 0 each",
+           "graphs": b.n, "vertices": int(b.total_V), "edges": int(b.total_E),
+           "one_launch": {"ms": round(one, 3), "edges_per_s": round(edges / (one / 1e3), 1),
+                          "kernel_launches": st["kernel_launches"]},
+           "one_call_per_graph": {"ms": round(seq_ms, 3),
+                                  "edges_per_s": round(edges / (seq_ms / 1e3), 1)},
+           "vs_one_call_per_graph": round(seq_ms / one, 3),
+           "identical": same,
+           "tunables": {"batch_threads": ctx.get_tunable("batch_threads"),
+                        "batch_edges_per_cta": ctx.get_tunable("batch_edges_per_cta")}}
+    b.close()
+    return res
 
 
 def bench_pagerank(ctx, api, args, flush):

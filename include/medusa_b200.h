@@ -194,6 +194,23 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
+/* ---- many graphs in one launch (no reference counterpart) ----------------- */
+/* A batch of independent graphs (reference order), e.g. 256 R-MAT graphs of
+ * uneven sizes.  mb_batch_run runs, for every graph, `pr_iters` PageRank
+ * supersteps from 1/V (as mb_pagerank) and then one BFS (as mb_bfs) from
+ * sources[i] (nullable: vertex 0), all in ONE persistent cooperative launch
+ * fed by a device work queue; each graph is worked by a team of CTAs sized
+ * by its edge count.  Outputs are concatenated: graph i's ranks and levels
+ * at [vbase[i], vbase[i+1]) (mb_batch_vertex_offsets); host or device. */
+typedef struct mb_batch mb_batch;
+int mb_batch_generate(mb_ctx *ctx, int32_t n, const mb_gen_params *params, mb_batch **out);
+int mb_batch_info(const mb_batch *b, int32_t *num_graphs, int64_t *total_vertices,
+                  int64_t *total_edges);
+int mb_batch_vertex_offsets(const mb_batch *b, int64_t *vbase);
+int mb_batch_run(mb_ctx *ctx, mb_batch *b, int32_t pr_iters, const int32_t *sources,
+                 float *ranks_out, int32_t *levels_out, mb_stats *stats);
+int mb_batch_destroy(mb_batch *b);
+
 /* ---- tunables (no reference counterpart) --------------------------------- */
 /* Launch and routing parameters that change speed, never results; set by
  * the autotuner (medusa_b200/autotune.py) or by hand.  value -1 restores
@@ -206,8 +223,12 @@ int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
 #define MB_TUNE_VERTEX_BLOCKS_PER_SM 2 /* CTAs per SM of the per-vertex / per-word
                                           kernels (default 8) */
 #define MB_TUNE_TAIL_EDGES 3 /* frontier out-edges up to which schedule 0 runs in the
-                                persistent single-CTA tail (default 16384, at most 16384) */
-#define MB_NUM_TUNABLES 4
+                                persistent single-CTA tail (default 16384) */
+#define MB_TUNE_BATCH_THREADS 4 /* threads per CTA of the many-graph kernel (default 256;
+                                   a multiple of 32, 64..1024) */
+#define MB_TUNE_BATCH_EDGES_PER_CTA 5 /* many-graph kernel: a graph gets one CTA per this
+                                         many edges + vertices (default 65536) */
+#define MB_NUM_TUNABLES 6
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

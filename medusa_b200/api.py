@@ -22,9 +22,9 @@ MB_POLICY_FIXED, MB_POLICY_LEARNED, MB_POLICY_FORCED, MB_POLICY_ORACLE_BEST = 0,
 MB_GEN_RMAT, MB_GEN_UNIFORM, MB_GEN_GRID = 0, 1, 2
 MB_MODEL_BFS, MB_MODEL_BATCHED, MB_MODEL_SSSP = 0, 1, 2
 MB_TUNE_SSSP_BM_PUSH_MIN, MB_TUNE_PUSH_BLOCKS_PER_SM, MB_TUNE_VERTEX_BLOCKS_PER_SM, \
-    MB_TUNE_TAIL_EDGES = 0, 1, 2, 3
+    MB_TUNE_TAIL_EDGES, MB_TUNE_BATCH_THREADS, MB_TUNE_BATCH_EDGES_PER_CTA = 0, 1, 2, 3, 4, 5
 TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_sm": 2,
-            "tail_edges": 3}
+            "tail_edges": 3, "batch_threads": 4, "batch_edges_per_cta": 5}
 NUM_SCHEDULES = 8
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
@@ -97,6 +97,12 @@ def _load():
                                               ctypes.POINTER(F32)]),
         "mb_scheduler_num_params": (I32, []),
         "mb_set_tunable": (ctypes.c_int, [P, I32, ctypes.c_int64]),
+        "mb_batch_generate": (ctypes.c_int, [P, I32, P, ctypes.POINTER(P)]),
+        "mb_batch_info": (ctypes.c_int, [P, ctypes.POINTER(I32), ctypes.POINTER(I64),
+                                         ctypes.POINTER(I64)]),
+        "mb_batch_vertex_offsets": (ctypes.c_int, [P, P]),
+        "mb_batch_run": (ctypes.c_int, [P, P, I32, P, P, P, P]),
+        "mb_batch_destroy": (ctypes.c_int, [P]),
         "mb_get_tunable": (ctypes.c_int, [P, I32, ctypes.POINTER(ctypes.c_int64)]),
         "mb_scheduler_get_weights": (ctypes.c_int, [P, I32, P]),
         "mb_scheduler_set_weights": (ctypes.c_int, [P, I32, P]),
@@ -257,6 +263,65 @@ class Graph:
         return out, st.as_dict()
 
 
+class Batch:
+    """Many independent graphs run together (mb_batch_*)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.h = ctypes.c_void_p(handle)
+        n = ctypes.c_int32(0)
+        V = ctypes.c_int64(0)
+        E = ctypes.c_int64(0)
+        _check(lib.mb_batch_info(self.h, ctypes.byref(n), ctypes.byref(V), ctypes.byref(E)))
+        self.n, self.total_V, self.total_E = n.value, V.value, E.value
+        self.vbase = np.zeros(self.n + 1, np.int64)
+        _check(lib.mb_batch_vertex_offsets(self.h, self.vbase.ctypes.data))
+
+    def close(self):
+        if self.h:
+            lib.mb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, pr_iters=20, sources=None, ranks=None, levels=None):
+        """PageRank then one BFS on every graph, one launch: (ranks, levels, stats),
+        concatenated by vbase."""
+        src = None
+        if sources is not None:
+            src = np.ascontiguousarray(sources, np.int32)
+            assert len(src) == self.n
+        if ranks is None:
+            ranks = np.empty(self.total_V, np.float32)
+        if levels is None:
+            levels = np.empty(self.total_V, np.int32)
+        st = Stats()
+        _check(lib.mb_batch_run(self.ctx.h, self.h, int(pr_iters), _ptr(src), _ptr(ranks),
+                                _ptr(levels), ctypes.byref(st)), self.ctx.h)
+        return ranks, levels, st.as_dict()
+
+    def split(self, arr):
+        return [arr[self.vbase[i]:self.vbase[i + 1]] for i in range(self.n)]
+
+
+def c4b_params(n=256, seed=1):
+    """The many-graph workload: n R-MAT graphs, (a,b,c) = (0.45,0.15,0.15),
+    vertices 2^10..2^18 log-uniform (2^s with s uniform in [10, 18], rounded to
+    a whole scale), average degree uniform in [4, 32]; seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        scale = int(rng.integers(10, 19))
+        deg = float(rng.uniform(4, 32))
+        out.append(rmat_params(scale, int(round(deg * (1 << scale))), 0.45, 0.15, 0.15,
+                               seed=seed * 100003 + i))
+    return out
+
+
 class Context:
     """One CUDA device, one stream, and the device scratch of every run."""
 
@@ -383,6 +448,13 @@ class Context:
                                        _ptr(dst) if E else None, _ptr(w) if E else None,
                                        flags, ctypes.byref(g)), self.h)
         return Graph(self, g.value)
+
+    def batch_generate(self, params_list):
+        arr = (GenParams * len(params_list))(*params_list)
+        h = ctypes.c_void_p()
+        _check(lib.mb_batch_generate(self.h, len(params_list), ctypes.cast(arr, ctypes.c_void_p),
+                                     ctypes.byref(h)), self.h)
+        return Batch(self, h.value)
 
     def generate(self, params, reference_order=True):
         g = ctypes.c_void_p()

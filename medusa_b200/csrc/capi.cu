@@ -8,6 +8,7 @@
 #include "bfs.cuh"
 #include "learn.cuh"
 #include "msbfs.cuh"
+#include "multigraph.cuh"
 #include "mssssp.cuh"
 #include "pagerank.cuh"
 #include "sched.cuh"
@@ -27,6 +28,11 @@ void graph_generate(Context &ctx, Graph &g, const mb_gen_params &p, uint32_t fla
 
 struct mb_ctx {
     mb::Context c;
+};
+
+struct mb_batch {
+    mb::Batch b;
+    int device = 0;
 };
 struct mb_graph {
     mb::Graph g;
@@ -206,6 +212,10 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "blocks per SM must be 1..32");
     if (which == MB_TUNE_TAIL_EDGES && value > (1 << 24))
         return set_error(ctx, MB_ERR_INVALID, "tail edges must be <= 2^24");
+    if (which == MB_TUNE_BATCH_THREADS && value != -1 && (value < 64 || value > 1024 || value % 32))
+        return set_error(ctx, MB_ERR_INVALID, "batch threads must be a multiple of 32 in 64..1024");
+    if (which == MB_TUNE_BATCH_EDGES_PER_CTA && value == 0)
+        return set_error(ctx, MB_ERR_INVALID, "batch edges per CTA must be >= 1");
     ctx->c.tunable[which] = value;
     ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
     return MB_OK;
@@ -437,6 +447,75 @@ int mb_graph_destroy(mb_graph *g) {
     g->g.apps = nullptr;
     g->g.release();
     delete g;
+    return MB_OK;
+}
+
+int mb_batch_generate(mb_ctx *ctx, int32_t n, const mb_gen_params *params, mb_batch **out) {
+    if (!ctx || !out || !params) return set_error(ctx, MB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (n < 1) return set_error(ctx, MB_ERR_INVALID, "a batch holds at least one graph");
+    mb_batch *b = new (std::nothrow) mb_batch();
+    if (!b) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        b->device = ctx->c.device;
+        for (int32_t i = 0; i < n; i++)
+            if (params[i].kind != MB_GEN_GRID && params[i].num_edges > 0x7FFFFFFFll)
+                mb::fail(MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
+        mb::batch_generate(ctx->c, b->b, params, n);
+    });
+    if (rc != MB_OK) {
+        mb_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return MB_OK;
+}
+
+int mb_batch_info(const mb_batch *b, int32_t *num_graphs, int64_t *total_vertices,
+                  int64_t *total_edges) {
+    if (!b) return set_error(nullptr, MB_ERR_INVALID, "null batch");
+    if (num_graphs) *num_graphs = (int32_t)b->b.graphs.size();
+    if (total_vertices) *total_vertices = b->b.total_V;
+    if (total_edges) *total_edges = b->b.total_E;
+    return MB_OK;
+}
+
+int mb_batch_vertex_offsets(const mb_batch *b, int64_t *vbase) {
+    if (!b || !vbase) return set_error(nullptr, MB_ERR_INVALID, "null argument");
+    std::memcpy(vbase, b->b.vbase.data(), sizeof(int64_t) * b->b.vbase.size());
+    return MB_OK;
+}
+
+int mb_batch_run(mb_ctx *ctx, mb_batch *b, int32_t pr_iters, const int32_t *sources,
+                 float *ranks_out, int32_t *levels_out, mb_stats *stats) {
+    return guarded(ctx, [&] {
+        if (!ctx || !b || !ranks_out || !levels_out) mb::fail(MB_ERR_INVALID, "null argument");
+        if (b->device != ctx->c.device) mb::fail(MB_ERR_INVALID, "batch lives on another device");
+        if (pr_iters < 0) mb::fail(MB_ERR_INVALID, "pr_iters must be >= 0");
+        use_device(ctx);
+        const int32_t n = (int32_t)b->b.graphs.size();
+        std::vector<int32_t> src;
+        if (sources) src = fetch_i32(sources, n);
+        const size_t nv = (size_t)b->b.total_V;
+        const bool dev_r = mb::is_device_ptr(ranks_out), dev_l = mb::is_device_ptr(levels_out);
+        float *r = ranks_out;
+        int32_t *l = levels_out;
+        if (!dev_r) r = (float *)b->b.rank.reserve(sizeof(float) * std::max<size_t>(nv, 1));
+        if (!dev_l) l = (int32_t *)b->b.level.reserve(sizeof(int32_t) * std::max<size_t>(nv, 1));
+        mb::batch_run(ctx->c, b->b, pr_iters, sources ? src.data() : nullptr, r, l, stats);
+        if (!dev_r) MB_CUDA(cudaMemcpyAsync(ranks_out, r, sizeof(float) * nv, cudaMemcpyDeviceToHost, ctx->c.stream));
+        if (!dev_l) MB_CUDA(cudaMemcpyAsync(levels_out, l, sizeof(int32_t) * nv, cudaMemcpyDeviceToHost, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int mb_batch_destroy(mb_batch *b) {
+    if (!b) return MB_OK;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    b->b.release();
+    delete b;
     return MB_OK;
 }
 

@@ -32,7 +32,7 @@
 namespace mb {
 namespace {
 
-constexpr int kWin = 1024;               // edges staged per warp per window
+constexpr int kWin = 512;                // edges staged per warp per window
 constexpr int kPrWarps = 8;              // warps per CTA
 constexpr int kPrThreads = kPrWarps * 32;
 
@@ -196,6 +196,10 @@ void PrState::ensure(Context &ctx, const Graph &g) {
                                    v, slots++));
     }
     hf.push_back(slots);
+    // longest blocks first: the warps that take hub blocks start earliest
+    // (the order of the items does not change any sum)
+    std::stable_sort(it.begin(), it.end(),
+                     [](const int4 &x, const int4 &y) { return (x.y - x.x) > (y.y - y.x); });
     nitems = (int32_t)it.size();
     nhub = (int32_t)hv.size();
     items.reserve(sizeof(int4) * std::max<size_t>(it.size(), 1));

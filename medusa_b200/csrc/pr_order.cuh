@@ -32,7 +32,7 @@ template <class F>
 __device__ __forceinline__ float pr_warp_block_sum(int64_t j0, int64_t j1, F val) {
     const int lane = threadIdx.x & 31;
     float s = 0.f;
-#pragma unroll 4
+#pragma unroll 8
     for (int64_t j = j0 + lane; j < j1; j += 32) s += val(j);
 #pragma unroll
     for (int off = 16; off; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
