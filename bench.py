@@ -175,6 +175,11 @@ def run_medusa(args):
     p = c2_params(api)
     g = ctx.generate(p)
     V = g.V
+    tuned = {}
+    if not args.no_autotune:
+        # launch and routing parameters for this graph (results never change)
+        from medusa_b200 import autotune
+        tuned.update(autotune.tune_traversals(ctx, g, 0)[0])
     lv_dev = torch.empty(V, dtype=torch.int32, device=dev)
     d_dev = torch.empty(V, dtype=torch.float32, device=dev)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
@@ -243,7 +248,8 @@ def run_medusa(args):
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "schedule_policy": "fixed (direction-optimising rule)",
                    "loop": ("host-driven loop (one flag read per superstep)" if args.hostloop
-                            else "one CUDA graph per BSP loop (device-side convergence)")},
+                            else "one CUDA graph per BSP loop (device-side convergence)"),
+                   "autotuned": {k: int(v) for k, v in tuned.items()}},
         "bfs": {"gteps": round(sb_last["edges_traversed"] / sb_last["device_ms"] / 1e6, 3),
                 "ms": round(sb_last["device_ms"], 4), "supersteps": sb_last["supersteps"],
                 "edges_traversed": sb_last["edges_traversed"],
@@ -273,6 +279,8 @@ def run_medusa(args):
     if not args.no_pagerank:
         out["pagerank"] = bench_pagerank(ctx, api, args, flush)
     g.close()
+    for k in api.TUNABLES:  # each configuration tunes its own
+        ctx.set_tunable(k, -1)
     if not args.no_configs and not args.no_forms:  # C5's learned arm needs the trained models
         out["configs"] = bench_configs(ctx, api, args, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -382,13 +390,14 @@ def bench_configs(ctx, api, args, flush):
     """The other configurations: C3 road-like grid, C4a batched sources on a
     2^22-vertex R-MAT, C5 2^24-vertex R-MAT at scale (fixed vs learned)."""
     import torch
-    from medusa_b200 import scheduler
+    from medusa_b200 import autotune, scheduler
     pk, _ = peaks()
     reps = max(1, min(args.steps, 3))
     out = {}
     # C3: 1448x1448 grid, 10% of the edges dropped, 0.5% shortcuts, weights [1,100]
     g = ctx.generate(api.grid_params(1448, 1448, 0.1, 0.005, seed=SEED, wmin=1, wmax=100))
     V = g.V
+    tuned3 = {} if args.no_autotune else autotune.tune_traversals(ctx, g, 0, reps=2)[0]
     lv = torch.empty(V, dtype=torch.int32, device="cuda")
     dd = torch.empty(V, dtype=torch.float32, device="cuda")
     for _ in range(2):
@@ -400,8 +409,11 @@ def bench_configs(ctx, api, args, flush):
                                   "int [1,100], seed 1, source 0 (corner)",
                       "vertices": V, "edges": g.E,
                       "bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
-                      "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk)}
+                      "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk),
+                      "autotuned": {k: int(v) for k, v in tuned3.items()}}
     g.close()
+    for k in tuned3:
+        ctx.set_tunable(k, -1)
     del lv, dd
     # C4a: 64 BFS + 32 SSSP sources on R-MAT 2^22 / 2^26, batched vs one loop per source
     g = ctx.generate(api.rmat_params(22, 1 << 26, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000))
@@ -433,6 +445,7 @@ def bench_configs(ctx, api, args, flush):
     # C5: R-MAT 2^24 / 2^28, (0.57,0.19,0.19,0.05), weights [1,1000]; fixed vs learned
     g = ctx.generate(api.rmat_params(24, 1 << 28, 0.57, 0.19, 0.19, seed=SEED, wmin=1, wmax=1000))
     V, E = g.V, g.E
+    tuned5 = {} if args.no_autotune else autotune.tune_traversals(ctx, g, 0, reps=2)[0]
     lv = torch.empty(V, dtype=torch.int32, device="cuda")
     dd = torch.empty(V, dtype=torch.float32, device="cuda")
     rk = torch.empty(V, dtype=torch.float32, device="cuda")
@@ -466,21 +479,27 @@ def bench_configs(ctx, api, args, flush):
                       "edges_per_s": round(E / (per / 1e3), 1),
                       "roofline": {"achieved_gbs": round(b / (per / 1e3) / 1e9, 1),
                                    "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}}
+    c5["autotuned"] = {k: int(v) for k, v in tuned5.items()}
     out["c5_scale"] = c5
     g.close()
+    for k in tuned5:
+        ctx.set_tunable(k, -1)
     del lv, dd, rk
-    out["c4b_many_graphs"] = bench_many_graphs(ctx, api, reps)
+    out["c4b_many_graphs"] = bench_many_graphs(ctx, api, reps, not args.no_autotune)
     return out
 
 
-def bench_many_graphs(ctx, api, reps):
+def bench_many_graphs(ctx, api, reps, tune=True):
     """C4b: 256 R-MAT graphs of uneven sizes, 20 PageRank supersteps + one
     BFS each, in ONE persistent launch vs one library call per graph."""
     import torch
+    from medusa_b200 import autotune
     ps = api.c4b_params(256, seed=SEED)
     b = ctx.batch_generate(ps)
     ranks = torch.empty(b.total_V, dtype=torch.float32, device="cuda")
     levels = torch.empty(b.total_V, dtype=torch.int32, device="cuda")
+    tuned, table = ({}, []) if not tune else autotune.tune_batch(ctx, b, 20, reps=2, ranks=ranks,
+                                                                levels=levels)
     b.run(20, None, ranks, levels)
     ms = []
     for _ in range(reps):
@@ -511,9 +530,11 @@ def bench_many_graphs(ctx, api, reps):
                                   "edges_per_s": round(edges / (seq_ms / 1e3), 1)},
            "vs_one_call_per_graph": round(seq_ms / one, 3),
            "identical": same,
-           "tunables": {"batch_threads": ctx.get_tunable("batch_threads"),
-                        "batch_edges_per_cta": ctx.get_tunable("batch_edges_per_cta")}}
+           "autotuned": {k: int(v) for k, v in tuned.items()},
+           "autotune_candidates": len(table)}
     b.close()
+    ctx.set_tunable("batch_threads", -1)
+    ctx.set_tunable("batch_edges_per_cta", -1)
     return res
 
 
@@ -613,6 +634,8 @@ def main():
     ap.add_argument("--impl", default="medusa", choices=["medusa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pagerank", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="run with the built-in launch parameters instead of tuned ones")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the C3 grid, C4a batched and C5 at-scale measurements")
     ap.add_argument("--no-forms", action="store_true",

@@ -260,7 +260,9 @@ int mb_scheduler_collect(mb_ctx *ctx, const mb_graph *g, int32_t app, int32_t so
  * softmax of the negated relative times, each sample weighted by its best
  * time.  Arrays may be host or device.
  * *final_loss (nullable) gets the loss after training.  The weights then
- * serve MB_POLICY_LEARNED. */
+ * serve MB_POLICY_LEARNED; the model also records the range of each feature
+ * in the training set, and inside a run it overrides the fixed rule only
+ * on supersteps whose features lie in that range. */
 int mb_scheduler_train(mb_ctx *ctx, int32_t model, const float *features, const float *times,
                        int32_t n, int32_t epochs, float lr, uint64_t seed, float *final_loss);
 /* Number of MLP parameters (row-major w1[32][6], b1[32], w2[32][32], b2[32],
@@ -276,8 +278,10 @@ int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features,
                       const float *times, int32_t n, float *grad_out, float *loss_out);
 /* The schedule the model's weights pick for each of n feature rows (host
  * arrays).  fallback (nullable, host): the rule a run applies, keep
- * fallback[i] (the fixed rule's choice) unless the network's best output
- * beats that schedule's output by more than 1.0. */
+ * fallback[i] (the fixed rule's choice) unless the features lie within the
+ * training range (+- 1/32) and the network's best output beats that
+ * schedule's output by more than 1.0.  Weights set by
+ * mb_scheduler_set_weights have an unbounded range. */
 int mb_scheduler_pick(mb_ctx *ctx, int32_t model, const float *features,
                       const int32_t *fallback, int32_t n, int32_t *out);
 

@@ -1,0 +1,88 @@
+"""Autotuner for the library's launch and routing parameters (MB_TUNE_*).
+
+The tunables change only how fast a run goes, never its result (the tests
+check every path against the oracle), so the tuner simply times candidate
+settings on the caller's own graph with the library's device clock and keeps
+the fastest.  Search: coordinate descent -- one tunable at a time over its
+candidate values, the others held at their best so far -- for `passes`
+rounds.  Every candidate is timed `reps` times after one untimed run (the
+first run after a change rebuilds the loop's CUDA graph); the median counts.
+
+    from medusa_b200 import api, autotune
+    best, table = autotune.tune_sssp(ctx, graph, source=0)   # leaves best set
+"""
+import numpy as np
+
+
+def _median_ms(fn, reps):
+    fn()
+    return float(np.median([fn()["device_ms"] for _ in range(reps)]))
+
+
+def tune(ctx, run, space, reps=3, passes=1):
+    """Coordinate descent over `space` ({tunable name: [values]}); `run()`
+    performs one run and returns its stats.  Leaves the best values set and
+    returns (best {name: value}, [(setting, ms), ...])."""
+    best = {k: ctx.get_tunable(k) for k in space}
+    table = []
+    best_ms = _median_ms(run, reps)
+    table.append((dict(best), best_ms))
+    for _ in range(passes):
+        for name, values in space.items():
+            for v in values:
+                if v == best[name]:
+                    continue
+                ctx.set_tunable(name, v)
+                ms = _median_ms(run, reps)
+                trial = dict(best)
+                trial[name] = v
+                table.append((trial, ms))
+                if ms < best_ms:
+                    best_ms, best[name] = ms, v
+            ctx.set_tunable(name, best[name])
+    return best, table
+
+
+def tune_sssp(ctx, g, source=0, reps=3):
+    """Bitmap-output push threshold and push grid for SSSP on graph g."""
+    E = max(int(g.E), 1)
+    space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
+             "push_blocks_per_sm": [-1, 4, 6, 12, 16]}
+    return tune(ctx, lambda: g.sssp([source])[1], space, reps)
+
+
+def tune_bfs(ctx, g, source=0, reps=3):
+    """Persistent-tail size and the push / per-vertex grids for BFS on g."""
+    space = {"tail_edges": [-1, 4096, 8192, 32768, 65536],
+             "push_blocks_per_sm": [-1, 4, 6, 12, 16],
+             "vertex_blocks_per_sm": [-1, 4, 12, 16]}
+    return tune(ctx, lambda: g.bfs([source])[1], space, reps)
+
+
+def tune_traversals(ctx, g, source=0, reps=3):
+    """Every BFS/SSSP tunable at once, timing one BFS plus one SSSP (the
+    tunables are per context and the two apps share the push grid)."""
+    E = max(int(g.E), 1)
+
+    def run():
+        sb = g.bfs([source])[1]
+        ss = g.sssp([source])[1]
+        return {"device_ms": sb["device_ms"] + ss["device_ms"]}
+
+    space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
+             "tail_edges": [-1, 4096, 65536],
+             "push_blocks_per_sm": [-1, 4, 6, 12, 16],
+             "vertex_blocks_per_sm": [-1, 4, 12, 16]}
+    return tune(ctx, run, space, reps)
+
+
+def tune_batch(ctx, batch, pr_iters=20, reps=3, ranks=None, levels=None):
+    """CTA size and edges per CTA (team size) of the many-graph kernel.
+    ranks/levels: output buffers to reuse (device tensors avoid the copies)."""
+    if ranks is None:
+        ranks = np.empty(batch.total_V, np.float32)
+    if levels is None:
+        levels = np.empty(batch.total_V, np.int32)
+    space = {"batch_threads": [-1, 128, 512],
+             "batch_edges_per_cta": [-1, 1 << 14, 1 << 15, 1 << 17, 1 << 18]}
+    return tune(ctx, lambda: batch.run(pr_iters, None, ranks, levels)[2], space, reps, passes=2)

@@ -115,8 +115,8 @@ int mb_create(int device, mb_ctx **out) {
         MB_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         MB_CUDA(cudaMallocHost((void **)&ctx->c.pinned_small, mb::Context::kSmallBytes));
         for (mb::DevBuf &b : ctx->c.mlp) {
-            b.reserve(sizeof(float) * mb::kMlpParams);
-            MB_CUDA(cudaMemset(b.p, 0, sizeof(float) * mb::kMlpParams));
+            b.reserve(sizeof(float) * mb::kModelFloats);
+            MB_CUDA(cudaMemset(b.p, 0, sizeof(float) * mb::kModelFloats));
         }
     });
     if (rc != MB_OK) {
@@ -296,6 +296,8 @@ int mb_scheduler_set_weights(mb_ctx *ctx, int32_t model, const float *w) {
         use_device(ctx);
         mb::DevBuf &W = model_weights(ctx, model);
         MB_CUDA(cudaMemcpy(W.p, w, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        mb::mlp_set_open_bounds(ctx->c, W.as<float>());
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         model_ready(ctx, model) = true;
     });
 }

@@ -166,6 +166,25 @@ __global__ void k_adam(float *P, const float *G, float *m, float *v, int t, floa
     P[i] -= lr * (mh / (sqrtf(vh) + eps) + wd * P[i]);
 }
 
+// Per-feature range of the training set into P[kBoundsOff ..]: lo then hi
+// (features are >= 0, so their bit patterns order like the values).
+__global__ void k_feat_bounds(const float *X, int32_t n, float *P) {
+    unsigned *lo = (unsigned *)&P[kBoundsOff], *hi = (unsigned *)&P[kBoundsOff + kFeat];
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int f = 0; f < kFeat; f++) {
+            const unsigned b = __float_as_uint(fmaxf(X[(size_t)i * kFeat + f], 0.f));
+            atomicMin(&lo[f], b);
+            atomicMax(&hi[f], b);
+        }
+}
+
+__global__ void k_bounds_init(float *P, float lo, float hi) {
+    if (threadIdx.x < kFeat) {
+        P[kBoundsOff + threadIdx.x] = lo;
+        P[kBoundsOff + kFeat + threadIdx.x] = hi;
+    }
+}
+
 // He-uniform initialisation from a seeded hash (deterministic)
 __global__ void k_mlp_init(float *P, uint64_t seed) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -230,11 +249,19 @@ float mlp_train(Context &ctx, float *P, const float *X_dev, const float *T_dev, 
         MB_CHECK_LAUNCH();
     }
     mlp_grad(ctx, P, X_dev, T_dev, n, G.as<float>(), L.as<float>());
+    k_bounds_init<<<1, 32, 0, s>>>(P, 3.0e38f, 0.f);
+    k_feat_bounds<<<std::max(1, std::min(ctx.num_sms, (n + 255) / 256)), 256, 0, s>>>(X_dev, n, P);
+    MB_CHECK_LAUNCH();
     float loss = 0.f;
     MB_CUDA(cudaMemcpyAsync(&loss, L.p, sizeof(float), cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
     G.release(); M.release(); Vb.release(); L.release();
     return loss;
+}
+
+void mlp_set_open_bounds(Context &ctx, float *P) {
+    k_bounds_init<<<1, 32, 0, ctx.stream>>>(P, -3.0e38f, 3.0e38f);
+    MB_CHECK_LAUNCH();
 }
 
 void mlp_pick(Context &ctx, const float *P, const float *X_dev, const int32_t *fallback_dev,

@@ -17,6 +17,9 @@ void mlp_grad(Context &ctx, const float *P_dev, const float *X_dev, const float 
 // initialisation with full-batch Adam; returns the final loss.
 float mlp_train(Context &ctx, float *P, const float *X_dev, const float *T_dev, int32_t n,
                 int32_t epochs, float lr, uint64_t seed);
+// Training range of a model set from outside (weights given by the caller):
+// unbounded.
+void mlp_set_open_bounds(Context &ctx, float *P);
 // Schedule the MLP with weights P picks for each of n feature rows; with
 // fallback_dev (nullable), the in-run rule: fallback[i] unless the network's
 // best output beats it by kOverrideMargin.

@@ -20,6 +20,12 @@ struct MlpLayout {
     static constexpr int total = b3 + kOut;
 };
 constexpr int kMlpParams = MlpLayout::total;
+// A model's device block: the parameters, then the per-feature range of its
+// training set (lo[kFeat], hi[kFeat]) -- inside a run the network may
+// override the fixed rule only on features inside that range.
+constexpr int kBoundsOff = kMlpParams;
+constexpr int kModelFloats = kMlpParams + 2 * kFeat;
+constexpr float kBoundsSlack = 1.0f / 32.0f;  // one doubling of any count
 
 // Scheduler features of a superstep, all in [0, 1].  Counts are absolute
 // (log2 / 32), not relative to the graph: whether a superstep is latency- or
@@ -61,6 +67,7 @@ __device__ __forceinline__ float warp_allsum_f(float x) {
 struct MlpRegs {
     float w1r[kFeat], w2r[kHid], w3r[kOut];
     float bias1, bias2, bias3;
+    float lo, hi;  // lane i < kFeat: training range of feature i
 };
 
 // Issue every weight load (independent, coalesced); callers start this
@@ -76,13 +83,17 @@ __device__ __forceinline__ void mlp_load_warp(const float *__restrict__ P, MlpRe
     r.bias1 = __ldg(&P[MlpLayout::b1 + lane]);
     r.bias2 = __ldg(&P[MlpLayout::b2 + lane]);
     r.bias3 = __ldg(&P[MlpLayout::b3 + (lane < kOut ? lane : 0)]);
+    r.lo = __ldg(&P[kBoundsOff + (lane < kFeat ? lane : 0)]);
+    r.hi = __ldg(&P[kBoundsOff + kFeat + (lane < kFeat ? lane : 0)]);
 }
 
 // The decision of one full warp (same value in every lane).  Among the
 // schedules whose bit is set in `allowed`, the one with the largest output;
-// with a fallback schedule (>= 0, allowed), that one is kept unless the
-// best output beats it by more than `margin` (logits): the fixed rule stays
-// in charge where the network is not clearly better.
+// with a fallback schedule (>= 0, allowed), that one is kept unless every
+// feature lies within the training range (+- kBoundsSlack) and the best
+// output beats the fallback's by more than `margin` (logits): the fixed rule
+// stays in charge where the network has not seen such a superstep or is not
+// clearly better.
 __device__ inline int mlp_decide_warp(const MlpRegs &r, const float *f, unsigned allowed,
                                       int fallback, float margin) {
     const int lane = threadIdx.x & 31;
@@ -119,8 +130,14 @@ __device__ inline int mlp_decide_warp(const MlpRegs &r, const float *f, unsigned
         }
     }
     if (best >= kOut) best = 0;
-    if (fallback >= 0 && fallback < kOut && ((allowed >> fallback) & 1u) && !(bv - o_fb > margin))
-        return fallback;
+    if (fallback >= 0 && fallback < kOut && ((allowed >> fallback) & 1u)) {
+        float fl = 0.f;
+#pragma unroll
+        for (int i = 0; i < kFeat; i++)
+            if (lane == i) fl = f[i];
+        const bool inside = lane >= kFeat || (fl >= r.lo - kBoundsSlack && fl <= r.hi + kBoundsSlack);
+        if (!__all_sync(0xffffffffu, inside) || !(bv - o_fb > margin)) return fallback;
+    }
     return best;
 }
 

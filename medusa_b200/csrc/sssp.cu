@@ -199,11 +199,14 @@ __global__ void __launch_bounds__(kPushThreads) k_push_edge_bm(SsspArgs a) {
 }
 
 // After k_push_edge_bm: next-frontier bitmap -> next queue (with the
-// claimed-vertex count), clearing the bitmap; one warp per word.
+// claimed-vertex count), clearing the bitmap; one warp per word.  Every
+// vertex taken is stamped as updated in this superstep, as the claim of the
+// queue path does (schedule 6 sends from the stamped vertices).
 __global__ void __launch_bounds__(256) k_nbm2q(SsspArgs a) {
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int nxt = c->cur ^ 1;
+    const int32_t sv = c->step + 1;
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     uint32_t cn = 0;
@@ -214,6 +217,7 @@ __global__ void __launch_bounds__(256) k_nbm2q(SsspArgs a) {
         const int32_t v = (int32_t)(w * 32 + lane);
         const bool in = (word >> lane) & 1u;
         const uint32_t deg = in ? (uint32_t)a.f.outdeg[v] : 0u;
+        if (in) a.stamp[v] = sv;
         cn += in;
         enqueue_warp(in && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
                      pick(a.f.tf, nxt));

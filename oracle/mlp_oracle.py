@@ -90,15 +90,23 @@ def loss_and_grad(P, X, T):
 
 
 OVERRIDE_MARGIN = 1.0
+BOUNDS_SLACK = 1.0 / 32
 
 
-def pick(P, X, fallback=None):
+def pick(P, X, fallback=None, bounds=None):
     """argmax of the outputs; with fallback, keep fallback[i] unless the
-    best output beats its output by more than OVERRIDE_MARGIN."""
+    row's features lie within bounds = (lo[6], hi[6]) +- BOUNDS_SLACK (None:
+    unbounded) and the best output beats the fallback's by more than
+    OVERRIDE_MARGIN."""
+    X = np.asarray(X, np.float64)
     o = forward(P, X)[4]
     best = o.argmax(axis=1)
     if fallback is None:
         return best
     fb = np.asarray(fallback)
     idx = np.arange(len(o))
-    return np.where(o[idx, best] - o[idx, fb] > OVERRIDE_MARGIN, best, fb)
+    ok = o[idx, best] - o[idx, fb] > OVERRIDE_MARGIN
+    if bounds is not None:
+        lo, hi = (np.asarray(b, np.float64) for b in bounds)
+        ok &= ((X >= lo - BOUNDS_SLACK) & (X <= hi + BOUNDS_SLACK)).all(axis=1)
+    return np.where(ok, best, fb)

@@ -1,0 +1,43 @@
+"""The autotuner: it leaves a valid setting behind, and tuned runs return
+the same results as default ones."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tune_traversals_keeps_results(gpu_ctx):
+    from medusa_b200 import api, autotune
+    g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.45, 0.15, 0.15, seed=3, wmin=1, wmax=1000))
+    try:
+        lv0, _ = g.bfs([0])
+        d0, _ = g.sssp([0])
+        best, table = autotune.tune_traversals(gpu_ctx, g, 0, reps=1)
+        assert len(table) > 5
+        for k, v in best.items():
+            assert gpu_ctx.get_tunable(k) == v
+        lv1, _ = g.bfs([0])
+        d1, _ = g.sssp([0])
+        np.testing.assert_array_equal(lv0, lv1)
+        np.testing.assert_array_equal(d0.view(np.uint32), d1.view(np.uint32))
+    finally:
+        g.close()
+        for k in api.TUNABLES:
+            gpu_ctx.set_tunable(k, -1)
+
+
+def test_tune_batch(gpu_ctx):
+    from medusa_b200 import api, autotune
+    b = gpu_ctx.batch_generate([api.rmat_params(s, 8 << s, 0.45, 0.15, 0.15, seed=s)
+                                for s in range(8, 14)])
+    try:
+        r0, l0, _ = b.run(5)
+        best, table = autotune.tune_batch(gpu_ctx, b, 5, reps=1)
+        assert set(best) == {"batch_threads", "batch_edges_per_cta"}
+        r1, l1, _ = b.run(5)
+        np.testing.assert_array_equal(r0.view(np.uint32), r1.view(np.uint32))
+        np.testing.assert_array_equal(l0, l1)
+    finally:
+        b.close()
+        gpu_ctx.set_tunable("batch_threads", -1)
+        gpu_ctx.set_tunable("batch_edges_per_cta", -1)

@@ -284,7 +284,45 @@ def test_sssp_bitmap_output_push(ctx, api, name):
         for i, s in enumerate(c["sources"]):
             d, st = g.sssp([int(s)])
             np.testing.assert_array_equal(d[0], c["sssp_dist"][i])
+        # the bitmap push followed by every other schedule (replayed list
+        # 0, s, 0, s, ...): each must see the frontier the push left
+        s0 = int(c["sources"][0])
+        for other in range(1, 8):
+            ctx.set_replay([0, other] * 64)
+            ctx.set_policy(api.MB_POLICY_ORACLE_BEST)
+            d, st = g.sssp([s0])
+            ctx.set_policy(api.MB_POLICY_FIXED)
+            np.testing.assert_array_equal(d[0], c["sssp_dist"][0], err_msg="0,%d" % other)
     finally:
+        ctx.set_policy(api.MB_POLICY_FIXED)
+        ctx.set_tunable("sssp_bm_push_min", -1)
+        ctx.set_tunable("tail_edges", -1)
+        g.close()
+
+
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "uniform_2k"])
+def test_random_schedule_sequences(ctx, api, name):
+    """Seeded random schedule sequences (replayed), with the bitmap-output
+    push and the persistent tail on and off: every mix of schedules gives
+    the reference's levels and distances (the learned policy can produce
+    any mix)."""
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    rng = np.random.default_rng(11)
+    s0 = int(c["sources"][0])
+    try:
+        for trial in range(6):
+            ctx.set_tunable("sssp_bm_push_min", 1 if trial % 2 == 0 else -1)
+            ctx.set_tunable("tail_edges", 0 if (trial // 2) % 2 == 0 else -1)
+            ctx.set_replay(list(rng.integers(0, 8, 512)))
+            ctx.set_policy(api.MB_POLICY_ORACLE_BEST)
+            lv, _ = g.bfs([s0])
+            d, _ = g.sssp([s0])
+            ctx.set_policy(api.MB_POLICY_FIXED)
+            np.testing.assert_array_equal(lv[0], c["bfs_level"][0], err_msg="bfs trial %d" % trial)
+            np.testing.assert_array_equal(d[0], c["sssp_dist"][0], err_msg="sssp trial %d" % trial)
+    finally:
+        ctx.set_policy(api.MB_POLICY_FIXED)
         ctx.set_tunable("sssp_bm_push_min", -1)
         ctx.set_tunable("tail_edges", -1)
         g.close()

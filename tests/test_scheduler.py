@@ -77,6 +77,23 @@ def test_gpu_pick_matches_oracle(gpu_ctx):
     assert (got_fb != fb).any() and (got_fb == fb).any()
 
 
+@pytest.mark.gpu
+def test_trained_model_keeps_fixed_rule_outside_its_training_range(gpu_ctx):
+    """A model trained on features inside a box falls back to the given
+    (fixed-rule) schedule for rows outside it, in the in-run rule."""
+    rng = np.random.default_rng(9)
+    X = rng.uniform(0.2, 0.4, (400, 6)).astype(np.float32)
+    T = np.full((400, 8), 1.0, np.float32)
+    T[:, 7] = 0.01  # schedule 7 is by far the best inside the box
+    gpu_ctx.scheduler_train(X, T, epochs=400, lr=1e-2, seed=3, model=0)
+    inside = rng.uniform(0.25, 0.35, (50, 6)).astype(np.float32)
+    outside = inside.copy()
+    outside[:, 1] = 0.9  # one feature far outside
+    fb = np.zeros(50, np.int32)
+    assert (gpu_ctx.scheduler_pick(inside, 0, fallback=fb) == 7).all()
+    assert (gpu_ctx.scheduler_pick(outside, 0, fallback=fb) == 0).all()
+
+
 @pytest.fixture(scope="module")
 def trained(gpu_ctx):
     """Both scheduler models trained on traces of two seeds of three
