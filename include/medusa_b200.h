@@ -194,6 +194,30 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
 
+/* Device layout of a graph, for code compiled against the header-only
+ * operator API (include/medusa/medusa.h), whose functor kernels read it in
+ * place.  Pointers stay valid until mb_graph_destroy.  row/col/esrc/wt: the
+ * CSR in the reference's AA edge order (SSSP/EdgeDataType.cu:138-186; esrc is
+ * srcVertexID, wt is null for an unweighted graph); rrow/rcol: the reverse
+ * CSR, whose position j is message slot j; mslot: msgDstID; outdeg:
+ * edge_count (SSSP/VertexDataType.cu:64-85). */
+typedef struct mb_graph_view {
+    int32_t num_vertices;
+    int64_t num_edges;
+    const int32_t *row, *col, *esrc, *rrow, *rcol, *mslot, *outdeg;
+    const float *wt;
+} mb_graph_view;
+int mb_graph_device_view(const mb_graph *g, mb_graph_view *view);
+
+/* Graph from GTgraph text (the reference's on-disk format, read by
+ * GTGraph::get_parition, MultipleGPU/PartitionManager.cu:153-213): "c"
+ * comment lines, one "p <kind> V E" line, "a <src> <dst> <weight>" edge lines
+ * with 1-based ids; edges keep file order (AddEdge order).  The text is
+ * parsed on the GPU (one thread per line) and the graph built on the device.
+ * text: host or device bytes, len bytes long. */
+int mb_graph_from_gtgraph(mb_ctx *ctx, const char *text, int64_t len, uint32_t flags,
+                          mb_graph **out);
+
 /* ---- many graphs in one launch (no reference counterpart) ----------------- */
 /* A batch of independent graphs (reference order), e.g. 256 R-MAT graphs of
  * uneven sizes.  mb_batch_run runs, for every graph, `pr_iters` PageRank

@@ -103,6 +103,7 @@ def _load():
         "mb_batch_vertex_offsets": (ctypes.c_int, [P, P]),
         "mb_batch_run": (ctypes.c_int, [P, P, I32, P, P, P, P]),
         "mb_batch_destroy": (ctypes.c_int, [P]),
+        "mb_graph_from_gtgraph": (ctypes.c_int, [P, P, I64, U32, ctypes.POINTER(P)]),
         "mb_get_tunable": (ctypes.c_int, [P, I32, ctypes.POINTER(ctypes.c_int64)]),
         "mb_scheduler_get_weights": (ctypes.c_int, [P, I32, P]),
         "mb_scheduler_set_weights": (ctypes.c_int, [P, I32, P]),
@@ -447,6 +448,22 @@ class Context:
         _check(lib.mb_graph_from_edges(self.h, int(V), E, _ptr(src) if E else None,
                                        _ptr(dst) if E else None, _ptr(w) if E else None,
                                        flags, ctypes.byref(g)), self.h)
+        return Graph(self, g.value)
+
+    def graph_from_gtgraph(self, text, reference_order=True):
+        """Graph from GTgraph text: bytes, a str path, or a device uint8 tensor
+        (parsed on the GPU)."""
+        if isinstance(text, str):
+            with open(text, "rb") as f:
+                text = f.read()
+        if isinstance(text, (bytes, bytearray)):
+            buf = np.frombuffer(bytes(text), np.uint8)
+            ptr, n = (buf.ctypes.data if len(buf) else None), len(buf)
+        else:
+            ptr, n = _ptr(text), int(text.numel())
+        g = ctypes.c_void_p()
+        flags = MB_ORDER_REFERENCE if reference_order else MB_ORDER_INPUT
+        _check(lib.mb_graph_from_gtgraph(self.h, ptr, n, flags, ctypes.byref(g)), self.h)
         return Graph(self, g.value)
 
     def batch_generate(self, params_list):

@@ -18,6 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmedusa_b200.so")
+APPS_DIR = os.path.join(HERE, "apps")
+APPS_BIN = os.path.join(APPS_DIR, "medusa_apps")
 ROOT = os.path.dirname(HERE)
 NVCC = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
 
@@ -32,7 +34,8 @@ def _sources():
 
 def _headers():
     return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-            + glob.glob(os.path.join(ROOT, "include", "*.h")))
+            + glob.glob(os.path.join(ROOT, "include", "*.h"))
+            + glob.glob(os.path.join(ROOT, "include", "medusa", "*.h")))
 
 
 def _stale(target, deps):
@@ -75,7 +78,25 @@ def build(force=False, jobs=None, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s" % r.stderr[-6000:])
+    build_apps(force)
     return LIB
+
+
+def build_apps(force=False):
+    """The operator-API apps (medusa_b200/apps) -> medusa_b200/apps/medusa_apps,
+    linked against the in-tree library (rpath $ORIGIN/..)."""
+    srcs = glob.glob(os.path.join(APPS_DIR, "*.cu")) + glob.glob(os.path.join(APPS_DIR, "*.cuh"))
+    deps = srcs + [LIB] + glob.glob(os.path.join(ROOT, "include", "medusa", "*.h"))
+    if not force and not _stale(APPS_BIN, deps):
+        return APPS_BIN
+    cmd = ([NVCC, "-std=c++17", "-O3", "-lineinfo"] + ARCH +
+           ["-I", os.path.join(ROOT, "include"), "-I", APPS_DIR,
+            os.path.join(APPS_DIR, "apps_main.cu"), "-o", APPS_BIN,
+            "-L", HERE, "-lmedusa_b200", "-Xlinker", "-rpath,$ORIGIN/.."])
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("apps build failed:\n%s" % r.stderr[-6000:])
+    return APPS_BIN
 
 
 def main(argv=None):

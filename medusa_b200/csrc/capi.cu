@@ -416,6 +416,41 @@ int mb_generate_edges_host(const mb_gen_params *p, int32_t *src, int32_t *dst, f
     });
 }
 
+int mb_graph_device_view(const mb_graph *g, mb_graph_view *v) {
+    if (!g || !v) return set_error(nullptr, MB_ERR_INVALID, "null argument");
+    v->num_vertices = g->g.V;
+    v->num_edges = g->g.E;
+    v->row = g->g.row.as<int32_t>();
+    v->col = g->g.col.as<int32_t>();
+    v->esrc = g->g.esrc.as<int32_t>();
+    v->rrow = g->g.rrow.as<int32_t>();
+    v->rcol = g->g.rcol.as<int32_t>();
+    v->mslot = g->g.mslot.as<int32_t>();
+    v->outdeg = g->g.outdeg.as<int32_t>();
+    v->wt = g->g.weighted ? g->g.wt.as<float>() : nullptr;
+    return MB_OK;
+}
+
+int mb_graph_from_gtgraph(mb_ctx *ctx, const char *text, int64_t len, uint32_t flags,
+                          mb_graph **out) {
+    if (!ctx || !out || (!text && len > 0)) return set_error(ctx, MB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (flags & ~MB_ORDER_REFERENCE) return set_error(ctx, MB_ERR_INVALID, "unknown flags");
+    mb_graph *g = new (std::nothrow) mb_graph();
+    if (!g) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        mb::graph_from_gtgraph(ctx->c, g->g, text, len, flags);
+        g->g.device = ctx->c.device;
+    });
+    if (rc != MB_OK) {
+        mb_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return MB_OK;
+}
+
 int mb_graph_info(const mb_graph *g, int32_t *V, int64_t *E) {
     if (!g) return set_error(nullptr, MB_ERR_INVALID, "null graph");
     if (V) *V = g->g.V;
