@@ -155,6 +155,26 @@ def sssp_bytes(st, V):
     return 12 * st["edges_traversed"] + 20 * st["vertices_reached"] + 4 * V
 
 
+def reset_tunables(ctx, api):
+    for k in api.TUNABLES:
+        ctx.set_tunable(k, -1)
+    ctx.set_sssp_delta(0.0)
+
+
+def reduce_over_ranks(dev_ms, edges, dist=None, device="cpu"):
+    """Replicas: the job's time is the slowest rank's device time and its
+    work the sum of every rank's traversed edges (no data-path collective:
+    each rank runs its own copy of the workload)."""
+    import torch
+    if dist is None:
+        return float(dev_ms), float(edges)
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([edges], dtype=torch.float64, device=device)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
 def run_medusa(args):
     import torch
     from medusa_b200 import api
@@ -209,16 +229,7 @@ def run_medusa(args):
             sb_last, ss_last = sb, ss
         torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
-    t_max = dev_ms
-    if dist:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        e = torch.tensor([edges], dtype=torch.float64, device=dev)
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        edges_all = float(e.item())
-    else:
-        edges_all = float(edges)
+    t_max, edges_all = reduce_over_ranks(dev_ms, edges, dist, dev)
     value = edges_all / (t_max / 1e3) / 1e9
 
     # end to end through the C ABI with pinned host buffers
@@ -249,7 +260,7 @@ def run_medusa(args):
                    "schedule_policy": "fixed (direction-optimising rule)",
                    "loop": ("host-driven loop (one flag read per superstep)" if args.hostloop
                             else "one CUDA graph per BSP loop (device-side convergence)"),
-                   "autotuned": {k: int(v) for k, v in tuned.items()}},
+                   "autotuned": {k: float(v) for k, v in tuned.items()}},
         "bfs": {"gteps": round(sb_last["edges_traversed"] / sb_last["device_ms"] / 1e6, 3),
                 "ms": round(sb_last["device_ms"], 4), "supersteps": sb_last["supersteps"],
                 "edges_traversed": sb_last["edges_traversed"],
@@ -279,8 +290,7 @@ def run_medusa(args):
     if not args.no_pagerank:
         out["pagerank"] = bench_pagerank(ctx, api, args, flush)
     g.close()
-    for k in api.TUNABLES:  # each configuration tunes its own
-        ctx.set_tunable(k, -1)
+    reset_tunables(ctx, api)  # each configuration tunes its own
     if not args.no_configs and not args.no_forms:  # C5's learned arm needs the trained models
         out["configs"] = bench_configs(ctx, api, args, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -410,10 +420,9 @@ def bench_configs(ctx, api, args, flush):
                       "vertices": V, "edges": g.E,
                       "bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
                       "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk),
-                      "autotuned": {k: int(v) for k, v in tuned3.items()}}
+                      "autotuned": {k: float(v) for k, v in tuned3.items()}}
     g.close()
-    for k in tuned3:
-        ctx.set_tunable(k, -1)
+    reset_tunables(ctx, api)
     del lv, dd
     # C4a: 64 BFS + 32 SSSP sources on R-MAT 2^22 / 2^26, batched vs one loop per source
     g = ctx.generate(api.rmat_params(22, 1 << 26, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000))
@@ -479,11 +488,10 @@ def bench_configs(ctx, api, args, flush):
                       "edges_per_s": round(E / (per / 1e3), 1),
                       "roofline": {"achieved_gbs": round(b / (per / 1e3) / 1e9, 1),
                                    "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}}
-    c5["autotuned"] = {k: int(v) for k, v in tuned5.items()}
+    c5["autotuned"] = {k: float(v) for k, v in tuned5.items()}
     out["c5_scale"] = c5
     g.close()
-    for k in tuned5:
-        ctx.set_tunable(k, -1)
+    reset_tunables(ctx, api)
     del lv, dd, rk
     out["c4b_many_graphs"] = bench_many_graphs(ctx, api, reps, not args.no_autotune)
     return out

@@ -331,6 +331,7 @@ class Context:
         _check(lib.mb_create(int(device), ctypes.byref(h)))
         self.h = h
         self.policy = (MB_POLICY_FIXED, 0)
+        self.sssp_delta = 0.0
 
     def close(self):
         if self.h:
@@ -354,6 +355,7 @@ class Context:
     def set_sssp_delta(self, delta):
         """SSSP near-far bucket width (> 0), 0 for plain Bellman-Ford, < 0 per-graph default."""
         _check(lib.mb_set_sssp_delta(self.h, float(delta)), self.h)
+        self.sssp_delta = float(delta)
 
     def set_persistent_tail(self, enable):
         _check(lib.mb_set_persistent_tail(self.h, 1 if enable else 0), self.h)

@@ -19,11 +19,22 @@ def _median_ms(fn, reps):
     return float(np.median([fn()["device_ms"] for _ in range(reps)]))
 
 
+def _get(ctx, name):
+    return ctx.sssp_delta if name == "sssp_delta" else ctx.get_tunable(name)
+
+
+def _set(ctx, name, value):
+    if name == "sssp_delta":  # the near-far bucket width (0: off, -1: per-graph default)
+        ctx.set_sssp_delta(value)
+    else:
+        ctx.set_tunable(name, value)
+
+
 def tune(ctx, run, space, reps=3, passes=1):
     """Coordinate descent over `space` ({tunable name: [values]}); `run()`
     performs one run and returns its stats.  Leaves the best values set and
     returns (best {name: value}, [(setting, ms), ...])."""
-    best = {k: ctx.get_tunable(k) for k in space}
+    best = {k: _get(ctx, k) for k in space}
     table = []
     best_ms = _median_ms(run, reps)
     table.append((dict(best), best_ms))
@@ -32,14 +43,14 @@ def tune(ctx, run, space, reps=3, passes=1):
             for v in values:
                 if v == best[name]:
                     continue
-                ctx.set_tunable(name, v)
+                _set(ctx, name, v)
                 ms = _median_ms(run, reps)
                 trial = dict(best)
                 trial[name] = v
                 table.append((trial, ms))
                 if ms < best_ms:
                     best_ms, best[name] = ms, v
-            ctx.set_tunable(name, best[name])
+            _set(ctx, name, best[name])
     return best, table
 
 
@@ -70,6 +81,7 @@ def tune_traversals(ctx, g, source=0, reps=3):
         return {"device_ms": sb["device_ms"] + ss["device_ms"]}
 
     space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
+             "sssp_delta": [0.0, -1.0, 100.0, 1000.0, 10000.0],
              "tail_edges": [-1, 4096, 65536],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16]}

@@ -24,6 +24,7 @@ def test_tune_traversals_keeps_results(gpu_ctx):
         g.close()
         for k in api.TUNABLES:
             gpu_ctx.set_tunable(k, -1)
+        gpu_ctx.set_sssp_delta(0.0)
 
 
 def test_tune_batch(gpu_ctx):
