@@ -193,6 +193,18 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
  * (MPG/main.cu:148-169, MPG/UserOperators.h:16-43,119-144,175-270). */
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
+/* PageRank summation order.  MB_PR_ORDER_FIXED (default): a fixed order
+ * the same for every schedule -- a sequential fold in message-slot order up
+ * to 64 in-edges (the reference's CPU fold over the AA layout), 4096-edge
+ * warp blocks above; within 1e-5 of the reference on graphs without hubs.
+ * MB_PR_ORDER_REFERENCE: the reference's own MEG layout (vertices sorted by
+ * out-degree with std::sort, column-major edge slots, MedusaRT/GraphConverter.cu
+ * :136-165, MPG/EdgeDataType.cu:45-131) folded sequentially -- the reference's
+ * FP32 result bit for bit, at the cost of serial folds on hubs; the ordering
+ * is built on first use per graph (a host sort of V out-degrees). */
+#define MB_PR_ORDER_FIXED 0
+#define MB_PR_ORDER_REFERENCE 1
+int mb_set_pagerank_order(mb_ctx *ctx, int32_t order);
 
 /* Device layout of a graph, for code compiled against the header-only
  * operator API (include/medusa/medusa.h), whose functor kernels read it in

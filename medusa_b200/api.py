@@ -21,6 +21,7 @@ MB_ORDER_INPUT, MB_ORDER_REFERENCE = 0, 1
 MB_POLICY_FIXED, MB_POLICY_LEARNED, MB_POLICY_FORCED, MB_POLICY_ORACLE_BEST = 0, 1, 2, 3
 MB_GEN_RMAT, MB_GEN_UNIFORM, MB_GEN_GRID = 0, 1, 2
 MB_MODEL_BFS, MB_MODEL_BATCHED, MB_MODEL_SSSP = 0, 1, 2
+MB_PR_ORDER_FIXED, MB_PR_ORDER_REFERENCE = 0, 1
 MB_TUNE_SSSP_BM_PUSH_MIN, MB_TUNE_PUSH_BLOCKS_PER_SM, MB_TUNE_VERTEX_BLOCKS_PER_SM, \
     MB_TUNE_TAIL_EDGES, MB_TUNE_BATCH_THREADS, MB_TUNE_BATCH_EDGES_PER_CTA = 0, 1, 2, 3, 4, 5
 TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_sm": 2,
@@ -97,6 +98,7 @@ def _load():
                                               ctypes.POINTER(F32)]),
         "mb_scheduler_num_params": (I32, []),
         "mb_set_tunable": (ctypes.c_int, [P, I32, ctypes.c_int64]),
+        "mb_set_pagerank_order": (ctypes.c_int, [P, I32]),
         "mb_batch_generate": (ctypes.c_int, [P, I32, P, ctypes.POINTER(P)]),
         "mb_batch_info": (ctypes.c_int, [P, ctypes.POINTER(I32), ctypes.POINTER(I64),
                                          ctypes.POINTER(I64)]),
@@ -432,6 +434,11 @@ class Context:
         v = ctypes.c_int64(0)
         _check(lib.mb_get_tunable(self.h, w, ctypes.byref(v)), self.h)
         return v.value
+
+    def set_pagerank_order(self, order):
+        """MB_PR_ORDER_FIXED (fast, fixed order) or MB_PR_ORDER_REFERENCE (the
+        reference's MEG order, its FP32 result bit for bit)."""
+        _check(lib.mb_set_pagerank_order(self.h, int(order)), self.h)
 
     def set_batching(self, enable):
         _check(lib.mb_set_batching(self.h, 1 if enable else 0), self.h)

@@ -191,6 +191,14 @@ int mb_set_persistent_grid(mb_ctx *ctx, int enable) {
     return MB_OK;
 }
 
+int mb_set_pagerank_order(mb_ctx *ctx, int32_t order) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    if (order != MB_PR_ORDER_FIXED && order != MB_PR_ORDER_REFERENCE)
+        return set_error(ctx, MB_ERR_INVALID, "unknown PageRank order");
+    ctx->c.pr_order = order;
+    return MB_OK;
+}
+
 int mb_set_batching(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.batching = enable != 0;

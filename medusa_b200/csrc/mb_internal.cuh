@@ -134,6 +134,7 @@ struct Context {
     bool batching = true;          // several BFS sources: one masked traversal per 64
     bool replay_then_fixed = false;  // replay policy: fixed rule after the list
     int32_t max_step = -1;           // >= 0: runs stop after this superstep
+    int pr_order = MB_PR_ORDER_FIXED;  // PageRank summation order
     // launch and routing parameters (MB_TUNE_*); -1: the built-in default
     int64_t tunable[MB_NUM_TUNABLES] = {-1, -1, -1, -1, -1, -1};
     uint64_t tune_gen = 0;  // bumped on every change (loop graphs are rebuilt)

@@ -39,7 +39,7 @@ constexpr int kPrThreads = kPrWarps * 32;
 struct PrArgs {
     int32_t V;
     int64_t E;
-    const int32_t *rrow, *rcol, *outdeg, *row, *mslot;
+    const int32_t *rrow, *rcol, *outdeg, *row, *mslot;  // rcol/mslot: of the order in use
     const float *contrib_in;   // rank[u]/outdeg[u] of the previous superstep
     float *contrib_out;
     float *rank_out;
@@ -93,8 +93,9 @@ __global__ void k_hub_finalize(PrArgs a) {
 // Main combine+update: one warp per 32 consecutive vertices.  The warp
 // streams the group's in-edges (contiguous in reverse-CSR order) through a
 // shared-memory window, coalesced; each lane then folds its own vertex's
-// part of the window in order.
-template <bool kFromMsg>
+// part of the window in order.  kAllLight (the reference's MEG order): every
+// vertex, hubs included, is folded sequentially by its lane.
+template <bool kFromMsg, bool kAllLight = false>
 __global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
     __shared__ float win[kPrWarps][kWin];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
             b = a.rrow[v];
             e = a.rrow[v + 1];
         }
-        const bool heavy = valid && (e - b) > kPrLight;
+        const bool heavy = !kAllLight && valid && (e - b) > kPrLight;
         const int64_t g0 = a.rrow[vb], g1 = a.rrow[ve];
         float sum = 0.f;
         // heavy vertices are finished by k_heavy_blocks / k_hub_finalize
@@ -164,7 +165,98 @@ __global__ void k_fill(float *x, int32_t n, float v) {
         x[i] = v;
 }
 
+// MEG order, step 1: edge e (the k-th out-edge of u in reference order) has
+// MEG position colstart[k] + rank[u]; order[pos] = e.
+__global__ void k_meg_scatter(const int32_t *row, const int32_t *esrc, const int32_t *rank,
+                              const int32_t *colstart, int64_t E, uint32_t *order) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = esrc[e];
+        const int32_t k = (int32_t)(e - row[u]);
+        order[(int64_t)colstart[k] + rank[u]] = (uint32_t)e;
+    }
+}
+
+// step 2: (destination, edge) pairs in MEG position order, for the stable
+// sort by destination
+__global__ void k_meg_keys(const uint32_t *order, const int32_t *col, int64_t E, uint32_t *keys) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < E;
+         i += (int64_t)gridDim.x * blockDim.x)
+        keys[i] = (uint32_t)col[order[i]];
+}
+
+// step 3: slot p of the sorted sequence holds edge vals[p]
+__global__ void k_meg_finish(const uint32_t *vals, const int32_t *esrc, int64_t E, int32_t *meg_src,
+                             int32_t *meg_slot) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < E;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t e = vals[p];
+        meg_src[p] = esrc[e];
+        meg_slot[e] = (int32_t)p;
+    }
+}
+
 }  // namespace
+
+void build_meg_order(Context &ctx, const Graph &g, PrState &st) {
+    if (st.meg_built) return;
+    const int32_t V = g.V;
+    const int64_t E = g.E;
+    cudaStream_t s = ctx.stream;
+    std::vector<int32_t> row((size_t)V + 1);
+    MB_CUDA(cudaMemcpy(row.data(), g.row.p, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyDeviceToHost));
+    // GraphIR::sortByDegree: std::sort of the vertices in id order by a
+    // degree-descending comparator.  The permutation std::sort produces
+    // depends only on the comparison results, so sorting (degree, id)
+    // records with the same comparison reproduces the reference's.
+    struct Node {
+        int32_t deg, id;
+    };
+    std::vector<Node> nodes((size_t)V);
+    for (int32_t v = 0; v < V; v++) nodes[v] = Node{row[v + 1] - row[v], v};
+    std::sort(nodes.begin(), nodes.end(), [](const Node &l, const Node &r) { return l.deg > r.deg; });
+    std::vector<int32_t> rank((size_t)V);
+    for (int32_t i = 0; i < V; i++) rank[nodes[i].id] = i;
+    // buildMEG: column k holds the k-th edge of every vertex with more than
+    // k edges, in sorted order; colstart[k] = edges in columns before k
+    const int32_t maxdeg = V ? nodes[0].deg : 0;
+    std::vector<int64_t> cnt((size_t)maxdeg + 2, 0);
+    for (int32_t v = 0; v < V; v++) cnt[row[v + 1] - row[v]]++;
+    std::vector<int32_t> colstart((size_t)maxdeg + 1, 0);
+    int64_t above = (int64_t)V - cnt[0], acc = 0;  // vertices with degree > k
+    for (int32_t k = 0; k < maxdeg; k++) {
+        colstart[k] = (int32_t)acc;
+        acc += above;
+        above -= cnt[k + 1];
+    }
+    colstart[maxdeg] = (int32_t)acc;
+    DevBuf d_rank, d_col, order, keys;
+    d_rank.reserve(sizeof(int32_t) * std::max<size_t>(V, 1));
+    d_col.reserve(sizeof(int32_t) * colstart.size());
+    const size_t eb = sizeof(uint32_t) * (size_t)std::max<int64_t>(E, 1);
+    order.reserve(eb);
+    keys.reserve(eb);
+    st.meg_src.reserve(eb);
+    st.meg_slot.reserve(eb);
+    MB_CUDA(cudaMemcpyAsync(d_rank.p, rank.data(), sizeof(int32_t) * (size_t)V, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(d_col.p, colstart.data(), sizeof(int32_t) * colstart.size(), cudaMemcpyHostToDevice, s));
+    if (E > 0) {
+        const int grid = grid_for(E, 256, ctx.num_sms * 16);
+        k_meg_scatter<<<grid, 256, 0, s>>>(g.row.as<int32_t>(), g.esrc.as<int32_t>(), d_rank.as<int32_t>(),
+                                           d_col.as<int32_t>(), E, order.as<uint32_t>());
+        k_meg_keys<<<grid, 256, 0, s>>>(order.as<uint32_t>(), g.col.as<int32_t>(), E, keys.as<uint32_t>());
+        MB_CHECK_LAUNCH();
+        int bits = 1;
+        while (bits < 32 && ((int64_t)1 << bits) < (int64_t)V) bits++;
+        radix_sort_pairs(ctx, keys.as<uint32_t>(), order.as<uint32_t>(), E, bits, s);
+        k_meg_finish<<<grid, 256, 0, s>>>(order.as<uint32_t>(), g.esrc.as<int32_t>(), E,
+                                          st.meg_src.as<int32_t>(), st.meg_slot.as<int32_t>());
+        MB_CHECK_LAUNCH();
+    }
+    MB_CUDA(cudaStreamSynchronize(s));
+    d_rank.release(); d_col.release(); order.release(); keys.release();
+    st.meg_built = true;
+}
 
 void PrState::ensure(Context &ctx, const Graph &g) {
     if (built && V == g.V && E == g.E) return;
@@ -216,6 +308,8 @@ void PrState::ensure(Context &ctx, const Graph &g) {
 void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init, int sched,
                   mb_stats *stats) {
     st.ensure(ctx, g);
+    const bool ref_order = ctx.pr_order == MB_PR_ORDER_REFERENCE;
+    if (ref_order) build_meg_order(ctx, g, st);
     cudaStream_t s = ctx.stream;
     const bool unfused = sched == MB_SCHED_PUSH_UNFUSED;
     auto args = [&](int parity) {
@@ -223,10 +317,10 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         a.V = g.V;
         a.E = g.E;
         a.rrow = g.rrow.as<int32_t>();
-        a.rcol = g.rcol.as<int32_t>();
+        a.rcol = ref_order ? st.meg_src.as<int32_t>() : g.rcol.as<int32_t>();
         a.outdeg = g.outdeg.as<int32_t>();
         a.row = g.row.as<int32_t>();
-        a.mslot = g.mslot.as<int32_t>();
+        a.mslot = ref_order ? st.meg_slot.as<int32_t>() : g.mslot.as<int32_t>();
         a.contrib_in = st.contrib[parity].as<float>();
         a.contrib_out = st.contrib[parity ^ 1].as<float>();
         a.rank_out = st.rank.as<float>();
@@ -253,6 +347,13 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         MB_CHECK_LAUNCH();
         for (int it = 0; it < iters; it++) {
             PrArgs a = args(it & 1);
+            if (ref_order) {
+                if (unfused) k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
+                if (unfused) k_pr_pull<true, true><<<grid_pull, kPrThreads, 0, cs>>>(a);
+                else k_pr_pull<false, true><<<grid_pull, kPrThreads, 0, cs>>>(a);
+                MB_CHECK_LAUNCH();
+                continue;
+            }
             if (unfused) {
                 k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
                 if (a.nitems) k_heavy_blocks<true><<<grid_for((int64_t)a.nitems * 32, 256, grid_heavy), 256, 0, cs>>>(a);
@@ -274,7 +375,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     MB_CUDA(cudaEventCreate(&e1));
     try {
         if (ctx.use_graphs) {
-            if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_sched != sched) {
+            if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_sched != sched ||
+                st.g_order != ctx.pr_order) {
                 if (st.exec) cudaGraphExecDestroy(st.exec);
                 st.exec = nullptr;
                 cudaGraph_t gr;
@@ -292,6 +394,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                 st.g_iters = iters;
                 st.g_init = init;
                 st.g_sched = sched;
+                st.g_order = ctx.pr_order;
             }
             MB_CUDA(cudaEventRecord(e0, s));
             MB_CUDA(cudaGraphLaunch(st.exec, s));
@@ -313,7 +416,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             stats->schedule_count[unfused ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE] = iters;
             stats->edges_scanned = (int64_t)iters * g.E;
             stats->kernel_launches =
-                1 + (int64_t)iters * (1 + (st.nitems > 0) + (st.nhub > 0) + unfused) + (iters == 0);
+                ref_order ? 1 + (int64_t)iters * (1 + unfused) + (iters == 0)
+                          : 1 + (int64_t)iters * (1 + (st.nitems > 0) + (st.nhub > 0) + unfused) + (iters == 0);
         }
     } catch (...) {
         cudaEventDestroy(e0);

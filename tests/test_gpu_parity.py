@@ -87,6 +87,27 @@ def test_pagerank_matches_reference(ctx, name):
     g.close()
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_pagerank_reference_order_is_the_reference_bit_for_bit(ctx, api, name):
+    """MB_PR_ORDER_REFERENCE replays GraphIR::sortByDegree + buildMEG: the
+    ranks equal the reference's own FP32 output (the golden fixture made by
+    its CPU path over the MEG layout), hubs included, for both PageRank
+    schedules."""
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
+    try:
+        for sched in (0, 6):
+            ctx.set_policy(api.MB_POLICY_FORCED, sched)
+            r, _ = g.pagerank(c["pr_iters"], 1.0 / c["V"])
+            np.testing.assert_array_equal(r.view(np.uint32), c["pr_rank"].view(np.uint32),
+                                          err_msg="schedule %d" % sched)
+    finally:
+        ctx.set_policy(api.MB_POLICY_FIXED)
+        ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
+        g.close()
+
+
 @pytest.mark.parametrize("name", ["tiny", "rmat_s10", "grid_24", "hub", "uniform_2k"])
 def test_every_schedule_bit_identical(gpu_ctx, api, name):
     c = load_golden(name)
