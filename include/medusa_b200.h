@@ -230,6 +230,19 @@ int mb_graph_device_view(const mb_graph *g, mb_graph_view *view);
 int mb_graph_from_gtgraph(mb_ctx *ctx, const char *text, int64_t len, uint32_t flags,
                           mb_graph **out);
 
+/* ---- visualisation coordinates, headless ---------------------------------- */
+/* The reference renders vertices as quads and edges as lines through OpenGL
+ * vertex buffers (MedusaRT/GraphRenderingAPI.cu:33-44 DrawNodes, :69-78
+ * DrawEdges).  No graphics stack is used here: the same coordinates are
+ * written to caller buffers (host or device).
+ * mb_vis_node_quads: pos[2V] (x, y per vertex), radius[V] ->
+ *   quads[8V] = (x-r, y+r-1), (x+r-1, y+r-1), (x+r-1, y-r), (x-r, y-r).
+ * mb_vis_edge_lines: pos[2V] -> lines[4E] = (pos[src], pos[dst]) per edge in
+ *   the graph's edge order (the reference's edge array order). */
+int mb_vis_node_quads(mb_ctx *ctx, int32_t num_vertices, const float *pos, const int32_t *radius,
+                      float *quads_out);
+int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *lines_out);
+
 /* ---- many graphs in one launch (no reference counterpart) ----------------- */
 /* A batch of independent graphs (reference order), e.g. 256 R-MAT graphs of
  * uneven sizes.  mb_batch_run runs, for every graph, `pr_iters` PageRank

@@ -99,6 +99,8 @@ def _load():
         "mb_scheduler_num_params": (I32, []),
         "mb_set_tunable": (ctypes.c_int, [P, I32, ctypes.c_int64]),
         "mb_set_pagerank_order": (ctypes.c_int, [P, I32]),
+        "mb_vis_node_quads": (ctypes.c_int, [P, I32, P, P, P]),
+        "mb_vis_edge_lines": (ctypes.c_int, [P, P, P, P]),
         "mb_batch_generate": (ctypes.c_int, [P, I32, P, ctypes.POINTER(P)]),
         "mb_batch_info": (ctypes.c_int, [P, ctypes.POINTER(I32), ctypes.POINTER(I64),
                                          ctypes.POINTER(I64)]),
@@ -254,6 +256,13 @@ class Graph:
         _check(lib.mb_sssp(self.ctx.h, self.h, src.ctypes.data, len(src), _ptr(out),
                            ctypes.byref(st)), self.ctx.h)
         return out, st.as_dict()
+
+    def vis_edge_lines(self, pos):
+        """Endpoints of every edge (DrawEdges) in edge order: pos [V,2] -> [E,2,2]."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        out = np.empty((self.E, 2, 2), np.float32)
+        _check(lib.mb_vis_edge_lines(self.ctx.h, self.h, pos.ctypes.data, out.ctypes.data), self.ctx.h)
+        return out
 
     def pagerank(self, iters, init=None, out=None):
         if init is None:
@@ -434,6 +443,16 @@ class Context:
         v = ctypes.c_int64(0)
         _check(lib.mb_get_tunable(self.h, w, ctypes.byref(v)), self.h)
         return v.value
+
+    def vis_node_quads(self, pos, radius):
+        """Quad corners of every vertex (DrawNodes): pos [V,2] float32, radius
+        [V] int32 -> [V,4,2] float32."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        radius = np.ascontiguousarray(radius, np.int32)
+        out = np.empty((len(radius), 4, 2), np.float32)
+        _check(lib.mb_vis_node_quads(self.h, len(radius), pos.ctypes.data, radius.ctypes.data,
+                                     out.ctypes.data), self.h)
+        return out
 
     def set_pagerank_order(self, order):
         """MB_PR_ORDER_FIXED (fast, fixed order) or MB_PR_ORDER_REFERENCE (the

@@ -24,6 +24,8 @@ struct AppStates {
 };
 int64_t generate_edges_host(const mb_gen_params &p, int32_t *src, int32_t *dst, float *w);
 void graph_generate(Context &ctx, Graph &g, const mb_gen_params &p, uint32_t flags);
+void vis_node_quads(Context &ctx, int32_t V, const float *pos, const int32_t *radius, float *quads);
+void vis_edge_lines(Context &ctx, const Graph &g, const float *pos, float *lines);
 }  // namespace mb
 
 struct mb_ctx {
@@ -189,6 +191,50 @@ int mb_set_persistent_grid(mb_ctx *ctx, int enable) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     ctx->c.persist = enable != 0;
     return MB_OK;
+}
+
+namespace {
+// n bytes from host or device memory into a device buffer (returns the pointer to use)
+const void *stage_in(mb::DevBuf &b, const void *p, size_t n) {
+    if (mb::is_device_ptr(p)) return p;
+    b.reserve(std::max<size_t>(n, 1));
+    if (n) MB_CUDA(cudaMemcpy(b.p, p, n, cudaMemcpyHostToDevice));
+    return b.p;
+}
+}  // namespace
+
+int mb_vis_node_quads(mb_ctx *ctx, int32_t V, const float *pos, const int32_t *radius, float *quads) {
+    return guarded(ctx, [&] {
+        if (!ctx || V < 0 || (V > 0 && (!pos || !radius || !quads))) mb::fail(MB_ERR_INVALID, "bad arguments");
+        use_device(ctx);
+        mb::DevBuf bp, br, bq;
+        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)V);
+        const int32_t *dr = (const int32_t *)stage_in(br, radius, sizeof(int32_t) * (size_t)V);
+        float *dq = quads;
+        const bool dev_out = mb::is_device_ptr(quads);
+        if (!dev_out) dq = (float *)bq.reserve(sizeof(float) * 8 * std::max<size_t>(V, 1));
+        mb::vis_node_quads(ctx->c, V, dp, dr, dq);
+        if (!dev_out && V)
+            MB_CUDA(cudaMemcpyAsync(quads, dq, sizeof(float) * 8 * (size_t)V, cudaMemcpyDeviceToHost, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *lines) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, g);
+        if (!pos || !lines) mb::fail(MB_ERR_INVALID, "bad arguments");
+        use_device(ctx);
+        mb::DevBuf bp, bl;
+        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)g->g.V);
+        float *dl = lines;
+        const bool dev_out = mb::is_device_ptr(lines);
+        const size_t nb = sizeof(float) * 4 * (size_t)g->g.E;
+        if (!dev_out) dl = (float *)bl.reserve(std::max<size_t>(nb, 16));
+        mb::vis_edge_lines(ctx->c, g->g, dp, dl);
+        if (!dev_out && nb) MB_CUDA(cudaMemcpyAsync(lines, dl, nb, cudaMemcpyDeviceToHost, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
 }
 
 int mb_set_pagerank_order(mb_ctx *ctx, int32_t order) {

@@ -15,7 +15,7 @@ def test_tune_traversals_keeps_results(gpu_ctx):
         best, table = autotune.tune_traversals(gpu_ctx, g, 0, reps=1)
         assert len(table) > 5
         for k, v in best.items():
-            assert gpu_ctx.get_tunable(k) == v
+            assert autotune._get(gpu_ctx, k) == v
         lv1, _ = g.bfs([0])
         d1, _ = g.sssp([0])
         np.testing.assert_array_equal(lv0, lv1)
