@@ -155,6 +155,60 @@ def sssp_bytes(st, V):
     return 12 * st["edges_traversed"] + 20 * st["vertices_reached"] + 4 * V
 
 
+BRANCH_KERNELS = {0: "k_push_edge_q", 1: "k_push_warp_q", 4: "k_pull_stream", 5: "k_pull_warp",
+                  6: "reference split", 7: "full pull", 17: "k_tail", 19: "k_push_edge_bm + k_nbm2q"}
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dominant_kernel_traffic.md")
+
+
+def measured_traffic_ratio(kernel):
+    """DRAM bytes per algorithmic byte of `kernel`, from the committed ncu
+    summary (a line "| <kernel> | ... | <ratio> |" in its table), or None."""
+    try:
+        for line in open(TRAFFIC_FILE):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 2 and cells[0] == kernel:
+                return float(cells[-1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def kernel_roofline(ctx, g, V, pk, pk_kind):
+    """The dominant kernel of one BFS + one SSSP: every superstep's branch
+    timed alone (CUDA events, host-driven loop), algorithmic bytes per
+    superstep from its frontier (BFS 8 B per frontier out-edge + 20 B per
+    frontier vertex, SSSP 12 + 20), the branch with the largest total time."""
+    ctx.set_tracing(True)
+    try:
+        g.bfs([0])
+        g.sssp([0])
+        tr = ctx.get_trace()
+    finally:
+        ctx.set_tracing(False)
+    per = {}
+    for r in tr:
+        per_edge = 8 if r["app"] == 0 else 12
+        key = (int(r["app"]), int(r["branch"]))
+        ms, b, n = per.get(key, (0.0, 0.0, 0))
+        per[key] = (ms + float(r["ms"]),
+                    b + per_edge * float(r["frontier_edges"]) + 20.0 * float(r["frontier_vertices"]),
+                    n + 1)
+    (app, br), (ms, byts, n) = max(per.items(), key=lambda kv: kv[1][0])
+    name = BRANCH_KERNELS.get(br % 8 if br < 16 else br, "branch %d" % br)
+    achieved = byts / (ms / 1e3) / 1e9
+    ratio = measured_traffic_ratio(name)
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk, "unit": "GB/s",
+            "frac": round(achieved / pk, 4),
+            "traffic": None if ratio is None else round(ratio * byts / n),
+            "peak_kind": pk_kind,
+            "kernel": "%s (%s, branch %d)" % (name, ("BFS", "SSSP")[app], br),
+            "launches": n, "avg_launch_ms": round(ms / n, 4),
+            "algorithmic_bytes_per_launch": round(byts / n),
+            "share_of_traced_time": round(ms / sum(v[0] for v in per.values()), 3),
+            "traffic_source": None if ratio is None else
+            "DRAM bytes / algorithmic bytes of this kernel from profiles/dominant_kernel_traffic.md"}
+
+
 def reset_tunables(ctx, api):
     for k in api.TUNABLES:
         ctx.set_tunable(k, -1)
@@ -274,13 +328,14 @@ def run_medusa(args):
                  "edges_scanned": ss_last["edges_scanned"]},
         "e2e": {"value": round(e2e_val, 3), "unit": "GTEPS", "h2d_bytes_per_step": 8,
                 "d2h_bytes_per_step": 8 * V},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk,
-                     "unit": "GB/s", "frac": round(achieved / pk, 4), "traffic": None,
-                     "peak_kind": pk_kind,
-                     "kernel": "BFS + SSSP superstep loops (one CUDA graph each)",
-                     "bytes_per_step": {"bfs": round(bfs_gb, 4), "sssp": round(sssp_gb, 4),
-                                        "unit": "GB",
-                                        "formula": "BFS 8*E_r+20*V_r+4*V; SSSP 12*E_r+20*V_r+4*V"}},
+        "roofline": kernel_roofline(ctx, g, V, pk, pk_kind),
+        "roofline_loops": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk,
+                           "unit": "GB/s", "frac": round(achieved / pk, 4),
+                           "peak_kind": pk_kind,
+                           "what": "BFS + SSSP superstep loops (one CUDA graph each), whole step",
+                           "bytes_per_step": {"bfs": round(bfs_gb, 4), "sssp": round(sssp_gb, 4),
+                                              "unit": "GB",
+                                              "formula": "BFS 8*E_r+20*V_r+4*V; SSSP 12*E_r+20*V_r+4*V"}},
         "gpu_launches": int(launches),
         "wall_s": round(wall, 3),
         "clocks": clk.summary(),

@@ -64,9 +64,11 @@ class Stats(ctypes.Structure):
 
 
 def _load():
-    if not os.path.exists(LIB_PATH):
+    # MEDUSA_B200_LIB: another build of the library (a variant for comparisons)
+    path = os.environ.get("MEDUSA_B200_LIB", LIB_PATH)
+    if not os.path.exists(path):
         raise ImportError("libmedusa_b200.so is not built: run `python -m medusa_b200.build`")
-    lib = ctypes.CDLL(LIB_PATH)
+    lib = ctypes.CDLL(path)
     P, I32, I64, U32, F32 = (ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32,
                              ctypes.c_float)
     sigs = {
@@ -99,6 +101,8 @@ def _load():
         "mb_scheduler_num_params": (I32, []),
         "mb_set_tunable": (ctypes.c_int, [P, I32, ctypes.c_int64]),
         "mb_set_pagerank_order": (ctypes.c_int, [P, I32]),
+        "mb_set_tracing": (ctypes.c_int, [P, ctypes.c_int]),
+        "mb_get_trace": (ctypes.c_int, [P, P, I32, ctypes.POINTER(I32)]),
         "mb_vis_node_quads": (ctypes.c_int, [P, I32, P, P, P]),
         "mb_vis_edge_lines": (ctypes.c_int, [P, P, P, P]),
         "mb_batch_generate": (ctypes.c_int, [P, I32, P, ctypes.POINTER(P)]),
@@ -453,6 +457,20 @@ class Context:
         _check(lib.mb_vis_node_quads(self.h, len(radius), pos.ctypes.data, radius.ctypes.data,
                                      out.ctypes.data), self.h)
         return out
+
+    TRACE_DTYPE = np.dtype([("app", np.int32), ("step", np.int32), ("sched", np.int32),
+                            ("branch", np.int32), ("frontier_vertices", np.uint32),
+                            ("frontier_edges", np.uint64), ("ms", np.float32)], align=True)
+
+    def set_tracing(self, enable):
+        """Host-driven loops with every superstep timed alone (CUDA events)."""
+        _check(lib.mb_set_tracing(self.h, 1 if enable else 0), self.h)
+
+    def get_trace(self, max_records=1 << 16):
+        out = np.zeros(max_records, self.TRACE_DTYPE)
+        n = ctypes.c_int32(0)
+        _check(lib.mb_get_trace(self.h, out.ctypes.data, max_records, ctypes.byref(n)), self.h)
+        return out[:n.value].copy()
 
     def set_pagerank_order(self, order):
         """MB_PR_ORDER_FIXED (fast, fixed order) or MB_PR_ORDER_REFERENCE (the

@@ -45,8 +45,15 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, jobs=None, verbose=False):
-    """Compile (when stale) and return the path of the shared library."""
+def build(force=False, jobs=None, verbose=False, defines=(), out_dir=None):
+    """Compile (when stale) and return the path of the shared library.
+    defines/out_dir: a variant build (e.g. ["MB_TILE_EDGES=2048"]) into its own
+    directory, for comparisons; the default build is the product."""
+    global OBJ, LIB
+    if out_dir:
+        OBJ = os.path.join(out_dir, "_build")
+        LIB = os.path.join(out_dir, "libmedusa_b200.so")
+    extra = [f for d in defines for f in ("-D", d)]
     os.makedirs(OBJ, exist_ok=True)
     srcs = _sources()
     hdrs = _headers()
@@ -60,7 +67,7 @@ def build(force=False, jobs=None, verbose=False):
 
     def cc(job):
         s, o = job
-        cmd = [NVCC] + NVFLAGS + ["-c", s, "-o", o]
+        cmd = [NVCC] + NVFLAGS + extra + ["-c", s, "-o", o]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -78,7 +85,8 @@ def build(force=False, jobs=None, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s" % r.stderr[-6000:])
-    build_apps(force)
+    if not out_dir:
+        build_apps(force)
     return LIB
 
 

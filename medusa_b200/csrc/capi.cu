@@ -237,6 +237,24 @@ int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *l
     });
 }
 
+int mb_set_tracing(mb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
+    ctx->c.tracing = enable != 0;
+    ctx->c.trace.clear();
+    return MB_OK;
+}
+
+int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out) {
+    if (!ctx || !n_out || max < 0 || (max > 0 && !out)) return set_error(ctx, MB_ERR_INVALID, "bad arguments");
+    const int32_t n = (int32_t)std::min<size_t>(ctx->c.trace.size(), (size_t)max);
+    for (int32_t i = 0; i < n; i++) {
+        const auto &r = ctx->c.trace[i];
+        out[i] = mb_trace_rec{r.app, r.step, r.sched, r.branch, r.n, r.m, r.ms};
+    }
+    *n_out = n;
+    return MB_OK;
+}
+
 int mb_set_pagerank_order(mb_ctx *ctx, int32_t order) {
     if (!ctx) return set_error(nullptr, MB_ERR_INVALID, "null context");
     if (order != MB_PR_ORDER_FIXED && order != MB_PR_ORDER_REFERENCE)

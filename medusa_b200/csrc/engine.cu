@@ -42,7 +42,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
     MB_CUDA(cudaEventCreate(&e0));
     MB_CUDA(cudaEventCreate(&e1));
     try {
-        if (ctx.use_graphs) {
+        if (ctx.use_graphs && !ctx.tracing) {
             if (!st.lg.exec || st.owner != (const void *)&ctx || st.owner_mlp != (const void *)fa.mlp ||
                 st.owner_gen != ctx.tune_gen) {
                 const int cap = sp.cap, app = sp.app;
@@ -83,6 +83,8 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
                     r.step = hc->step;
                     r.sched = hc->sched;
                     r.branch = hc->branch;
+                    r.n = hc->front_n;
+                    r.m = hc->front_m;
                     for (int i = 0; i < 8; i++) r.feat[i] = hc->feat[i];
                     MB_CUDA(cudaEventRecord(t0, s));
                     sp.branch(hc->branch, s);

@@ -23,7 +23,10 @@ template <class T>
 __device__ __forceinline__ T ldg2(const T *p) { return __ldcg(p); }
 
 
-constexpr int kTile = 1024;          // edges per merge-path tile
+#ifndef MB_TILE_EDGES
+#define MB_TILE_EDGES 512
+#endif
+constexpr int kTile = MB_TILE_EDGES;  // edges per merge-path tile
 constexpr int kPushThreads = 256;    // threads per push CTA
 constexpr int kTileItems = kTile / kPushThreads;
 

@@ -147,6 +147,8 @@ struct Context {
         int32_t app, step, sched, branch;
         float feat[8];
         float ms;
+        uint32_t n;  // frontier vertices and out-edges the superstep started from
+        uint64_t m;
     };
     std::vector<TraceRec> trace;
     void *ctrl_readback() { return pinned_small + kCtrlOff; }

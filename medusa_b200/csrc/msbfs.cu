@@ -597,6 +597,8 @@ void run_msbfs(Context &ctx, Graph &g, MsBfsState &st, const int32_t *sources, i
                     r.step = hc->step;
                     r.sched = hc->sched;
                     r.branch = hc->branch;
+                    r.n = hc->active;
+                    r.m = hc->active_edges;
                     for (int i = 0; i < 8; i++) r.feat[i] = hc->feat[i];
                     MB_CUDA(cudaEventRecord(t0, s));
                     branch(hc->branch, s);
