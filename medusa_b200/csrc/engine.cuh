@@ -144,12 +144,23 @@ __device__ inline int route(const Ctrl *c, int s) {
     return branch_of(s, c->mode);
 }
 
+// Counters other CTAs updated with atomics: read at L2 (kL2) where those
+// CTAs may still be running (the persistent kernels), a plain load in the
+// select kernel (every superstep kernel has finished; its bookkeeping reads
+// the control block after one warp-wide prefetch into L1).
+template <bool kL2, class T>
+__device__ __forceinline__ T ctl_ld(const T *p) {
+    if (kL2) return ldg2(p);
+    return *p;
+}
+
 // Decide the next superstep from the current frontier (one thread).
+template <bool kL2 = true>
 __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     uint32_t n;
     uint64_t m;
     if (c->mode == FMT_QUEUE) {
-        const unsigned long long q = ldg2(&c->q[c->cur]);
+        const unsigned long long q = ctl_ld<kL2>(&c->q[c->cur]);
         n = (uint32_t)(q >> 32);
         m = (uint32_t)q;
     } else {
@@ -163,7 +174,7 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
         return;
     }
     if (n == 0 || m == 0) {  // nothing left to expand
-        if (app == APP_SSSP && ldg2(&c->far_n[c->fcur]) > 0) {
+        if (app == APP_SSSP && ctl_ld<kL2>(&c->far_n[c->fcur]) > 0) {
             // near-far: next bucket
             c->thresh += c->p.delta;
             c->sched = kSchedSplit;
@@ -190,7 +201,8 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     c->branch = route(c, s);
 }
 
-// Called by thread 0 of the last CTA of a superstep kernel.
+// Bookkeeping after a superstep (one thread).
+template <bool kL2 = true>
 __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, int out_fmt) {
     if (c->sched == kSchedSplit) {
         c->splits++;
@@ -203,9 +215,9 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
         c->work += c->sched <= MB_SCHED_PUSH_WARP_BITMAP ? c->front_m : (uint64_t)E;
     }
     // accumulators and queue counters were updated with atomics
-    const uint32_t acc_n = ldg2(&c->acc_n);
-    const uint64_t acc_m = ldg2((const unsigned long long *)&c->acc_m);
-    const unsigned long long qn = ldg2(&c->q[c->cur ^ 1]);
+    const uint32_t acc_n = ctl_ld<kL2>(&c->acc_n);
+    const uint64_t acc_m = ctl_ld<kL2>((const unsigned long long *)&c->acc_m);
+    const unsigned long long qn = ctl_ld<kL2>(&c->q[c->cur ^ 1]);
     if (app == APP_BFS) {  // claimed vertices and their out-edges
         c->reached += acc_n;
         c->edges_reached += out_fmt == FMT_QUEUE ? (uint32_t)qn : acc_m;
@@ -232,7 +244,7 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
         c->n_unvisited -= (int64_t)c->nf;
     }
     c->step++;
-    choose_next(c, app, V, E);
+    choose_next<kL2>(c, app, V, E);
     if (out_fmt != FMT_QUEUE) c->prev_nf = c->nf;
 }
 
@@ -311,12 +323,22 @@ __device__ __forceinline__ uint32_t tail_mask(int64_t w, int32_t V) {
 // MLP on the features it left.
 __device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
     Ctrl *c = a.ctrl;
+    {
+        // the control block's lines and the run parameters' head, all at once
+        const int lane = threadIdx.x & 31;
+        const char *hot = (const char *)&c->q[0];
+        const size_t hot_bytes = sizeof(Ctrl) - offsetof(Ctrl, q);
+        if ((size_t)lane * 128 < hot_bytes)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(hot + (size_t)lane * 128));
+        if (lane == 31) asm volatile("prefetch.global.L1 [%0];" ::"l"((const char *)&c->p));
+        __syncwarp();
+    }
     const bool use_mlp = a.mlp && c->p.policy == MB_POLICY_LEARNED;  // warp-uniform
     MlpRegs r;
     if (use_mlp) mlp_load_warp(a.mlp, r);  // in flight during the bookkeeping
     if ((threadIdx.x & 31) == 0 && c->pending) {
         c->pending = 0;
-        finish_superstep(c, app, a.V, a.E, sched_output(c->sched));
+        finish_superstep<false>(c, app, a.V, a.E, sched_output(c->sched));
     }
     __syncwarp();
     const bool learned = use_mlp && !c->done && c->sched != kSchedSplit;

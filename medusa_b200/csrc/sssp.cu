@@ -199,28 +199,36 @@ __global__ void __launch_bounds__(kPushThreads) k_push_edge_bm(SsspArgs a) {
 }
 
 // After k_push_edge_bm: next-frontier bitmap -> next queue (with the
-// claimed-vertex count), clearing the bitmap; one warp per word.  Every
-// vertex taken is stamped as updated in this superstep, as the claim of the
-// queue path does (schedule 6 sends from the stamped vertices).
-__global__ void __launch_bounds__(256) k_nbm2q(SsspArgs a) {
+// claimed-vertex count), clearing the bitmap.  Each round a block takes one
+// word per warp and publishes the round's vertices with ONE atomic (the
+// block queue) instead of one per warp on the same counter.  Every vertex
+// taken is stamped as updated in this superstep, as the claim of the queue
+// path does (schedule 6 sends from the stamped vertices).
+__global__ void __launch_bounds__(kPushThreads) k_nbm2q(SsspArgs a) {
+    __shared__ BlockQueue bq;
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
     const int nxt = c->cur ^ 1;
     const int32_t sv = c->step + 1;
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t wpb = blockDim.x >> 5;
+    if (threadIdx.x == 0) bq.n = 0;
+    __syncthreads();
     uint32_t cn = 0;
-    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < a.f.W; w += warps) {
-        const uint32_t word = a.nbm[w];
-        if (!word) continue;  // warp-uniform
-        if (lane == 0) a.nbm[w] = 0u;
+    for (int64_t w0 = (int64_t)blockIdx.x * wpb; w0 < a.f.W; w0 += (int64_t)gridDim.x * wpb) {
+        const int64_t w = w0 + (threadIdx.x >> 5);
+        const uint32_t word = w < a.f.W ? a.nbm[w] : 0u;
+        if (word && lane == 0) a.nbm[w] = 0u;
         const int32_t v = (int32_t)(w * 32 + lane);
         const bool in = (word >> lane) & 1u;
-        const uint32_t deg = in ? (uint32_t)a.f.outdeg[v] : 0u;
-        if (in) a.stamp[v] = sv;
-        cn += in;
-        enqueue_warp(in && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
-                     pick(a.f.tf, nxt));
+        uint32_t deg = 0;
+        if (in) {
+            deg = (uint32_t)a.f.outdeg[v];
+            a.stamp[v] = sv;
+            cn++;
+        }
+        bq_push(bq, in && deg > 0, v, deg);
+        bq_flush(bq, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt), pick(a.f.tf, nxt));
     }
     flush_counts(c, cn, 0);
 }
@@ -812,7 +820,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         }
         if (branch == kBranchPushBm) {
             k_push_edge_bm<<<grid_push, kPushThreads, 0, s>>>(a);
-            k_nbm2q<<<grid_vtx, 256, 0, s>>>(a);
+            k_nbm2q<<<grid_vtx, kPushThreads, 0, s>>>(a);
             MB_CHECK_LAUNCH();
             return;
         }
