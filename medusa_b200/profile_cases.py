@@ -9,7 +9,9 @@ CASE: c2-bfs, c2-sssp (R-MAT 2^20 / 2^24, source 0), c1-pr (uniform
 grid), c5s-bfs, c5s-sssp, c5s-pr (the C5 generator at 2^21 / 2^25: a case
 small enough for full ncu captures).  Prints one line per repetition with
 the library's device time.  --hostloop runs the host-driven loop (kernels in
-conditional-node graphs are invisible to ncu)."""
+conditional-node graphs are invisible to ncu); --trace prints each superstep
+of the last repetition (BFS 8 B per frontier out-edge + 20 B per frontier
+vertex, SSSP 12 + 20, as algorithmic bytes)."""
 import argparse
 import sys
 
@@ -37,6 +39,8 @@ def main(argv=None):
     ap.add_argument("case")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--hostloop", action="store_true")
+    ap.add_argument("--trace", action="store_true",
+                    help="print every superstep (branch, frontier, CUDA-event ms) of the last rep")
     args = ap.parse_args(argv)
     ctx = api.Context(0)
     if args.hostloop:
@@ -44,6 +48,8 @@ def main(argv=None):
     g = ctx.generate(params(args.case))
     kind = args.case.split("-")[1]
     for i in range(args.reps):
+        if args.trace and i == args.reps - 1:
+            ctx.set_tracing(True)
         if kind == "bfs":
             _, st = g.bfs([0])
         elif kind == "sssp":
@@ -54,6 +60,14 @@ def main(argv=None):
             raise SystemExit("unknown case " + args.case)
         print("%s rep %d: %.4f ms, %d supersteps, %d launches" %
               (args.case, i, st["device_ms"], st["supersteps"], st["kernel_launches"]), flush=True)
+    if args.trace:
+        per_edge = 8 if kind == "bfs" else 12
+        print("step branch sched frontier_vertices frontier_edges ms algorithmic_bytes")
+        for r in ctx.get_trace():
+            b = per_edge * int(r["frontier_edges"]) + 20 * int(r["frontier_vertices"])
+            print("%d %d %d %d %d %.4f %d" % (r["step"], r["branch"], r["sched"],
+                                             r["frontier_vertices"], r["frontier_edges"], r["ms"], b))
+        ctx.set_tracing(False)
     g.close()
     ctx.close()
     return 0
