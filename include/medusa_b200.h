@@ -260,6 +260,24 @@ int mb_batch_run(mb_ctx *ctx, mb_batch *b, int32_t pr_iters, const int32_t *sour
                  float *ranks_out, int32_t *levels_out, mb_stats *stats);
 int mb_batch_destroy(mb_batch *b);
 
+/* ---- superstep traces (no reference counterpart) ------------------------- */
+/* With tracing on, BFS / SSSP / batched-BFS loops run host-driven and every
+ * superstep's branch (its kernels, conversion included) is timed alone with
+ * CUDA events; mb_get_trace returns the records of the runs since tracing
+ * was turned on (oldest first, up to max). */
+typedef struct mb_trace_rec {
+    int32_t app;      /* 0 BFS, 1 SSSP, 2 batched BFS */
+    int32_t step;     /* superstep number */
+    int32_t sched;    /* schedule (MB_SCHED_*; 8: near-far split) */
+    int32_t branch;   /* loop branch: schedule, +8 with a frontier conversion, 16 split,
+                         17 persistent tail, 18 persistent grid, 19 bitmap-output push */
+    uint32_t frontier_vertices;
+    uint64_t frontier_edges;
+    float ms;
+} mb_trace_rec;
+int mb_set_tracing(mb_ctx *ctx, int enable);
+int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
+
 /* ---- tunables (no reference counterpart) --------------------------------- */
 /* Launch and routing parameters that change speed, never results; set by
  * the autotuner (medusa_b200/autotune.py) or by hand.  value -1 restores
@@ -272,7 +290,7 @@ int mb_batch_destroy(mb_batch *b);
 #define MB_TUNE_VERTEX_BLOCKS_PER_SM 2 /* CTAs per SM of the per-vertex / per-word
                                           kernels (default 8) */
 #define MB_TUNE_TAIL_EDGES 3 /* frontier out-edges up to which schedule 0 runs in the
-                                persistent single-CTA tail (default 16384) */
+                                persistent single-CTA tail (default and maximum 8192) */
 #define MB_TUNE_BATCH_THREADS 4 /* threads per CTA of the many-graph kernel (default 256;
                                    a multiple of 32, 64..1024) */
 #define MB_TUNE_BATCH_EDGES_PER_CTA 5 /* many-graph kernel: a graph gets one CTA per this

@@ -19,8 +19,9 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->replay_then_fixed = ctx.replay_then_fixed ? 1 : 0;
     p->max_step = ctx.max_step;
     p->bm_push_min = bm_push_min;
-    p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0 ? (uint32_t)ctx.tunable[MB_TUNE_TAIL_EDGES]
-                                                        : kTailEdges;
+    p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0
+                        ? (uint32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_TAIL_EDGES], kTailEdges)
+                        : kTailEdges;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));

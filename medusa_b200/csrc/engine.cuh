@@ -39,7 +39,13 @@ constexpr int kBranchPersist = kBranchTail + 1;
 constexpr int kBranchPushBm = kBranchPersist + 1;
 constexpr int kNumBranches = kBranchPushBm + 1;
 constexpr int kTailThreads = 1024;
-constexpr uint32_t kTailEntries = 2048, kTailEdges = 16384;
+constexpr uint32_t kTailEntries = 2048, kTailEdges = 8192;
+// The SSSP tail keeps its frontier in shared memory: room for kSTailCap
+// next-frontier vertices (<= the frontier's out-edges, <= kTailEdges) and a
+// hash set of twice that.
+constexpr int kSTailCap = 8192;
+constexpr size_t kTailSmemBytes = 4 * (size_t)(2 * kSTailCap + 3 * kSTailCap + kTailEntries + 33);
+static_assert(kTailEdges <= (uint32_t)kSTailCap, "tail edges exceed the shared-memory tail");
 
 // Device-resident control block of one run.
 struct Ctrl {

@@ -500,16 +500,10 @@ __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
     flush_counts(c, cn, cm);
 }
 
-// Persistent small-frontier tail (schedule 0 in one CTA): consecutive
-// supersteps in one launch while the queue frontier stays within the tail
-// limits; the CTA does each superstep's bookkeeping itself.  Counters that
-// other threads bump with atomics are read through L2 (ldg2).
-__global__ void __launch_bounds__(kTailThreads) k_tail(SsspArgs a, int cap) {
-    count_launch(a.f.ctrl);
-    __shared__ uint32_t s_off[kTailEntries];
-    __shared__ int32_t s_row[kTailEntries];
-    __shared__ float s_du[kTailEntries];
-    __shared__ int s_go;
+// Tail over a frontier kept in global memory (the queue path): used when
+// near-far buckets are on (their far pile lives in global memory).
+__device__ void tail_global(const SsspArgs &a, int cap, uint32_t *s_off, int32_t *s_row, float *s_du,
+                            int &s_go) {
     Ctrl *c = a.f.ctrl;
     for (;;) {
         const int cur = ldg2(&c->cur), nxt = cur ^ 1;
@@ -568,8 +562,219 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(SsspArgs a, int cap) {
         __syncthreads();
         if (!s_go) break;
     }
+}
+
+// Exclusive scan of x[0..n) in shared memory by the whole CTA (n <= 8 *
+// blockDim.x); returns the total.  Uses the 32-entry s_warp scratch.
+__device__ uint32_t block_excl_scan(uint32_t *x, uint32_t n, uint32_t *s_warp) {
+    constexpr int kPer = kSTailCap / kTailThreads;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t i0 = threadIdx.x * kPer;
+    uint32_t loc[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+        loc[k] = i0 + k < n ? x[i0 + k] : 0u;
+        sum += loc[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t t = lane < nw ? s_warp[lane] : 0u, ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += y;
+        }
+        if (lane < nw) s_warp[lane] = ti - t;  // exclusive
+        if (lane == 31) s_warp[32] = ti;      // total
+    }
+    __syncthreads();
+    uint32_t off = s_warp[wid] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kPer; k++)
+        if (i0 + k < n) {
+            x[i0 + k] = off;
+            off += loc[k];
+        }
+    const uint32_t total = s_warp[32];
+    __syncthreads();
+    return total;
+}
+
+// Persistent small-frontier tail with the frontier in SHARED memory: ONE CTA
+// runs consecutive supersteps of schedule 0 while the frontier stays within
+// kTailEntries vertices and p.tail_edges (<= kSTailCap) out-edges.  Per
+// superstep only three dependent global round trips remain: the frontier's
+// distances, its edges (column, weight), the destinations' distances.  An
+// improving relaxation issues a fire-and-forget atomicMin and inserts the
+// destination into a shared-memory hash set (the dedup that the global claim
+// does elsewhere; the CTA is the only one running).  The control block is
+// kept current every superstep (same bookkeeping, same decisions as the
+// other paths); the global queue is written only when the tail ends, with
+// the stamps that mark its vertices as updated.
+__device__ void tail_smem(const SsspArgs &a, int cap, char *smem, int &s_go) {
+    Ctrl *c = a.f.ctrl;
+    int32_t *s_hash = (int32_t *)smem;                       // kSTailCap * 2
+    int32_t *s_q = s_hash + 2 * kSTailCap;                   // kSTailCap
+    int32_t *s_row = s_q + kSTailCap;                        // kSTailCap
+    uint32_t *s_deg = (uint32_t *)(s_row + kSTailCap);       // kSTailCap (degree, then offset)
+    float *s_du = (float *)(s_deg + kSTailCap);              // kTailEntries
+    uint32_t *s_warp = (uint32_t *)(s_du + kTailEntries);    // 33
+    __shared__ uint32_t s_n, s_m;
+    constexpr int32_t kEmpty = -1;
+    constexpr uint32_t kHashMask = 2 * kSTailCap - 1;
+    for (uint32_t i = threadIdx.x; i < 2 * kSTailCap; i += kTailThreads) s_hash[i] = kEmpty;
+    // the frontier from the global queue
+    {
+        const int cur = c->cur;
+        const unsigned long long q = c->q[cur];
+        const uint32_t n = (uint32_t)(q >> 32);
+        const int32_t *qv = pick(a.f.qv, cur);
+        for (uint32_t j = threadIdx.x; j < n; j += kTailThreads) {
+            const int32_t u = qv[j];
+            s_q[j] = u;
+            const int32_t r0 = a.row[u];
+            s_row[j] = r0;
+            s_deg[j] = (uint32_t)(a.row[u + 1] - r0);
+        }
+        if (threadIdx.x == 0) s_n = n;
+        __syncthreads();
+    }
+    for (;;) {
+        const uint32_t n = s_n;
+        for (uint32_t j = threadIdx.x; j < n; j += kTailThreads) s_du[j] = ld_dist(a, s_q[j]);
+        const uint32_t m = block_excl_scan(s_deg, n, s_warp);  // s_deg -> offsets
+        // relax every frontier edge: each thread takes kTR consecutive edges
+        // (one search, then a walk) and issues all their loads before using
+        // any, so one round trip covers the whole frontier (m <= kSTailCap)
+        constexpr int kTR = kSTailCap / kTailThreads;
+        bool reduced = false;
+        {
+            const uint32_t e0 = threadIdx.x * kTR;
+            int32_t v[kTR];
+            float nd[kTR], dv[kTR];
+            int j = e0 < m ? upper_bound_minus1(s_deg, (int)n, e0) : 0;
+#pragma unroll
+            for (int r = 0; r < kTR; r++) {
+                const uint32_t e_idx = e0 + r;
+                v[r] = -1;
+                nd[r] = 0.f;
+                if (e_idx < m) {
+                    while (j + 1 < (int)n && s_deg[j + 1] <= e_idx) j++;
+                    const int32_t e = s_row[j] + (int32_t)(e_idx - s_deg[j]);
+                    v[r] = __ldg(&a.col[e]);
+                    nd[r] = s_du[j] + __ldg(&a.wt[e]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kTR; r++) dv[r] = v[r] >= 0 ? ld_dist(a, v[r]) : 0.f;
+#pragma unroll
+            for (int r = 0; r < kTR; r++) {
+                if (v[r] >= 0 && nd[r] < dv[r]) {
+                    atomicMin((unsigned *)&a.dist[v[r]], __float_as_uint(nd[r]));  // no result needed
+                    reduced = true;
+                    uint32_t h = ((uint32_t)v[r] * 2654435761u) & kHashMask;
+                    for (;;) {  // the set holds <= m <= kSTailCap < 2 * kSTailCap slots
+                        const int32_t old = atomicCAS(&s_hash[h], kEmpty, v[r]);
+                        if (old == kEmpty || old == v[r]) break;
+                        h = (h + 1) & kHashMask;
+                    }
+                }
+            }
+        }
+        // the next superstep reads these distances (at L2) from other threads:
+        // the fire-and-forget reductions must be performed first, which the
+        // CTA barrier alone does not order
+        if (reduced) __threadfence();
+        if (threadIdx.x == 0) {
+            s_n = 0;
+            s_m = 0;
+        }
+        __syncthreads();
+        // the set -> the next frontier (clearing the set).  As the queue path
+        // does, only vertices with out-edges join it: the merge-path kernels
+        // size their per-tile staging on at least one edge per entry.
+        uint32_t mloc = 0;
+        for (uint32_t i = threadIdx.x; i < 2 * kSTailCap; i += kTailThreads) {
+            const int32_t v = s_hash[i];
+            if (v != kEmpty) {
+                s_hash[i] = kEmpty;
+                const int32_t r0 = a.row[v];
+                const uint32_t d = (uint32_t)(a.row[v + 1] - r0);
+                if (d > 0) {
+                    const uint32_t pos = atomicAdd(&s_n, 1u);
+                    s_q[pos] = v;
+                    s_row[pos] = r0;
+                    s_deg[pos] = d;
+                    mloc += d;
+                }
+            }
+        }
+        mloc = warp_sum(mloc);
+        if ((threadIdx.x & 31) == 0 && mloc) atomicAdd(&s_m, mloc);
+        __syncthreads();
+        const uint32_t n2 = s_n, m2 = s_m;
+        if (threadIdx.x == 0) {
+            const int nxt = c->cur ^ 1;
+            c->q[nxt] = ((unsigned long long)n2 << 32) | m2;
+            c->acc_n = n2;
+            c->acc_m = 0;
+            __threadfence();
+            finish_superstep<false>(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+            c->iter++;
+            if (c->iter > cap && !c->done) {
+                c->err |= ERR_STEP_CAP;
+                c->done = 1;
+            }
+            s_go = !c->done && c->branch == kBranchTail;
+            __threadfence();
+        }
+        __syncthreads();
+        if (!s_go) break;
+    }
+    // publish the frontier to the global queue (offsets, tile starts, stamps)
+    const uint32_t n = s_n;
+    if (n == 0) return;
+    const int cur = c->cur;  // finish_superstep made the next queue current
+    const int32_t sv = c->step;
+    block_excl_scan(s_deg, n, s_warp);
+    int32_t *qv = pick(a.f.qv, cur);
+    uint32_t *qo = pick(a.f.qo, cur);
+    int32_t *tf = pick(a.f.tf, cur);
+    const uint32_t m = (uint32_t)c->q[cur];
+    for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+        const int32_t v = s_q[i];
+        const uint32_t off = s_deg[i];
+        const uint32_t d = (i + 1 < n ? s_deg[i + 1] : m) - off;  // >= 1
+        qv[i] = v;
+        qo[i] = off;
+        a.stamp[v] = sv;
+        for (uint32_t t = (off + kTile - 1) / kTile; t <= (off + d - 1) / kTile; t++) tf[t] = (int32_t)i;
+    }
+}
+
+#ifndef MB_TAIL_MIN_BLOCKS
+#define MB_TAIL_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kTailThreads, MB_TAIL_MIN_BLOCKS) k_tail(SsspArgs a, int cap) {
+    count_launch(a.f.ctrl);
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_go;
+    if (a.f.ctrl->p.delta > 0.f) {
+        tail_global(a, cap, (uint32_t *)smem, (int32_t *)(smem + 4 * kTailEntries),
+                    (float *)(smem + 8 * kTailEntries), s_go);
+    } else {
+        tail_smem(a, cap, smem, s_go);
+    }
     // every superstep this kernel ran is finished already
-    if (threadIdx.x == 0) c->pending = 0;
+    if (threadIdx.x == 0) a.f.ctrl->pending = 0;
 }
 
 // Near-far split: the threshold was just raised by delta; every far-pile
@@ -787,6 +992,8 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
     const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
+    MB_CUDA(cudaFuncSetAttribute((const void *)k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTailSmemBytes));
     LoopSpec sp;
     sp.st = &st;
     sp.fa = a.f;
@@ -810,7 +1017,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
             return;
         }
         if (branch == kBranchTail) {
-            k_tail<<<1, kTailThreads, 0, s>>>(a, sp.cap);
+            k_tail<<<1, kTailThreads, kTailSmemBytes, s>>>(a, sp.cap);
             MB_CHECK_LAUNCH();
             return;
         }
