@@ -88,6 +88,15 @@ struct PushSmem {
     BlockQueue bq;
 };
 
+// Combining a warp's same-destination relaxations with __match_any_sync
+// (one distance read and one reduction per distinct destination) measured
+// 1.7x (R-MAT 2^20/2^24) to 2.4x (R-MAT 2^24/2^28) SLOWER on B200 than one
+// read per edge: the match costs more than the L2 requests it saves.  Kept
+// behind this switch, off.
+#ifndef MB_SSSP_MATCH
+#define MB_SSSP_MATCH 0
+#endif
+
 // kBmOut: instead of claiming each improved vertex (an atomic with a
 // result) and appending it to the next queue, set its bit in a.nbm with a
 // fire-and-forget atomicOr; k_nbm2q then builds the next queue.
@@ -145,6 +154,23 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
                 }
             }
         }
+#if MB_SSSP_MATCH
+        // same-destination relaxations of a warp combined: one distance read
+        // and one reduction per distinct destination (R-MAT sends many edges
+        // to the same hubs); the lowest lane of each group keeps the minimum
+        if (kBmOut) {
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int r = 0; r < kTileItems; r++) {
+                const unsigned act = __ballot_sync(0xffffffffu, ok[r]);
+                if (ok[r]) {
+                    const unsigned peers = __match_any_sync(act, v[r]);
+                    nd[r] = __uint_as_float(__reduce_min_sync(peers, __float_as_uint(nd[r])));
+                    ok[r] = lane == __ffs(peers) - 1;
+                }
+            }
+        }
+#endif
 #pragma unroll
         for (int r = 0; r < kTileItems; r++) dv[r] = ok[r] ? ld_dist(a, v[r]) : 0.f;
         if (kBmOut) {
