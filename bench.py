@@ -535,6 +535,8 @@ def bench_configs(ctx, api, args, flush):
         r = scheduler.evaluate(ctx, X, T, F, model)
         per_step[name] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
     c5["per_superstep"] = per_step
+    if not args.no_autotune:
+        tuned5.update(autotune.tune_pagerank(ctx, g, 20, reps=2, out=rk)[0])
     g.pagerank(20, 1.0 / V, out=rk)
     mp, sp = _timed(lambda: g.pagerank(20, 1.0 / V, out=rk)[1], reps, flush)
     per = mp / 20
@@ -607,6 +609,10 @@ def bench_pagerank(ctx, api, args, flush):
     g = ctx.generate(p)
     V, E = g.V, g.E
     r = torch.empty(V, dtype=torch.float32, device="cuda")
+    tuned = {}
+    if not args.no_autotune:
+        from medusa_b200 import autotune
+        tuned = autotune.tune_pagerank(ctx, g, PR_ITERS, reps=3, out=r)[0]
     for _ in range(max(args.warmup, 1)):
         g.pagerank(PR_ITERS, 1.0 / V, out=r)
     ms = 0.0
@@ -620,7 +626,10 @@ def bench_pagerank(ctx, api, args, flush):
     b = 8 * E + 16 * V + 4
     ach = b / (per_iter_ms / 1e3) / 1e9
     g.close()
+    for k in tuned:
+        ctx.set_tunable(k, -1)
     return {"workload": "uniform 2^18 vertices, 2^22 edges, seed 1, 10 supersteps from 1/N",
+            "autotuned": {k: float(v) for k, v in tuned.items()},
             "edges_per_s": round(E / (per_iter_ms / 1e3), 1), "ms_per_superstep": round(per_iter_ms, 5),
             "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": pk, "unit": "GB/s",
                          "frac": round(ach / pk, 4),

@@ -295,7 +295,12 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                    a multiple of 32, 64..1024) */
 #define MB_TUNE_BATCH_EDGES_PER_CTA 5 /* many-graph kernel: a graph gets one CTA per this
                                          many edges + vertices (default 65536) */
-#define MB_NUM_TUNABLES 6
+#define MB_TUNE_PR_LIGHT_VPL 6 /* PageRank: light vertices (in-degree <= 64) per lane of
+                                  the fused pull, 1, 2 or 4 (default 2, or 1 when that
+                                  would give a resident warp fewer than four groups) */
+#define MB_TUNE_PR_SHORT_PAIR 7 /* PageRank: heavy-vertex blocks of <= 512 in-edges
+                                   folded at once by one warp, 1, 2 or 4 (default 2) */
+#define MB_NUM_TUNABLES 8
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

@@ -88,6 +88,14 @@ def tune_traversals(ctx, g, source=0, reps=3):
     return tune(ctx, run, space, reps)
 
 
+def tune_pagerank(ctx, g, iters=10, reps=3, out=None):
+    """Light vertices per lane of the fused pull and short heavy blocks per
+    warp, timing `iters` PageRank supersteps on g (out: a rank buffer to
+    reuse, e.g. a device tensor)."""
+    space = {"pr_light_vpl": [-1, 1, 2, 4], "pr_short_pair": [-1, 1, 2]}
+    return tune(ctx, lambda: g.pagerank(iters, 1.0 / g.V, out=out)[1], space, reps)
+
+
 def tune_batch(ctx, batch, pr_iters=20, reps=3, ranks=None, levels=None):
     """CTA size and edges per CTA (team size) of the many-graph kernel.
     ranks/levels: output buffers to reuse (device tensors avoid the copies)."""

@@ -288,6 +288,9 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "batch threads must be a multiple of 32 in 64..1024");
     if (which == MB_TUNE_BATCH_EDGES_PER_CTA && value == 0)
         return set_error(ctx, MB_ERR_INVALID, "batch edges per CTA must be >= 1");
+    if ((which == MB_TUNE_PR_LIGHT_VPL || which == MB_TUNE_PR_SHORT_PAIR) &&
+        !(value == -1 || value == 1 || value == 2 || value == 4))
+        return set_error(ctx, MB_ERR_INVALID, "PageRank lane/pair counts must be 1, 2 or 4");
     ctx->c.tunable[which] = value;
     ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
     return MB_OK;

@@ -11,9 +11,11 @@
 //
 // The sum runs in the fixed order of pr_order.cuh, the same for every
 // schedule, so schedules never change a bit of the result.  Work mapping:
-//   light vertices (in-degree <= kPrLight): one warp per 32 consecutive
-//     vertices streams their in-edges through a shared-memory window
-//     (coalesced) and each lane folds its own vertex;
+//   light vertices (in-degree <= kPrLight): their in-edge sources are copied
+//     once per graph into a compacted list; one warp per 128 consecutive
+//     light vertices streams their in-edges through a shared-memory window
+//     (coalesced) and each lane folds its own vertices (k_pr_light; the
+//     message-reading schedule uses k_pr_pull over the full reverse CSR);
 //   heavier vertices: their kPrBlock-edge blocks form a work list built once
 //     per graph, one 16-byte item per block (edge range, vertex, slot); one
 //     warp per item (k_heavy_blocks).  A vertex with a single block is
@@ -50,13 +52,21 @@ struct PrArgs {
     const int32_t *hub_first;    // first slot of each hub (nhub+1 entries)
     int32_t nhub;
     float *blk_sum;              // per-slot block sums of the hubs
+    int32_t nlong;               // items [0, nlong) are longer than kPrShortItem
+    const int32_t *light_v;      // light vertices, id order
+    const int32_t *light_row;    // their in-edge offsets into light_col (nlight+1)
+    const int32_t *light_col;    // their in-edge sources, reverse-CSR order
+    int32_t nlight;
 };
 
-__device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) {
+__device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum, int32_t d) {
     const float r = pr_update(sum);
     a.rank_out[v] = r;
-    const int32_t d = a.outdeg[v];
     a.contrib_out[v] = d > 0 ? r / (float)d : 0.0f;  // MPG/CPUFunctorHoster.cpp:80-82
+}
+
+__device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) {
+    pr_write(a, v, sum, a.outdeg[v]);
 }
 
 template <bool kFromMsg>
@@ -65,52 +75,96 @@ __device__ __forceinline__ float edge_val(const PrArgs &a, int64_t j) {
     return __ldg(&a.contrib_in[a.rcol[j]]);
 }
 
-// Heavy-vertex blocks: each warp folds kPair consecutive work items at once
-// (blocks of <= kPrBlock in-edges; the list is sorted by length, so
-// neighbours are about as long), kPair accumulators per lane.  Each item is
-// summed exactly as pr_warp_block_sum does (lane l folds edges l, l+32, ...
-// from 0, then the xor butterfly), so kPair never changes a bit; measured on
-// B200, 4 gains 7% at 2^28 edges and loses 10-25% at 2^24-2^25, so the
-// default is 1.  A single-block vertex is finished here.
-#ifndef MB_PR_PAIR
-#define MB_PR_PAIR 1
+// Heavy-vertex blocks (<= kPrBlock in-edges each), summed exactly as
+// pr_warp_block_sum does: lane l folds edges l, l+32, ... from 0, then the
+// xor butterfly.  The list is sorted longest first.  Its head (items longer
+// than kPrShortItem) takes one item per warp with kLongU loads of each lane
+// in flight; the rest take kShortPair items per warp at once (kShortU loads
+// of each item in flight), so short items do not leave a warp waiting on a
+// handful of loads.  Neither grouping changes a bit.  A single-block vertex
+// is finished here; a hub block writes its block sum.
+#ifndef MB_PR_LONG_UNROLL
+#define MB_PR_LONG_UNROLL 16
 #endif
-constexpr int kPair = MB_PR_PAIR;
+constexpr int kLongU = MB_PR_LONG_UNROLL;
+constexpr int kShortU = 4;
+constexpr int kPrShortItem = 32 * kShortU * 4;  // 512 edges
+constexpr int kShortPairDefault = 2;  // measured best at 2^20-2^28 edges
 
-template <bool kFromMsg>
+__host__ __device__ __forceinline__ int64_t heavy_units(int32_t nitems, int32_t nlong, int pair) {
+    return (int64_t)nlong + ((int64_t)nitems - nlong + pair - 1) / pair;
+}
+
+__device__ __forceinline__ void heavy_finish(const PrArgs &a, const int4 &it, float acc, int32_t d) {
+    if (it.w == -2) return;  // past the list
+    if (it.w < 0) pr_write(a, it.z, 0.f + acc, d);  // one block sum folded from 0
+    else a.blk_sum[it.w] = acc;
+}
+
+template <bool kFromMsg, int kShortPair>
 __global__ void __launch_bounds__(256) k_heavy_blocks(PrArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t b0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * kPair; b0 < a.nitems;
-         b0 += warps * kPair) {
-        int4 it[kPair];
-        int32_t len[kPair], lmax = 0;
-        float acc[kPair];
+    const int64_t units = heavy_units(a.nitems, a.nlong, kShortPair);
+    for (int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; u < units; u += warps) {
+        if (u < a.nlong) {
+            const int4 it = __ldg(&a.items[u]);
+            const int32_t d = (lane == 0 && it.w < 0) ? __ldg(&a.outdeg[it.z]) : 0;
+            const int32_t len = it.y - it.x;
+            float acc = 0.f;
+            for (int32_t k0 = 0; k0 < len; k0 += 32 * kLongU) {
+                float val[kLongU];
 #pragma unroll
-        for (int p = 0; p < kPair; p++) {
+                for (int q = 0; q < kLongU; q++) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    val[q] = k < len ? edge_val<kFromMsg>(a, (int64_t)it.x + k) : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < kLongU; q++)
+                    if (k0 + lane + 32 * q < len) acc += val[q];
+            }
+#pragma unroll
+            for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+            if (lane == 0) heavy_finish(a, it, acc, d);
+            continue;
+        }
+        const int64_t b0 = a.nlong + (u - a.nlong) * kShortPair;
+        int4 it[kShortPair];
+        int32_t len[kShortPair], d[kShortPair], lmax = 0;
+        float acc[kShortPair];
+#pragma unroll
+        for (int p = 0; p < kShortPair; p++) {
             it[p] = b0 + p < a.nitems ? __ldg(&a.items[b0 + p]) : make_int4(0, 0, 0, -2);
             len[p] = it[p].y - it[p].x;
             lmax = max(lmax, len[p]);
             acc[p] = 0.f;
         }
-#pragma unroll 4
-        for (int32_t k = lane; k < lmax; k += 32) {
 #pragma unroll
-            for (int p = 0; p < kPair; p++)
-                if (k < len[p]) acc[p] += edge_val<kFromMsg>(a, (int64_t)it[p].x + k);
+        for (int p = 0; p < kShortPair; p++)
+            d[p] = (lane == 0 && it[p].w == -1) ? __ldg(&a.outdeg[it[p].z]) : 0;
+        for (int32_t k0 = 0; k0 < lmax; k0 += 32 * kShortU) {
+            float val[kShortPair][kShortU];
+#pragma unroll
+            for (int p = 0; p < kShortPair; p++)
+#pragma unroll
+                for (int q = 0; q < kShortU; q++) {
+                    const int32_t k = k0 + lane + 32 * q;
+                    val[p][q] = k < len[p] ? edge_val<kFromMsg>(a, (int64_t)it[p].x + k) : 0.f;
+                }
+#pragma unroll
+            for (int p = 0; p < kShortPair; p++)
+#pragma unroll
+                for (int q = 0; q < kShortU; q++)
+                    if (k0 + lane + 32 * q < len[p]) acc[p] += val[p][q];
         }
 #pragma unroll
-        for (int p = 0; p < kPair; p++) {
+        for (int p = 0; p < kShortPair; p++) {
 #pragma unroll
             for (int off = 16; off; off >>= 1) acc[p] += __shfl_xor_sync(0xffffffffu, acc[p], off);
         }
         if (lane == 0) {
 #pragma unroll
-            for (int p = 0; p < kPair; p++) {
-                if (it[p].w == -2) continue;  // past the list
-                if (it[p].w < 0) pr_write(a, it[p].z, 0.f + acc[p]);  // one block sum folded from 0
-                else a.blk_sum[it[p].w] = acc[p];
-            }
+            for (int p = 0; p < kShortPair; p++) heavy_finish(a, it[p], acc[p], d[p]);
         }
     }
 }
@@ -172,6 +226,79 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_pull(PrArgs a) {
             __syncwarp();
         }
         if (valid && !heavy) pr_write(a, v, sum);
+    }
+}
+
+// Fused combine+update of the light vertices (in-degree <= kPrLight) from
+// the compacted light lists: one warp per group of 32 * kVPL consecutive
+// light vertices (lane l owns the group's vertices l, l+32, ...).  The warp
+// streams the group's in-edge sources (contiguous in light_col) through a
+// shared-memory window of gathered contributions, every load of a window in
+// flight at once, and each lane folds its vertices' parts of the window in
+// order: the sequential fold of pr_order.cuh.
+template <int kVPL>
+__global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
+    __shared__ float win[kPrWarps][kWin];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float *wv = win[wid];
+    constexpr int kG = 32 * kVPL;
+    const int64_t ngroups = ((int64_t)a.nlight + kG - 1) / kG;
+    const int64_t warps = (int64_t)gridDim.x * kPrWarps;
+    for (int64_t grp = (int64_t)blockIdx.x * kPrWarps + wid; grp < ngroups; grp += warps) {
+        const int32_t i0 = (int32_t)(grp * kG);
+        const int32_t iend = (int32_t)min((int64_t)i0 + kG, (int64_t)a.nlight);
+        int32_t v[kVPL], b[kVPL], e[kVPL], d[kVPL];
+        float sum[kVPL];
+#pragma unroll
+        for (int i = 0; i < kVPL; i++) {
+            const int32_t idx = i0 + 32 * i + lane;
+            v[i] = -1;
+            b[i] = e[i] = 0;
+            sum[i] = 0.f;
+            if (idx < iend) {
+                v[i] = __ldg(&a.light_v[idx]);
+                b[i] = __ldg(&a.light_row[idx]);
+                e[i] = __ldg(&a.light_row[idx + 1]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kVPL; i++) d[i] = v[i] >= 0 ? __ldg(&a.outdeg[v[i]]) : 0;
+        const int32_t g0 = __ldg(&a.light_row[i0]), g1 = __ldg(&a.light_row[iend]);
+        for (int32_t w0 = g0; w0 < g1; w0 += kWin) {
+            const int32_t w1 = min(w0 + kWin, g1);
+            int32_t src[kWin / 32];
+#pragma unroll
+            for (int r = 0; r < kWin / 32; r++) {
+                const int32_t j = w0 + lane + 32 * r;
+                src[r] = j < w1 ? __ldg(&a.light_col[j]) : -1;
+            }
+            float vals[kWin / 32];
+#pragma unroll
+            for (int r = 0; r < kWin / 32; r++) vals[r] = src[r] >= 0 ? __ldg(&a.contrib_in[src[r]]) : 0.f;
+#pragma unroll
+            for (int r = 0; r < kWin / 32; r++) wv[lane + 32 * r] = vals[r];
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < kVPL; i++) {
+                const int32_t lo = max(b[i], w0), hi = min(e[i], w1);
+                for (int32_t j = lo; j < hi; j++) sum[i] += wv[j - w0];
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int i = 0; i < kVPL; i++)
+            if (v[i] >= 0) pr_write(a, v[i], sum[i], d[i]);
+    }
+}
+
+// Copy each light vertex's in-edge sources out of the reverse CSR.
+__global__ void k_light_copy(const int32_t *light_v, const int32_t *light_row, int32_t nlight,
+                             const int32_t *rrow, const int32_t *rcol, int32_t *light_col) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlight;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = light_v[i], o = light_row[i];
+        const int32_t b = rrow[v], n = rrow[v + 1] - b;
+        for (int32_t k = 0; k < n; k++) light_col[o + k] = rcol[b + k];
     }
 }
 
@@ -328,6 +455,8 @@ void PrState::ensure(Context &ctx, const Graph &g) {
                      [](const int4 &x, const int4 &y) { return (x.y - x.x) > (y.y - y.x); });
     nitems = (int32_t)it.size();
     nhub = (int32_t)hv.size();
+    nlong = 0;
+    while (nlong < nitems && it[nlong].y - it[nlong].x > kPrShortItem) nlong++;
     items.reserve(sizeof(int4) * std::max<size_t>(it.size(), 1));
     hub_v.reserve(sizeof(int32_t) * std::max<size_t>(hv.size(), 1));
     hub_first.reserve(sizeof(int32_t) * hf.size());
@@ -335,8 +464,30 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     if (nitems) MB_CUDA(cudaMemcpy(items.p, it.data(), sizeof(int4) * it.size(), cudaMemcpyHostToDevice));
     if (nhub) MB_CUDA(cudaMemcpy(hub_v.p, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice));
     MB_CUDA(cudaMemcpy(hub_first.p, hf.data(), 4 * hf.size(), cudaMemcpyHostToDevice));
+    // light lists: the vertices with in-degree <= kPrLight and their in-edges
+    std::vector<int32_t> lv, lr(1, 0);
+    lv.reserve((size_t)V);
+    lr.reserve((size_t)V + 1);
+    for (int32_t v = 0; v < V; v++) {
+        const int32_t d = rrow[v + 1] - rrow[v];
+        if (d > kPrLight) continue;
+        lv.push_back(v);
+        lr.push_back(lr.back() + d);
+    }
+    nlight = (int32_t)lv.size();
+    light_v.reserve(sizeof(int32_t) * std::max<size_t>(lv.size(), 1));
+    light_row.reserve(sizeof(int32_t) * lr.size());
+    light_col.reserve(sizeof(int32_t) * std::max<size_t>((size_t)lr.back(), 1));
+    if (nlight) {
+        MB_CUDA(cudaMemcpy(light_v.p, lv.data(), 4 * lv.size(), cudaMemcpyHostToDevice));
+        MB_CUDA(cudaMemcpy(light_row.p, lr.data(), 4 * lr.size(), cudaMemcpyHostToDevice));
+        k_light_copy<<<grid_for(nlight, 256, ctx.num_sms * 16), 256, 0, ctx.stream>>>(
+            light_v.as<int32_t>(), light_row.as<int32_t>(), nlight, g.rrow.as<int32_t>(),
+            g.rcol.as<int32_t>(), light_col.as<int32_t>());
+        MB_CHECK_LAUNCH();
+        MB_CUDA(cudaStreamSynchronize(ctx.stream));
+    }
     built = true;
-    (void)ctx;
 }
 
 void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init, int sched,
@@ -365,6 +516,11 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         a.hub_first = st.hub_first.as<int32_t>();
         a.nhub = st.nhub;
         a.blk_sum = st.blk_sum.as<float>();
+        a.nlong = st.nlong;
+        a.light_v = st.light_v.as<int32_t>();
+        a.light_row = st.light_row.as<int32_t>();
+        a.light_col = st.light_col.as<int32_t>();
+        a.nlight = st.nlight;
         return a;
     };
     // grids of exactly the resident blocks (grid-stride loops: no tail wave)
@@ -374,7 +530,35 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         return ctx.num_sms * std::max(per_sm, 1);
     };
     const int grid_pull = resident((const void *)k_pr_pull<false>, kPrThreads);
-    const int grid_heavy = resident((const void *)k_heavy_blocks<false>, 256);
+    const int grid_heavy = resident((const void *)k_heavy_blocks<false, 4>, 256);
+    // light vertices per lane: the tunable, else 2 (measured best from 2^22
+    // to 2^28 edges) while every resident warp still gets four groups
+    const int grid_light = resident((const void *)k_pr_light<4>, kPrThreads);
+    int vpl = (int)ctx.tunable[MB_TUNE_PR_LIGHT_VPL];
+    if (vpl <= 0) {
+        vpl = 2;
+        while (vpl > 1 && (int64_t)st.nlight < (int64_t)32 * vpl * 4 * grid_light * kPrWarps) vpl >>= 1;
+    }
+    const int pair = ctx.tunable[MB_TUNE_PR_SHORT_PAIR] > 0 ? (int)ctx.tunable[MB_TUNE_PR_SHORT_PAIR]
+                                                             : kShortPairDefault;
+    const int64_t heavy_threads = heavy_units(st.nitems, st.nlong, pair) * 32;
+    auto heavy = [&](bool from_msg, cudaStream_t cs, const PrArgs &a) {
+        const int grid = grid_for(heavy_threads, 256, grid_heavy);
+        if (from_msg) {
+            if (pair == 1) k_heavy_blocks<true, 1><<<grid, 256, 0, cs>>>(a);
+            else if (pair == 2) k_heavy_blocks<true, 2><<<grid, 256, 0, cs>>>(a);
+            else k_heavy_blocks<true, 4><<<grid, 256, 0, cs>>>(a);
+        } else {
+            if (pair == 1) k_heavy_blocks<false, 1><<<grid, 256, 0, cs>>>(a);
+            else if (pair == 2) k_heavy_blocks<false, 2><<<grid, 256, 0, cs>>>(a);
+            else k_heavy_blocks<false, 4><<<grid, 256, 0, cs>>>(a);
+        }
+    };
+    auto light = [&](cudaStream_t cs, const PrArgs &a) {
+        if (vpl == 1) k_pr_light<1><<<grid_light, kPrThreads, 0, cs>>>(a);
+        else if (vpl == 2) k_pr_light<2><<<grid_light, kPrThreads, 0, cs>>>(a);
+        else k_pr_light<4><<<grid_light, kPrThreads, 0, cs>>>(a);
+    };
     const int grid_vtx = ctx.num_sms * 8;
     auto emit = [&](cudaStream_t cs) {
         k_pr_init<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init, st.contrib[0].as<float>());
@@ -390,11 +574,11 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             }
             if (unfused) {
                 k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
-                if (a.nitems) k_heavy_blocks<true><<<grid_for((int64_t)a.nitems * 32 / kPair + 32, 256, grid_heavy), 256, 0, cs>>>(a);
+                if (a.nitems) heavy(true, cs, a);
                 k_pr_pull<true><<<grid_pull, kPrThreads, 0, cs>>>(a);
             } else {
-                if (a.nitems) k_heavy_blocks<false><<<grid_for((int64_t)a.nitems * 32 / kPair + 32, 256, grid_heavy), 256, 0, cs>>>(a);
-                k_pr_pull<false><<<grid_pull, kPrThreads, 0, cs>>>(a);
+                if (a.nitems) heavy(false, cs, a);
+                if (a.nlight) light(cs, a);
             }
             if (a.nhub) k_hub_finalize<<<grid_for(a.nhub, 128, ctx.num_sms * 4), 128, 0, cs>>>(a);
             MB_CHECK_LAUNCH();
@@ -410,7 +594,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     try {
         if (ctx.use_graphs) {
             if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_sched != sched ||
-                st.g_order != ctx.pr_order) {
+                st.g_order != ctx.pr_order || st.g_tune != ctx.tune_gen) {
                 if (st.exec) cudaGraphExecDestroy(st.exec);
                 st.exec = nullptr;
                 cudaGraph_t gr;
@@ -429,6 +613,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                 st.g_init = init;
                 st.g_sched = sched;
                 st.g_order = ctx.pr_order;
+                st.g_tune = ctx.tune_gen;
             }
             MB_CUDA(cudaEventRecord(e0, s));
             MB_CUDA(cudaGraphLaunch(st.exec, s));
@@ -451,7 +636,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             stats->edges_scanned = (int64_t)iters * g.E;
             stats->kernel_launches =
                 ref_order ? 1 + (int64_t)iters * (1 + unfused) + (iters == 0)
-                          : 1 + (int64_t)iters * (1 + (st.nitems > 0) + (st.nhub > 0) + unfused) + (iters == 0);
+                          : 1 + (int64_t)iters * ((unfused ? 2 : st.nlight > 0) + (st.nitems > 0) + (st.nhub > 0)) +
+                                (iters == 0);
         }
     } catch (...) {
         cudaEventDestroy(e0);

@@ -42,3 +42,18 @@ def test_tune_batch(gpu_ctx):
         b.close()
         gpu_ctx.set_tunable("batch_threads", -1)
         gpu_ctx.set_tunable("batch_edges_per_cta", -1)
+
+
+def test_tune_pagerank_keeps_results(gpu_ctx):
+    from medusa_b200 import api, autotune
+    g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.57, 0.19, 0.19, seed=3))
+    try:
+        r0, _ = g.pagerank(5, 1.0 / g.V)
+        best, table = autotune.tune_pagerank(gpu_ctx, g, 5, reps=1)
+        assert set(best) == {"pr_light_vpl", "pr_short_pair"} and len(table) >= 5
+        r1, _ = g.pagerank(5, 1.0 / g.V)
+        np.testing.assert_array_equal(r0.view(np.uint32), r1.view(np.uint32))
+    finally:
+        g.close()
+        gpu_ctx.set_tunable("pr_light_vpl", -1)
+        gpu_ctx.set_tunable("pr_short_pair", -1)

@@ -87,6 +87,36 @@ def test_pagerank_matches_reference(ctx, name):
     g.close()
 
 
+def test_pagerank_launch_shapes_keep_every_bit(ctx, api):
+    """Every light-vertices-per-lane and short-blocks-per-warp setting, for
+    both PageRank schedules, on a skewed R-MAT whose in-degrees cover light
+    vertices, short and long heavy blocks and multi-block hubs: ranks equal
+    the oracle run in the kernels' summation order, bit for bit."""
+    p = api.rmat_params(14, 1 << 19, 0.57, 0.19, 0.19, seed=7)
+    V, src, dst, _ = api.generate_edges_host(p)
+    indeg = np.bincount(dst, minlength=V)
+    assert indeg.max() > 4096 and ((indeg > 512) & (indeg <= 4096)).any()
+    assert ((indeg > 64) & (indeg <= 512)).any()
+    aa = O.AAGraph(V, src, dst, None)
+    ro = O.pagerank(V, aa, None, 5, 1.0 / V, order="device")
+    g = ctx.graph_from_edges(V, src, dst, None)
+    try:
+        for vpl in (1, 2, 4):
+            for pair in (1, 2, 4):
+                ctx.set_tunable("pr_light_vpl", vpl)
+                ctx.set_tunable("pr_short_pair", pair)
+                for sched in (0, 6):
+                    ctx.set_policy(api.MB_POLICY_FORCED, sched)
+                    r, _ = g.pagerank(5, 1.0 / V)
+                    np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32),
+                                                  err_msg="vpl %d pair %d schedule %d" % (vpl, pair, sched))
+    finally:
+        ctx.set_policy(api.MB_POLICY_FIXED)
+        ctx.set_tunable("pr_light_vpl", -1)
+        ctx.set_tunable("pr_short_pair", -1)
+        g.close()
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_pagerank_reference_order_is_the_reference_bit_for_bit(ctx, api, name):
     """MB_PR_ORDER_REFERENCE replays GraphIR::sortByDegree + buildMEG: the
@@ -357,6 +387,11 @@ def test_tunables_validate_and_reset(gpu_ctx, api):
         gpu_ctx.set_tunable("push_blocks_per_sm", 0)
     with pytest.raises(api.MedusaError):
         gpu_ctx.set_tunable(99, 1)
+    for bad in (0, 3, 8):
+        with pytest.raises(api.MedusaError):
+            gpu_ctx.set_tunable("pr_light_vpl", bad)
+        with pytest.raises(api.MedusaError):
+            gpu_ctx.set_tunable("pr_short_pair", bad)
     gpu_ctx.set_tunable("push_blocks_per_sm", -1)
     assert gpu_ctx.get_tunable("push_blocks_per_sm") == -1
 
