@@ -69,10 +69,43 @@ __device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) 
     pr_write(a, v, sum, a.outdeg[v]);
 }
 
+// Streamed index arrays (read once per superstep) bypass L1, which is left
+// to the contribution gathers: a hot source's contribution then stays in L1
+// for the next warps that gather it.
+#ifndef MB_PR_STREAM
+#define MB_PR_STREAM 2
+#endif
+#ifndef MB_PR_GATHER
+#define MB_PR_GATHER 0
+#endif
+__device__ __forceinline__ int32_t ld_stream(const int32_t *p) {
+#if MB_PR_STREAM == 0
+    return __ldg(p);
+#elif MB_PR_STREAM == 1
+    return __ldcg(p);
+#elif MB_PR_STREAM == 2
+    int32_t v;
+    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+#else
+    return __ldcs(p);
+#endif
+}
+
+__device__ __forceinline__ float ld_gather(const float *p) {
+#if MB_PR_GATHER == 1
+    float v;
+    asm("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
 template <bool kFromMsg>
 __device__ __forceinline__ float edge_val(const PrArgs &a, int64_t j) {
     if (kFromMsg) return a.msg[j];
-    return __ldg(&a.contrib_in[a.rcol[j]]);
+    return ld_gather(&a.contrib_in[ld_stream(&a.rcol[j])]);
 }
 
 // Heavy-vertex blocks (<= kPrBlock in-edges each), summed exactly as
@@ -256,9 +289,9 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
             b[i] = e[i] = 0;
             sum[i] = 0.f;
             if (idx < iend) {
-                v[i] = __ldg(&a.light_v[idx]);
-                b[i] = __ldg(&a.light_row[idx]);
-                e[i] = __ldg(&a.light_row[idx + 1]);
+                v[i] = ld_stream(&a.light_v[idx]);
+                b[i] = ld_stream(&a.light_row[idx]);
+                e[i] = ld_stream(&a.light_row[idx + 1]);
             }
         }
 #pragma unroll
@@ -270,11 +303,11 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
 #pragma unroll
             for (int r = 0; r < kWin / 32; r++) {
                 const int32_t j = w0 + lane + 32 * r;
-                src[r] = j < w1 ? __ldg(&a.light_col[j]) : -1;
+                src[r] = j < w1 ? ld_stream(&a.light_col[j]) : -1;
             }
             float vals[kWin / 32];
 #pragma unroll
-            for (int r = 0; r < kWin / 32; r++) vals[r] = src[r] >= 0 ? __ldg(&a.contrib_in[src[r]]) : 0.f;
+            for (int r = 0; r < kWin / 32; r++) vals[r] = src[r] >= 0 ? ld_gather(&a.contrib_in[src[r]]) : 0.f;
 #pragma unroll
             for (int r = 0; r < kWin / 32; r++) wv[lane + 32 * r] = vals[r];
             __syncwarp();
@@ -530,34 +563,41 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         return ctx.num_sms * std::max(per_sm, 1);
     };
     const int grid_pull = resident((const void *)k_pr_pull<false>, kPrThreads);
-    const int grid_heavy = resident((const void *)k_heavy_blocks<false, 4>, 256);
     // light vertices per lane: the tunable, else 2 (measured best from 2^22
     // to 2^28 edges) while every resident warp still gets four groups
-    const int grid_light = resident((const void *)k_pr_light<4>, kPrThreads);
     int vpl = (int)ctx.tunable[MB_TUNE_PR_LIGHT_VPL];
     if (vpl <= 0) {
         vpl = 2;
-        while (vpl > 1 && (int64_t)st.nlight < (int64_t)32 * vpl * 4 * grid_light * kPrWarps) vpl >>= 1;
+        const int64_t warps = (int64_t)resident((const void *)k_pr_light<1>, kPrThreads) * kPrWarps;
+        while (vpl > 1 && (int64_t)st.nlight < (int64_t)32 * vpl * 4 * warps) vpl >>= 1;
     }
     const int pair = ctx.tunable[MB_TUNE_PR_SHORT_PAIR] > 0 ? (int)ctx.tunable[MB_TUNE_PR_SHORT_PAIR]
                                                              : kShortPairDefault;
+    // each variant's grid is its own resident block count (registers differ)
+    const void *heavy_fn[2][3] = {{(const void *)k_heavy_blocks<false, 1>, (const void *)k_heavy_blocks<false, 2>,
+                                   (const void *)k_heavy_blocks<false, 4>},
+                                  {(const void *)k_heavy_blocks<true, 1>, (const void *)k_heavy_blocks<true, 2>,
+                                   (const void *)k_heavy_blocks<true, 4>}};
+    const void *light_fn[3] = {(const void *)k_pr_light<1>, (const void *)k_pr_light<2>,
+                               (const void *)k_pr_light<4>};
+    const int pi = pair == 1 ? 0 : pair == 2 ? 1 : 2, vi = vpl == 1 ? 0 : vpl == 2 ? 1 : 2;
+#ifdef MB_PR_CARVEOUT
+    for (int f = 0; f < 2; f++)
+        MB_CUDA(cudaFuncSetAttribute(heavy_fn[f][pi], cudaFuncAttributePreferredSharedMemoryCarveout, MB_PR_CARVEOUT));
+#endif
     const int64_t heavy_threads = heavy_units(st.nitems, st.nlong, pair) * 32;
+    const int grid_heavy[2] = {grid_for(heavy_threads, 256, resident(heavy_fn[0][pi], 256)),
+                               grid_for(heavy_threads, 256, resident(heavy_fn[1][pi], 256))};
+    const int grid_light = resident(light_fn[vi], kPrThreads);
     auto heavy = [&](bool from_msg, cudaStream_t cs, const PrArgs &a) {
-        const int grid = grid_for(heavy_threads, 256, grid_heavy);
-        if (from_msg) {
-            if (pair == 1) k_heavy_blocks<true, 1><<<grid, 256, 0, cs>>>(a);
-            else if (pair == 2) k_heavy_blocks<true, 2><<<grid, 256, 0, cs>>>(a);
-            else k_heavy_blocks<true, 4><<<grid, 256, 0, cs>>>(a);
-        } else {
-            if (pair == 1) k_heavy_blocks<false, 1><<<grid, 256, 0, cs>>>(a);
-            else if (pair == 2) k_heavy_blocks<false, 2><<<grid, 256, 0, cs>>>(a);
-            else k_heavy_blocks<false, 4><<<grid, 256, 0, cs>>>(a);
-        }
+        PrArgs arg = a;
+        void *params[] = {&arg};
+        MB_CUDA(cudaLaunchKernel(heavy_fn[from_msg][pi], grid_heavy[from_msg], 256, params, 0, cs));
     };
     auto light = [&](cudaStream_t cs, const PrArgs &a) {
-        if (vpl == 1) k_pr_light<1><<<grid_light, kPrThreads, 0, cs>>>(a);
-        else if (vpl == 2) k_pr_light<2><<<grid_light, kPrThreads, 0, cs>>>(a);
-        else k_pr_light<4><<<grid_light, kPrThreads, 0, cs>>>(a);
+        PrArgs arg = a;
+        void *params[] = {&arg};
+        MB_CUDA(cudaLaunchKernel(light_fn[vi], grid_light, kPrThreads, params, 0, cs));
     };
     const int grid_vtx = ctx.num_sms * 8;
     auto emit = [&](cudaStream_t cs) {
