@@ -118,8 +118,9 @@ int mb_create(int device, mb_ctx **out) {
         MB_CUDA(cudaMallocHost((void **)&ctx->c.pinned_small, mb::Context::kSmallBytes));
         for (mb::DevBuf &b : ctx->c.mlp) {
             b.reserve(sizeof(float) * mb::kModelFloats);
-            MB_CUDA(cudaMemset(b.p, 0, sizeof(float) * mb::kModelFloats));
+            MB_CUDA(cudaMemsetAsync(b.p, 0, sizeof(float) * mb::kModelFloats, ctx->c.stream));
         }
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
     });
     if (rc != MB_OK) {
         t_last_error = ctx->c.last_error;
@@ -195,10 +196,10 @@ int mb_set_persistent_grid(mb_ctx *ctx, int enable) {
 
 namespace {
 // n bytes from host or device memory into a device buffer (returns the pointer to use)
-const void *stage_in(mb::DevBuf &b, const void *p, size_t n) {
+const void *stage_in(mb::DevBuf &b, const void *p, size_t n, cudaStream_t s) {
     if (mb::is_device_ptr(p)) return p;
     b.reserve(std::max<size_t>(n, 1));
-    if (n) MB_CUDA(cudaMemcpy(b.p, p, n, cudaMemcpyHostToDevice));
+    mb::copy_sync(s, b.p, p, n);
     return b.p;
 }
 }  // namespace
@@ -208,8 +209,8 @@ int mb_vis_node_quads(mb_ctx *ctx, int32_t V, const float *pos, const int32_t *r
         if (!ctx || V < 0 || (V > 0 && (!pos || !radius || !quads))) mb::fail(MB_ERR_INVALID, "bad arguments");
         use_device(ctx);
         mb::DevBuf bp, br, bq;
-        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)V);
-        const int32_t *dr = (const int32_t *)stage_in(br, radius, sizeof(int32_t) * (size_t)V);
+        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)V, ctx->c.stream);
+        const int32_t *dr = (const int32_t *)stage_in(br, radius, sizeof(int32_t) * (size_t)V, ctx->c.stream);
         float *dq = quads;
         const bool dev_out = mb::is_device_ptr(quads);
         if (!dev_out) dq = (float *)bq.reserve(sizeof(float) * 8 * std::max<size_t>(V, 1));
@@ -226,7 +227,7 @@ int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *l
         if (!pos || !lines) mb::fail(MB_ERR_INVALID, "bad arguments");
         use_device(ctx);
         mb::DevBuf bp, bl;
-        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)g->g.V);
+        const float *dp = (const float *)stage_in(bp, pos, sizeof(float) * 2 * (size_t)g->g.V, ctx->c.stream);
         float *dl = lines;
         const bool dev_out = mb::is_device_ptr(lines);
         const size_t nb = sizeof(float) * 4 * (size_t)g->g.E;
@@ -311,9 +312,9 @@ mb::DevBuf &model_weights(mb_ctx *ctx, int32_t m) {
 }
 bool &model_ready(mb_ctx *ctx, int32_t m) { return ctx->c.mlp_ready[m]; }
 // n*k floats from host or device memory into a temporary device buffer
-void to_device(mb::DevBuf &b, const float *p, size_t count) {
+void to_device(mb::DevBuf &b, const float *p, size_t count, cudaStream_t s) {
     b.reserve(sizeof(float) * std::max<size_t>(count, 1));
-    if (count) MB_CUDA(cudaMemcpy(b.p, p, sizeof(float) * count, cudaMemcpyDefault));
+    mb::copy_sync(s, b.p, p, sizeof(float) * count);
 }
 }  // namespace
 
@@ -343,8 +344,8 @@ int mb_scheduler_train(mb_ctx *ctx, int32_t model, const float *features, const 
             mb::fail(MB_ERR_INVALID, "bad training arguments");
         use_device(ctx);
         mb::DevBuf X, T;
-        to_device(X, features, (size_t)n * mb::kFeat);
-        to_device(T, times, (size_t)n * mb::kOut);
+        to_device(X, features, (size_t)n * mb::kFeat, ctx->c.stream);
+        to_device(T, times, (size_t)n * mb::kOut, ctx->c.stream);
         const float loss =
             mb::mlp_train(ctx->c, W.as<float>(), X.as<float>(), T.as<float>(), n, epochs, lr, seed);
         model_ready(ctx, model) = true;
@@ -361,7 +362,7 @@ int mb_scheduler_get_weights(mb_ctx *ctx, int32_t model, float *w) {
         if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
         mb::DevBuf &W = model_weights(ctx, model);
-        MB_CUDA(cudaMemcpy(w, W.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        mb::copy_sync(ctx->c.stream, w, W.p, sizeof(float) * mb::kMlpParams);
     });
 }
 
@@ -370,7 +371,7 @@ int mb_scheduler_set_weights(mb_ctx *ctx, int32_t model, const float *w) {
         if (!ctx || !w) mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
         mb::DevBuf &W = model_weights(ctx, model);
-        MB_CUDA(cudaMemcpy(W.p, w, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
+        mb::copy_sync(ctx->c.stream, W.p, w, sizeof(float) * mb::kMlpParams);
         mb::mlp_set_open_bounds(ctx->c, W.as<float>());
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
         model_ready(ctx, model) = true;
@@ -384,15 +385,15 @@ int mb_scheduler_grad(mb_ctx *ctx, const float *weights, const float *features, 
             mb::fail(MB_ERR_INVALID, "null argument");
         use_device(ctx);
         mb::DevBuf P, X, T, G, L;
-        to_device(P, weights, mb::kMlpParams);
-        to_device(X, features, (size_t)n * mb::kFeat);
-        to_device(T, times, (size_t)n * mb::kOut);
+        to_device(P, weights, mb::kMlpParams, ctx->c.stream);
+        to_device(X, features, (size_t)n * mb::kFeat, ctx->c.stream);
+        to_device(T, times, (size_t)n * mb::kOut, ctx->c.stream);
         G.reserve(sizeof(float) * mb::kMlpParams);
         L.reserve(2 * sizeof(float));
         mb::mlp_grad(ctx->c, P.as<float>(), X.as<float>(), T.as<float>(), n, G.as<float>(), L.as<float>());
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
-        MB_CUDA(cudaMemcpy(grad_out, G.p, sizeof(float) * mb::kMlpParams, cudaMemcpyDefault));
-        if (loss_out) MB_CUDA(cudaMemcpy(loss_out, L.p, sizeof(float), cudaMemcpyDefault));
+        mb::copy_sync(ctx->c.stream, grad_out, G.p, sizeof(float) * mb::kMlpParams);
+        if (loss_out) mb::copy_sync(ctx->c.stream, loss_out, L.p, sizeof(float));
         P.release(); X.release(); T.release(); G.release(); L.release();
     });
 }
@@ -404,19 +405,19 @@ int mb_scheduler_pick(mb_ctx *ctx, int32_t model, const float *features, const i
         use_device(ctx);
         mb::DevBuf &W = model_weights(ctx, model);
         mb::DevBuf X, O, F;
-        to_device(X, features, (size_t)n * mb::kFeat);
+        to_device(X, features, (size_t)n * mb::kFeat, ctx->c.stream);
         O.reserve(sizeof(int32_t) * std::max(n, 1));
         if (fallback) {
             F.reserve(sizeof(int32_t) * std::max(n, 1));
             for (int32_t i = 0; i < n; i++)
                 if (fallback[i] < 0 || fallback[i] >= MB_NUM_SCHEDULES)
                     mb::fail(MB_ERR_INVALID, "fallback schedule out of range");
-            if (n) MB_CUDA(cudaMemcpy(F.p, fallback, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+            mb::copy_sync(ctx->c.stream, F.p, fallback, sizeof(int32_t) * n);
         }
         mb::mlp_pick(ctx->c, W.as<float>(), X.as<float>(), fallback ? F.as<int32_t>() : nullptr, n,
                      O.as<int32_t>());
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
-        if (n) MB_CUDA(cudaMemcpy(out, O.p, sizeof(int32_t) * n, cudaMemcpyDefault));
+        mb::copy_sync(ctx->c.stream, out, O.p, sizeof(int32_t) * n);
         X.release();
         O.release();
         F.release();
@@ -442,9 +443,9 @@ int mb_graph_from_edges(mb_ctx *ctx, int32_t V, int64_t E, const int32_t *src, c
             bd.reserve(eb);
             if (w) bw.reserve(eb);
             if (E > 0) {
-                MB_CUDA(cudaMemcpy(bs.p, src, 4 * (size_t)E, cudaMemcpyDefault));
-                MB_CUDA(cudaMemcpy(bd.p, dst, 4 * (size_t)E, cudaMemcpyDefault));
-                if (w) MB_CUDA(cudaMemcpy(bw.p, w, 4 * (size_t)E, cudaMemcpyDefault));
+                mb::copy_sync(ctx->c.stream, bs.p, src, 4 * (size_t)E);
+                mb::copy_sync(ctx->c.stream, bd.p, dst, 4 * (size_t)E);
+                if (w) mb::copy_sync(ctx->c.stream, bw.p, w, 4 * (size_t)E);
             }
             mb::graph_build_from_device_edges(ctx->c, g->g, V, E, bs.as<uint32_t>(),
                                               bd.as<uint32_t>(), w ? bw.as<float>() : nullptr, flags);
@@ -540,13 +541,13 @@ int mb_graph_export(mb_ctx *ctx, const mb_graph *g, int32_t *row, int32_t *col, 
         use_device(ctx);
         const mb::Graph &G = g->g;
         const size_t vb = sizeof(int32_t) * (size_t)(G.V + 1), eb = sizeof(int32_t) * (size_t)G.E;
-        if (row) MB_CUDA(cudaMemcpy(row, G.row.p, vb, cudaMemcpyDefault));
-        if (rrow) MB_CUDA(cudaMemcpy(rrow, G.rrow.p, vb, cudaMemcpyDefault));
+        if (row) mb::copy_sync(ctx->c.stream, row, G.row.p, vb);
+        if (rrow) mb::copy_sync(ctx->c.stream, rrow, G.rrow.p, vb);
         if (G.E > 0) {
-            if (col) MB_CUDA(cudaMemcpy(col, G.col.p, eb, cudaMemcpyDefault));
-            if (w) MB_CUDA(cudaMemcpy(w, G.wt.p, eb, cudaMemcpyDefault));
-            if (rcol) MB_CUDA(cudaMemcpy(rcol, G.rcol.p, eb, cudaMemcpyDefault));
-            if (mslot) MB_CUDA(cudaMemcpy(mslot, G.mslot.p, eb, cudaMemcpyDefault));
+            if (col) mb::copy_sync(ctx->c.stream, col, G.col.p, eb);
+            if (w) mb::copy_sync(ctx->c.stream, w, G.wt.p, eb);
+            if (rcol) mb::copy_sync(ctx->c.stream, rcol, G.rcol.p, eb);
+            if (mslot) mb::copy_sync(ctx->c.stream, mslot, G.mslot.p, eb);
         }
     });
 }

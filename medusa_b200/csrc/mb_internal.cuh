@@ -162,6 +162,18 @@ struct Context {
     }
 };
 
+// Blocking copy ordered with the library's stream.  The stream is
+// non-blocking, so a plain cudaMemcpy (legacy default stream) is not ordered
+// with it, and a host-to-device cudaMemcpy from pageable memory may return
+// before its data has landed: a kernel queued next on the stream could read
+// the buffer early.  Every copy into a buffer that the stream's kernels read,
+// or out of one they write, goes through here.
+inline void copy_sync(cudaStream_t s, void *dst, const void *src, size_t n) {
+    if (!n) return;
+    MB_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyDefault, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+}
+
 // Pointer classification for the C ABI: device pointers are used in place,
 // anything else is treated as host memory and staged.
 inline bool is_device_ptr(const void *p) {

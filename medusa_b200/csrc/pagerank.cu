@@ -398,7 +398,7 @@ void build_meg_order(Context &ctx, const Graph &g, PrState &st) {
     const int64_t E = g.E;
     cudaStream_t s = ctx.stream;
     std::vector<int32_t> row((size_t)V + 1);
-    MB_CUDA(cudaMemcpy(row.data(), g.row.p, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyDeviceToHost));
+    copy_sync(ctx.stream, row.data(), g.row.p, sizeof(int32_t) * ((size_t)V + 1));
     // GraphIR::sortByDegree: std::sort of the vertices in id order by a
     // degree-descending comparator.  The permutation std::sort produces
     // depends only on the comparison results, so sorting (degree, id)
@@ -464,7 +464,7 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     // heavy-vertex work list, built once per graph from the in-degree offsets:
     // one item per block; hubs (more than one block) get block-sum slots
     std::vector<int32_t> rrow(V + 1);
-    MB_CUDA(cudaMemcpy(rrow.data(), g.rrow.p, sizeof(int32_t) * (V + 1), cudaMemcpyDeviceToHost));
+    copy_sync(ctx.stream, rrow.data(), g.rrow.p, sizeof(int32_t) * (V + 1));
     std::vector<int4> it;
     std::vector<int32_t> hv, hf;
     int32_t slots = 0;
@@ -494,9 +494,9 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     hub_v.reserve(sizeof(int32_t) * std::max<size_t>(hv.size(), 1));
     hub_first.reserve(sizeof(int32_t) * hf.size());
     blk_sum.reserve(sizeof(float) * std::max<int32_t>(slots, 1));
-    if (nitems) MB_CUDA(cudaMemcpy(items.p, it.data(), sizeof(int4) * it.size(), cudaMemcpyHostToDevice));
-    if (nhub) MB_CUDA(cudaMemcpy(hub_v.p, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice));
-    MB_CUDA(cudaMemcpy(hub_first.p, hf.data(), 4 * hf.size(), cudaMemcpyHostToDevice));
+    copy_sync(ctx.stream, items.p, it.data(), sizeof(int4) * it.size());
+    copy_sync(ctx.stream, hub_v.p, hv.data(), 4 * hv.size());
+    copy_sync(ctx.stream, hub_first.p, hf.data(), 4 * hf.size());
     // light lists: the vertices with in-degree <= kPrLight and their in-edges
     std::vector<int32_t> lv, lr(1, 0);
     lv.reserve((size_t)V);
@@ -512,8 +512,8 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     light_row.reserve(sizeof(int32_t) * lr.size());
     light_col.reserve(sizeof(int32_t) * std::max<size_t>((size_t)lr.back(), 1));
     if (nlight) {
-        MB_CUDA(cudaMemcpy(light_v.p, lv.data(), 4 * lv.size(), cudaMemcpyHostToDevice));
-        MB_CUDA(cudaMemcpy(light_row.p, lr.data(), 4 * lr.size(), cudaMemcpyHostToDevice));
+        copy_sync(ctx.stream, light_v.p, lv.data(), 4 * lv.size());
+        copy_sync(ctx.stream, light_row.p, lr.data(), 4 * lr.size());
         k_light_copy<<<grid_for(nlight, 256, ctx.num_sms * 16), 256, 0, ctx.stream>>>(
             light_v.as<int32_t>(), light_row.as<int32_t>(), nlight, g.rrow.as<int32_t>(),
             g.rcol.as<int32_t>(), light_col.as<int32_t>());
