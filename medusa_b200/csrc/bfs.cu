@@ -422,12 +422,15 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BfsArgs a, int cap) {
     __shared__ uint32_t s_off[kTailEntries];
     __shared__ int32_t s_row[kTailEntries];
     __shared__ int s_go;
-    Ctrl *c = a.f.ctrl;
+    __shared__ Ctrl s_ctrl;  // shadow of the control block (plain loads only)
+    Ctrl *const gc = a.f.ctrl;
+    ctrl_shadow_in(&s_ctrl, gc);
+    Ctrl *c = &s_ctrl;
     for (;;) {
-        const int cur = ldg2(&c->cur), nxt = cur ^ 1;
-        const unsigned long long q = ldg2(&c->q[cur]);
+        const int cur = c->cur, nxt = cur ^ 1;
+        const unsigned long long q = c->q[cur];
         const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
-        const int32_t lvl = ldg2(&c->step) + 1;
+        const int32_t lvl = c->step + 1;
         const int32_t *qv = pick(a.f.qv, cur);
         const uint32_t *qo = pick(a.f.qo, cur);
         for (uint32_t j = threadIdx.x; j < n; j += kTailThreads) {
@@ -457,20 +460,19 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(BfsArgs a, int cap) {
         flush_counts(c, cn, 0);
         __syncthreads();
         if (threadIdx.x == 0) {
-            __threadfence();
-            finish_superstep(c, APP_BFS, a.f.V, a.f.E, FMT_QUEUE);
+            finish_superstep<false>(c, APP_BFS, a.f.V, a.f.E, FMT_QUEUE);
             c->iter++;
             if (c->iter > cap && !c->done) {
                 c->err |= ERR_STEP_CAP;
                 c->done = 1;
             }
             s_go = !c->done && c->branch == kBranchTail;
-            __threadfence();
         }
         __syncthreads();
         if (!s_go) break;
     }
     if (threadIdx.x == 0) c->pending = 0;
+    ctrl_shadow_out(gc, c);
 }
 
 // Persistent BSP kernel (cooperative launch, all blocks resident): runs

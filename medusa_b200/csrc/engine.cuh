@@ -254,6 +254,25 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
     if (out_fmt != FMT_QUEUE) c->prev_nf = c->nf;
 }
 
+// The single-CTA tails run with a shadow of the control block in shared
+// memory (no other kernel runs while a tail does): the per-superstep
+// bookkeeping of thread 0 and the counter atomics of every thread then cost
+// shared-memory latency, not a chain of L2 round trips.  Code given the
+// shadow reads it with plain loads (ldg2 / ctl_ld<true> address global
+// memory only).  Called by every thread of the CTA.
+static_assert(sizeof(Ctrl) % 8 == 0, "control block copied in 8-byte words");
+__device__ inline void ctrl_shadow_in(Ctrl *s, const Ctrl *g) {
+    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long *>(s)[i] = reinterpret_cast<const unsigned long long *>(g)[i];
+    __syncthreads();
+}
+__device__ inline void ctrl_shadow_out(Ctrl *g, const Ctrl *s) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long *>(g)[i] = reinterpret_cast<const unsigned long long *>(s)[i];
+    __threadfence();
+}
+
 // Every engine kernel counts itself once (block 0, thread 0).
 __device__ __forceinline__ void count_launch(Ctrl *c) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&c->p.launches, 1u);

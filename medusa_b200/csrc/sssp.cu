@@ -530,14 +530,14 @@ __global__ void __launch_bounds__(256) k_msg_combine_update(SsspArgs a) {
 // near-far buckets are on (their far pile lives in global memory).
 __device__ void tail_global(const SsspArgs &a, int cap, uint32_t *s_off, int32_t *s_row, float *s_du,
                             int &s_go) {
-    Ctrl *c = a.f.ctrl;
+    Ctrl *c = a.f.ctrl;  // the shared-memory shadow (plain loads)
     for (;;) {
-        const int cur = ldg2(&c->cur), nxt = cur ^ 1;
-        const unsigned long long q = ldg2(&c->q[cur]);
+        const int cur = c->cur, nxt = cur ^ 1;
+        const unsigned long long q = c->q[cur];
         const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
-        const int32_t sv = ldg2(&c->step) + 1;
+        const int32_t sv = c->step + 1;
         const float delta = c->p.delta;
-        const float thresh = delta > 0.f ? ldg2(&c->thresh) : 3.0e38f;
+        const float thresh = delta > 0.f ? c->thresh : 3.0e38f;
         const int32_t *qv = pick(a.f.qv, cur);
         const uint32_t *qo = pick(a.f.qo, cur);
         for (uint32_t j = threadIdx.x; j < n; j += kTailThreads) {
@@ -575,15 +575,13 @@ __device__ void tail_global(const SsspArgs &a, int cap, uint32_t *s_off, int32_t
         flush_counts(c, cn, 0);
         __syncthreads();
         if (threadIdx.x == 0) {
-            __threadfence();
-            finish_superstep(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
+            finish_superstep<false>(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
             c->iter++;
             if (c->iter > cap && !c->done) {
                 c->err |= ERR_STEP_CAP;
                 c->done = 1;
             }
             s_go = !c->done && c->branch == kBranchTail;
-            __threadfence();
         }
         __syncthreads();
         if (!s_go) break;
@@ -752,7 +750,6 @@ __device__ void tail_smem(const SsspArgs &a, int cap, char *smem, int &s_go) {
             c->q[nxt] = ((unsigned long long)n2 << 32) | m2;
             c->acc_n = n2;
             c->acc_m = 0;
-            __threadfence();
             finish_superstep<false>(c, APP_SSSP, a.f.V, a.f.E, FMT_QUEUE);
             c->iter++;
             if (c->iter > cap && !c->done) {
@@ -760,7 +757,6 @@ __device__ void tail_smem(const SsspArgs &a, int cap, char *smem, int &s_go) {
                 c->done = 1;
             }
             s_go = !c->done && c->branch == kBranchTail;
-            __threadfence();
         }
         __syncthreads();
         if (!s_go) break;
@@ -793,14 +789,20 @@ __global__ void __launch_bounds__(kTailThreads, MB_TAIL_MIN_BLOCKS) k_tail(SsspA
     count_launch(a.f.ctrl);
     extern __shared__ __align__(16) char smem[];
     __shared__ int s_go;
-    if (a.f.ctrl->p.delta > 0.f) {
-        tail_global(a, cap, (uint32_t *)smem, (int32_t *)(smem + 4 * kTailEntries),
+    __shared__ Ctrl s_ctrl;  // shadow of the control block (plain loads only)
+    Ctrl *const gc = a.f.ctrl;
+    ctrl_shadow_in(&s_ctrl, gc);
+    SsspArgs sa = a;
+    sa.f.ctrl = &s_ctrl;
+    if (s_ctrl.p.delta > 0.f) {
+        tail_global(sa, cap, (uint32_t *)smem, (int32_t *)(smem + 4 * kTailEntries),
                     (float *)(smem + 8 * kTailEntries), s_go);
     } else {
-        tail_smem(a, cap, smem, s_go);
+        tail_smem(sa, cap, smem, s_go);
     }
     // every superstep this kernel ran is finished already
-    if (threadIdx.x == 0) a.f.ctrl->pending = 0;
+    if (threadIdx.x == 0) s_ctrl.pending = 0;
+    ctrl_shadow_out(gc, &s_ctrl);
 }
 
 // Near-far split: the threshold was just raised by delta; every far-pile
