@@ -261,6 +261,7 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
 // shadow reads it with plain loads (ldg2 / ctl_ld<true> address global
 // memory only).  Called by every thread of the CTA.
 static_assert(sizeof(Ctrl) % 8 == 0, "control block copied in 8-byte words");
+static_assert(offsetof(Ctrl, q) % 8 == 0, "the select kernel writes back from q on, in 8-byte words");
 __device__ inline void ctrl_shadow_in(Ctrl *s, const Ctrl *g) {
     for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x)
         reinterpret_cast<unsigned long long *>(s)[i] = reinterpret_cast<const unsigned long long *>(g)[i];
@@ -346,9 +347,10 @@ __device__ __forceinline__ uint32_t tail_mask(int64_t w, int32_t V) {
 // One full warp: finish the superstep that ran (frontier bookkeeping and
 // the choice of the next schedule), then, under the learned policy, run the
 // MLP on the features it left.
+template <bool kPrefetch = true>
 __device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
     Ctrl *c = a.ctrl;
-    {
+    if (kPrefetch) {
         // the control block's lines and the run parameters' head, all at once
         const int lane = threadIdx.x & 31;
         const char *hot = (const char *)&c->q[0];
@@ -397,12 +399,29 @@ static __global__ void k_select(FrontierArgs a, int app, int cap,
                                 cudaGraphConditionalHandle h_cont,
                                 cudaGraphConditionalHandle h_branch, int nbranch,
                                 int use_handles) {
-    Ctrl *c = a.ctrl;
-    count_launch(c);
-    bookkeep_warp(a, app);
+    // the warp copies the control block into shared memory (all loads in
+    // flight at once), thread 0 does the bookkeeping there, and the warp
+    // writes back the part after the run parameters (the only part the
+    // bookkeeping changes; the launch count is added in global memory)
+    Ctrl *const gc = a.ctrl;
+    count_launch(gc);
+    __shared__ Ctrl s_ctrl;
+    ctrl_shadow_in(&s_ctrl, gc);
+    FrontierArgs sa = a;
+    sa.ctrl = &s_ctrl;
+    bookkeep_warp<false>(sa, app);
+    Ctrl *c = &s_ctrl;
+    if (threadIdx.x == 0) {
+        count_iteration(c, cap);
+        if (!c->done) c->pending = 1;
+    }
+    __syncwarp();
+    {
+        constexpr int kFrom = (int)(offsetof(Ctrl, q) / 8), kTo = (int)(sizeof(Ctrl) / 8);
+        for (int i = kFrom + (int)threadIdx.x; i < kTo; i += (int)blockDim.x)
+            reinterpret_cast<unsigned long long *>(gc)[i] = reinterpret_cast<const unsigned long long *>(c)[i];
+    }
     if (threadIdx.x != 0) return;
-    count_iteration(c, cap);
-    if (!c->done) c->pending = 1;
     if (!use_handles) return;
     if (c->done) {
         cudaGraphSetConditional(h_branch, (unsigned)nbranch);  // no branch
