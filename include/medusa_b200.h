@@ -300,7 +300,11 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                   would give a resident warp fewer than four groups) */
 #define MB_TUNE_PR_SHORT_PAIR 7 /* PageRank: heavy-vertex blocks of <= 512 in-edges
                                    folded at once by one warp, 1, 2 or 4 (default 2) */
-#define MB_NUM_TUNABLES 8
+#define MB_TUNE_BFS_ALPHA 8 /* BFS fixed rule: bottom-up once frontier out-edges x alpha
+                               exceed the unvisited out-edges (default 15; 0: never) */
+#define MB_TUNE_BFS_BETA 9 /* BFS fixed rule: back to top-down below V / beta frontier
+                              vertices (default 20) */
+#define MB_NUM_TUNABLES 10
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

@@ -66,7 +66,9 @@ def tune_bfs(ctx, g, source=0, reps=3):
     """Persistent-tail size and the push / per-vertex grids for BFS on g."""
     space = {"tail_edges": [-1, 2048, 4096, 6144],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
-             "vertex_blocks_per_sm": [-1, 4, 12, 16]}
+             "vertex_blocks_per_sm": [-1, 4, 12, 16],
+             "bfs_alpha": [-1, 0, 4, 60],
+             "bfs_beta": [-1, 5, 80]}
     return tune(ctx, lambda: g.bfs([source])[1], space, reps)
 
 
@@ -84,7 +86,9 @@ def tune_traversals(ctx, g, source=0, reps=3):
              "sssp_delta": [0.0, -1.0, 100.0, 1000.0, 10000.0],
              "tail_edges": [-1, 2048, 4096],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
-             "vertex_blocks_per_sm": [-1, 4, 12, 16]}
+             "vertex_blocks_per_sm": [-1, 4, 12, 16],
+             "bfs_alpha": [-1, 0, 4, 60],
+             "bfs_beta": [-1, 5, 80]}
     return tune(ctx, run, space, reps)
 
 

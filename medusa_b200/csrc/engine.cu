@@ -19,6 +19,8 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->replay_then_fixed = ctx.replay_then_fixed ? 1 : 0;
     p->max_step = ctx.max_step;
     p->bm_push_min = bm_push_min;
+    p->bfs_alpha = ctx.tunable[MB_TUNE_BFS_ALPHA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_ALPHA] : 15;
+    p->bfs_beta = ctx.tunable[MB_TUNE_BFS_BETA] > 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_BETA] : 20;
     p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0
                         ? (uint32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_TAIL_EDGES], kTailEdges)
                         : kTailEdges;

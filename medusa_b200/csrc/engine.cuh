@@ -126,9 +126,9 @@ __device__ inline int route(const struct Ctrl *c, int s);
 __device__ inline int fixed_rule(const Ctrl *c, int app, int32_t V, int64_t E, uint32_t n,
                                  uint64_t m) {
     if (app == APP_SSSP) return MB_SCHED_PUSH_EDGE_QUEUE;
-    const int64_t alpha = 15, beta = 20;
+    const int64_t alpha = c->p.bfs_alpha, beta = c->p.bfs_beta;  // default 15 and 20
     if (c->mode == FMT_QUEUE) {
-        if ((int64_t)m * alpha > c->m_unvisited) return MB_SCHED_PULL_THREAD;
+        if (alpha > 0 && (int64_t)m * alpha > c->m_unvisited) return MB_SCHED_PULL_THREAD;
         return MB_SCHED_PUSH_EDGE_QUEUE;
     }
     if ((int64_t)n * beta < (int64_t)V && n < c->prev_nf) return MB_SCHED_PUSH_EDGE_QUEUE;

@@ -24,6 +24,9 @@ struct RunParams {
     uint32_t tail_edges;        // schedule 0 frontiers up to this many out-edges run in the tail
     uint32_t bm_push_min;       // SSSP: schedule 0 on a queue frontier with at least this many
                                 // out-edges writes a bitmap compacted after (0: never)
+    int32_t bfs_alpha;          // BFS fixed rule: go bottom-up when frontier out-edges * alpha
+                                // exceed the unvisited out-edges (0: never)
+    int32_t bfs_beta;           // BFS fixed rule: back to top-down below V / beta frontier vertices
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 

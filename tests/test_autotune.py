@@ -57,3 +57,24 @@ def test_tune_pagerank_keeps_results(gpu_ctx):
         g.close()
         gpu_ctx.set_tunable("pr_light_vpl", -1)
         gpu_ctx.set_tunable("pr_short_pair", -1)
+
+
+def test_bfs_rule_tunables_keep_levels(gpu_ctx):
+    """The direction-optimising rule's alpha (0: never bottom-up) and beta
+    change only which schedule runs: levels stay those of the default rule."""
+    from medusa_b200 import api
+    g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.45, 0.15, 0.15, seed=5))
+    try:
+        lv0, st0 = g.bfs([0])
+        assert st0["schedule_count"][4] > 0  # the default rule pulls on this graph
+        for alpha, beta in ((0, 20), (1, 1), (1000, 1000), (4, 5)):
+            gpu_ctx.set_tunable("bfs_alpha", alpha)
+            gpu_ctx.set_tunable("bfs_beta", beta)
+            lv, st = g.bfs([0])
+            np.testing.assert_array_equal(lv, lv0)
+            if alpha == 0:
+                assert st["schedule_count"][4] == 0
+    finally:
+        g.close()
+        gpu_ctx.set_tunable("bfs_alpha", -1)
+        gpu_ctx.set_tunable("bfs_beta", -1)
