@@ -3,7 +3,9 @@ single-kernel captures) and quick timings:
 
     python -m medusa_b200.profile_cases CASE [--reps N] [--hostloop]
 
-CASE: c2-bfs, c2-sssp (R-MAT 2^20 / 2^24, source 0), c1-pr (uniform
+CASE: c2-bfs, c2-sssp (R-MAT 2^20 / 2^24, source 0), c2-msssp (the same
+graph, SSSP from sources 0..31 in one batched traversal), c4a-msssp (R-MAT
+2^22 / 2^26, sources 0..31), c1-pr (uniform
 2^18 / 2^22, 10 supersteps), c5-bfs, c5-sssp (R-MAT 2^24 / 2^28,
 (0.57,0.19,0.19,0.05)), c5-pr (20 supersteps), c3-bfs, c3-sssp (1448^2
 grid), c5s-bfs, c5s-sssp, c5s-pr (the C5 generator at 2^21 / 2^25: a case
@@ -23,6 +25,8 @@ SEED = 1
 def params(case):
     if case.startswith("c2"):
         return api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000)
+    if case.startswith("c4a"):
+        return api.rmat_params(22, 1 << 26, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000)
     if case.startswith("c1"):
         return api.uniform_params(1 << 18, 1 << 22, seed=SEED)
     if case.startswith("c5s"):
@@ -54,6 +58,8 @@ def main(argv=None):
             _, st = g.bfs([0])
         elif kind == "sssp":
             _, st = g.sssp([0])
+        elif kind == "msssp":
+            _, st = g.sssp(list(range(32)))
         elif kind == "pr":
             _, st = g.pagerank(20 if args.case.startswith("c5") else 10, 1.0 / g.V)
         else:
