@@ -71,36 +71,15 @@ __device__ __forceinline__ void pr_write(const PrArgs &a, int32_t v, float sum) 
 
 // Streamed index arrays (read once per superstep) bypass L1, which is left
 // to the contribution gathers: a hot source's contribution then stays in L1
-// for the next warps that gather it.
-#ifndef MB_PR_STREAM
-#define MB_PR_STREAM 2
-#endif
-#ifndef MB_PR_GATHER
-#define MB_PR_GATHER 0
-#endif
+// for the next warps that gather it (4% at 2^28 edges; an evict_last hint on
+// the gathers measured 5% slower).
 __device__ __forceinline__ int32_t ld_stream(const int32_t *p) {
-#if MB_PR_STREAM == 0
-    return __ldg(p);
-#elif MB_PR_STREAM == 1
-    return __ldcg(p);
-#elif MB_PR_STREAM == 2
     int32_t v;
     asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
-#else
-    return __ldcs(p);
-#endif
 }
 
-__device__ __forceinline__ float ld_gather(const float *p) {
-#if MB_PR_GATHER == 1
-    float v;
-    asm("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
-#else
-    return __ldg(p);
-#endif
-}
+__device__ __forceinline__ float ld_gather(const float *p) { return __ldg(p); }
 
 template <bool kFromMsg>
 __device__ __forceinline__ float edge_val(const PrArgs &a, int64_t j) {
@@ -581,10 +560,6 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     const void *light_fn[3] = {(const void *)k_pr_light<1>, (const void *)k_pr_light<2>,
                                (const void *)k_pr_light<4>};
     const int pi = pair == 1 ? 0 : pair == 2 ? 1 : 2, vi = vpl == 1 ? 0 : vpl == 2 ? 1 : 2;
-#ifdef MB_PR_CARVEOUT
-    for (int f = 0; f < 2; f++)
-        MB_CUDA(cudaFuncSetAttribute(heavy_fn[f][pi], cudaFuncAttributePreferredSharedMemoryCarveout, MB_PR_CARVEOUT));
-#endif
     const int64_t heavy_threads = heavy_units(st.nitems, st.nlong, pair) * 32;
     const int grid_heavy[2] = {grid_for(heavy_threads, 256, resident(heavy_fn[0][pi], 256)),
                                grid_for(heavy_threads, 256, resident(heavy_fn[1][pi], 256))};
