@@ -304,7 +304,10 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                exceed the unvisited out-edges (default 15; 0: never) */
 #define MB_TUNE_BFS_BETA 9 /* BFS fixed rule: back to top-down below V / beta frontier
                               vertices (default 20) */
-#define MB_NUM_TUNABLES 10
+#define MB_TUNE_BULK_STAGE 10 /* SSSP edge-balanced push: 1 stages each tile's queue
+                                 entries into shared memory by bulk copies on the
+                                 TMA engine, 0 by the threads' loads (default 0) */
+#define MB_NUM_TUNABLES 11
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

@@ -58,7 +58,8 @@ def tune_sssp(ctx, g, source=0, reps=3):
     """Bitmap-output push threshold and push grid for SSSP on graph g."""
     E = max(int(g.E), 1)
     space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
-             "push_blocks_per_sm": [-1, 4, 6, 12, 16]}
+             "push_blocks_per_sm": [-1, 4, 6, 12, 16],
+             "bulk_stage": [-1, 1]}
     return tune(ctx, lambda: g.sssp([source])[1], space, reps)
 
 
@@ -88,7 +89,8 @@ def tune_traversals(ctx, g, source=0, reps=3):
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
-             "bfs_beta": [-1, 5, 80]}
+             "bfs_beta": [-1, 5, 80],
+             "bulk_stage": [-1, 1]}
     return tune(ctx, run, space, reps)
 
 

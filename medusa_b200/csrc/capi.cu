@@ -296,6 +296,8 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "BFS alpha / beta must be <= 2^20");
     if (which == MB_TUNE_BFS_BETA && value == 0)
         return set_error(ctx, MB_ERR_INVALID, "BFS beta must be >= 1");
+    if (which == MB_TUNE_BULK_STAGE && value > 1)
+        return set_error(ctx, MB_ERR_INVALID, "bulk staging is 0 or 1");
     ctx->c.tunable[which] = value;
     ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
     return MB_OK;

@@ -111,6 +111,7 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
         MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
         MB_CUDA(cudaStreamSynchronize(s));
         if (hc->err & ERR_STEP_CAP) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": superstep cap reached");
+        if (hc->err & ERR_BULK) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a bulk copy timed out");
         if (hc->err & ERR_BARRIER)
             fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a persistent-grid barrier timed out");
         if (stats) {

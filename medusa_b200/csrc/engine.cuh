@@ -21,6 +21,7 @@ namespace mb {
 constexpr int FMT_QUEUE = 0, FMT_BITMAP = 1, FMT_NONE = 2;
 constexpr int ERR_STEP_CAP = 1;
 constexpr int ERR_BARRIER = 2;     // a grid barrier of the persistent kernel gave up
+constexpr int ERR_BULK = 4;        // a bulk copy into shared memory did not complete in time
 // Internal step of near-far SSSP (not a user schedule): raise the distance
 // threshold and move far-pile vertices below it into the near queue.
 constexpr int kSchedSplit = MB_NUM_SCHEDULES;
@@ -584,8 +585,9 @@ struct FrontierState {
         const size_t tiles = (size_t)(E / kTile) + 2;
         for (int i = 0; i < 2; i++) {
             bm[i].reserve(sizeof(uint32_t) * (size_t)W);
-            qv[i].reserve(sizeof(int32_t) * (size_t)V);
-            qo[i].reserve(sizeof(uint32_t) * (size_t)V);
+            // +8: bulk copies of a tile's entries round their end up to 16 bytes
+            qv[i].reserve(sizeof(int32_t) * ((size_t)V + 8));
+            qo[i].reserve(sizeof(uint32_t) * ((size_t)V + 8));
             tf[i].reserve(sizeof(int32_t) * tiles);
         }
         ctrl.reserve(sizeof(Ctrl));

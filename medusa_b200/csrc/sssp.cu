@@ -28,6 +28,7 @@
 //     segmented min per destination, update
 //   7 full Bellman-Ford pull over every in-edge (the reference CPU form)
 #include "sssp.cuh"
+#include "bulk.cuh"
 
 namespace mb {
 namespace {
@@ -81,8 +82,16 @@ __device__ __forceinline__ void far_push(const SsspArgs &a, Ctrl *c, bool pred, 
 }
 
 // schedule 0: push, merge-path edge-balanced over the queue
+// A tile's queue entries (offsets and vertices) come into shared memory by
+// the threads' own loads, or (kBulk, MB_TUNE_BULK_STAGE) by one bulk copy
+// each on the TMA engine.  A tile holds at most kTile + 1 entries; the bulk
+// copy rounds their range out to 16-byte boundaries (at most 3 entries on
+// each side).  Measured on B200 the two are within 1% of each other.
+constexpr int kStage = kTile + 8;
 struct PushSmem {
-    uint32_t off[kTile + 1];
+    alignas(16) uint32_t qo_st[kStage];  // the offsets (threads' loads: from index 0)
+    alignas(16) int32_t qv_st[kStage];   // the vertices (bulk copies only)
+    uint64_t bar;
     int32_t row[kTile + 1];
     float du[kTile + 1];
     BlockQueue bq;
@@ -100,13 +109,19 @@ struct PushSmem {
 // kBmOut: instead of claiming each improved vertex (an atomic with a
 // result) and appending it to the next queue, set its bit in a.nbm with a
 // fire-and-forget atomicOr; k_nbm2q then builds the next queue.
-template <bool kBmOut>
+template <bool kBmOut, bool kBulk = false>
 __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm) {
-    uint32_t *s_off = sm.off;
+    uint32_t parity = 0;
     int32_t *s_row = sm.row;
     float *s_du = sm.du;
     BlockQueue &bq = sm.bq;
-    if (threadIdx.x == 0) bq.n = 0;
+    if (threadIdx.x == 0) {
+        bq.n = 0;
+        if (kBulk) {
+            mbar_init(&sm.bar, 1);
+            fence_barrier_init();
+        }
+    }
     __syncthreads();
     Ctrl *c = a.f.ctrl;
     const int cur = c->cur, nxt = cur ^ 1;
@@ -120,16 +135,48 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
     const int32_t *tf = pick(a.f.tf, cur);
     const uint32_t tiles = (m + kTile - 1) / kTile;
     uint32_t cn = 0;
-    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint32_t c0 = t * kTile, c1 = min(c0 + kTile, m);
+    bool stop = false;  // block-uniform: a bulk copy timed out
+    for (uint32_t t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
+        const uint32_t c0 = t * kTile;
+        uint32_t c1 = min(c0 + kTile, m);
         const int32_t i0 = tf[t];
         const int32_t i1 = (t + 1 < tiles) ? tf[t + 1] : (int32_t)n - 1;
-        const int k = i1 - i0 + 1;
-        for (int j = threadIdx.x; j < k; j += blockDim.x) {
-            const int32_t u = qv[i0 + j];
-            s_off[j] = qo[i0 + j];
-            s_row[j] = a.row[u];
-            s_du[j] = ld_dist(a, u);
+        int k = i1 - i0 + 1;
+        // entries [a0, a1) with a0 = i0 rounded down, a1 = i1 + 1 rounded up
+        // to 4 entries (16 bytes); the queues hold V + 8 entries
+        const int32_t a0 = i0 & ~3, a1 = (i1 + 1 + 3) & ~3;
+        if (kBulk && threadIdx.x == 0) {
+            const uint32_t bytes = 4u * (uint32_t)(a1 - a0);  // <= 4 * kStage
+            fence_proxy_async_smem();  // the last tile's reads of the stage buffers came first
+            mbar_arrive_expect_tx(&sm.bar, 2 * bytes);
+            bulk_g2s(sm.qo_st, qo + a0, bytes, &sm.bar);
+            bulk_g2s(sm.qv_st, qv + a0, bytes, &sm.bar);
+        }
+        const bool staged = !kBulk || mbar_wait(&sm.bar, parity);  // the same for every thread
+        if (!staged) {  // never seen: record it, give the copies one more
+            // bounded wait, and relax nothing more
+            if (threadIdx.x == 0) atomicOr(&c->err, ERR_BULK);
+            mbar_wait(&sm.bar, parity);
+            k = 0;
+            c1 = c0;
+            stop = true;
+        }
+        parity ^= 1u;
+        const uint32_t *s_off = sm.qo_st + (kBulk ? i0 - a0 : 0);
+        if (kBulk) {
+            const int32_t *s_qv = sm.qv_st + (i0 - a0);
+            for (int j = threadIdx.x; j < k; j += blockDim.x) {
+                const int32_t u = s_qv[j];
+                s_row[j] = a.row[u];
+                s_du[j] = ld_dist(a, u);
+            }
+        } else {
+            for (int j = threadIdx.x; j < k; j += blockDim.x) {
+                const int32_t u = qv[i0 + j];
+                sm.qo_st[j] = qo[i0 + j];
+                s_row[j] = a.row[u];
+                s_du[j] = ld_dist(a, u);
+            }
         }
         __syncthreads();
         // the thread's kTileItems CONSECUTIVE edges: one binary search for the
@@ -209,19 +256,22 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
         }
         bq_flush(bq, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt), pick(a.f.tf, nxt));
     }
-    flush_counts(c, cn, 0);
+    flush_counts(c, cn, 0);  // ends with a CTA barrier
+    if (kBulk && threadIdx.x == 0) mbar_inval(&sm.bar);  // a later call initialises it again
 }
 
+template <bool kBulk>
 __global__ void __launch_bounds__(kPushThreads) k_push_edge_q(SsspArgs a) {
     __shared__ PushSmem sm;
     count_launch(a.f.ctrl);
-    work_push_edge_q<false>(a, sm);
+    work_push_edge_q<false, kBulk>(a, sm);
 }
 
+template <bool kBulk>
 __global__ void __launch_bounds__(kPushThreads) k_push_edge_bm(SsspArgs a) {
     __shared__ PushSmem sm;
     count_launch(a.f.ctrl);
-    work_push_edge_q<true>(a, sm);
+    work_push_edge_q<true, kBulk>(a, sm);
 }
 
 // After k_push_edge_bm: next-frontier bitmap -> next queue (with the
@@ -1017,6 +1067,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
 
     const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
+    const bool bulk = ctx.tunable[MB_TUNE_BULK_STAGE] > 0;
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
     const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
@@ -1054,7 +1105,8 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
             return;
         }
         if (branch == kBranchPushBm) {
-            k_push_edge_bm<<<grid_push, kPushThreads, 0, s>>>(a);
+            if (bulk) k_push_edge_bm<true><<<grid_push, kPushThreads, 0, s>>>(a);
+            else k_push_edge_bm<false><<<grid_push, kPushThreads, 0, s>>>(a);
             k_nbm2q<<<grid_vtx, kPushThreads, 0, s>>>(a);
             MB_CHECK_LAUNCH();
             return;
@@ -1070,7 +1122,10 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
             MB_CHECK_LAUNCH();
         }
         switch (sched) {
-            case MB_SCHED_PUSH_EDGE_QUEUE: k_push_edge_q<<<grid_push, kPushThreads, 0, s>>>(a); break;
+            case MB_SCHED_PUSH_EDGE_QUEUE:
+                if (bulk) k_push_edge_q<true><<<grid_push, kPushThreads, 0, s>>>(a);
+                else k_push_edge_q<false><<<grid_push, kPushThreads, 0, s>>>(a);
+                break;
             case MB_SCHED_PUSH_WARP_QUEUE: k_push_warp_q<<<grid_push, kPushThreads, 0, s>>>(a); break;
             case MB_SCHED_PUSH_EDGE_BITMAP:
                 k_bm_clear<<<grid_vtx, 256, 0, s>>>(a.f, 1);

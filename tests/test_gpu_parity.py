@@ -67,6 +67,28 @@ def test_sssp_matches_reference(ctx, name):
     g.close()
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_sssp_bulk_staged_push_matches_reference(ctx, api, name):
+    """The edge-balanced pushes with each tile's queue entries brought into
+    shared memory by TMA bulk copies (queue and bitmap output, the latter
+    forced by a threshold of one edge): distances equal the reference's."""
+    c = load_golden(name)
+    g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    ctx.set_tunable("bulk_stage", 1)
+    try:
+        for bm_min in (-1, 1):
+            ctx.set_tunable("sssp_bm_push_min", bm_min)
+            ctx.set_tunable("tail_edges", 0)  # every superstep on the multi-CTA pushes
+            for i, s in enumerate(c["sources"]):
+                d, st = g.sssp([s])
+                np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32),
+                                              err_msg="bm_push_min %d" % bm_min)
+    finally:
+        for k in ("bulk_stage", "sssp_bm_push_min", "tail_edges"):
+            ctx.set_tunable(k, -1)
+        g.close()
+
+
 def check_pagerank(got, ref, r64, indeg, tol=1e-5, hub=2048):
     from test_oracle import check_pagerank as chk
     chk(got, ref, r64, indeg, tol, hub)
