@@ -307,7 +307,9 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
 #define MB_TUNE_BULK_STAGE 10 /* SSSP edge-balanced push: 1 stages each tile's queue
                                  entries into shared memory by bulk copies on the
                                  TMA engine, 0 by the threads' loads (default 0) */
-#define MB_NUM_TUNABLES 11
+#define MB_TUNE_BFS_GAMMA 11 /* BFS fixed rule: bottom-up only while the frontier has
+                                at least E / gamma out-edges (default 16; 0: no floor) */
+#define MB_NUM_TUNABLES 12
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

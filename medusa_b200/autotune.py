@@ -69,7 +69,8 @@ def tune_bfs(ctx, g, source=0, reps=3):
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
-             "bfs_beta": [-1, 5, 80]}
+             "bfs_beta": [-1, 5, 80],
+             "bfs_gamma": [-1, 0, 64]}
     return tune(ctx, lambda: g.bfs([source])[1], space, reps)
 
 
@@ -90,6 +91,7 @@ def tune_traversals(ctx, g, source=0, reps=3):
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
              "bfs_beta": [-1, 5, 80],
+             "bfs_gamma": [-1, 0, 64],
              "bulk_stage": [-1, 1]}
     return tune(ctx, run, space, reps)
 

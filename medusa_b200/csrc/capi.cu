@@ -292,7 +292,8 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
     if ((which == MB_TUNE_PR_LIGHT_VPL || which == MB_TUNE_PR_SHORT_PAIR) &&
         !(value == -1 || value == 1 || value == 2 || value == 4))
         return set_error(ctx, MB_ERR_INVALID, "PageRank lane/pair counts must be 1, 2 or 4");
-    if ((which == MB_TUNE_BFS_ALPHA || which == MB_TUNE_BFS_BETA) && value > (1 << 20))
+    if ((which == MB_TUNE_BFS_ALPHA || which == MB_TUNE_BFS_BETA || which == MB_TUNE_BFS_GAMMA) &&
+        value > (1 << 20))
         return set_error(ctx, MB_ERR_INVALID, "BFS alpha / beta must be <= 2^20");
     if (which == MB_TUNE_BFS_BETA && value == 0)
         return set_error(ctx, MB_ERR_INVALID, "BFS beta must be >= 1");

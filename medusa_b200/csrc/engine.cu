@@ -21,6 +21,7 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->bm_push_min = bm_push_min;
     p->bfs_alpha = ctx.tunable[MB_TUNE_BFS_ALPHA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_ALPHA] : 15;
     p->bfs_beta = ctx.tunable[MB_TUNE_BFS_BETA] > 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_BETA] : 20;
+    p->bfs_gamma = ctx.tunable[MB_TUNE_BFS_GAMMA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_GAMMA] : kBfsGammaDefault;
     p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0
                         ? (uint32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_TAIL_EDGES], kTailEdges)
                         : kTailEdges;

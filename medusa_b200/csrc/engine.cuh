@@ -128,8 +128,14 @@ __device__ inline int fixed_rule(const Ctrl *c, int app, int32_t V, int64_t E, u
                                  uint64_t m) {
     if (app == APP_SSSP) return MB_SCHED_PUSH_EDGE_QUEUE;
     const int64_t alpha = c->p.bfs_alpha, beta = c->p.bfs_beta;  // default 15 and 20
+    const int64_t gamma = c->p.bfs_gamma;
     if (c->mode == FMT_QUEUE) {
-        if (alpha > 0 && (int64_t)m * alpha > c->m_unvisited) return MB_SCHED_PULL_THREAD;
+        // bottom-up only for a frontier that is large in absolute terms too
+        // (at least E / gamma out-edges): near the end of a high-diameter
+        // traversal the unvisited out-edges run low while the frontier stays
+        // small, and a pull over every unvisited vertex costs more than the push
+        if (alpha > 0 && (int64_t)m * alpha > c->m_unvisited && (gamma == 0 || (int64_t)m * gamma >= E))
+            return MB_SCHED_PULL_THREAD;
         return MB_SCHED_PUSH_EDGE_QUEUE;
     }
     if ((int64_t)n * beta < (int64_t)V && n < c->prev_nf) return MB_SCHED_PUSH_EDGE_QUEUE;

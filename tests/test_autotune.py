@@ -60,16 +60,18 @@ def test_tune_pagerank_keeps_results(gpu_ctx):
 
 
 def test_bfs_rule_tunables_keep_levels(gpu_ctx):
-    """The direction-optimising rule's alpha (0: never bottom-up) and beta
-    change only which schedule runs: levels stay those of the default rule."""
+    """The direction-optimising rule's alpha (0: never bottom-up), beta and
+    gamma (the frontier-size floor for bottom-up) change only which schedule
+    runs: levels stay those of the default rule."""
     from medusa_b200 import api
     g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.45, 0.15, 0.15, seed=5))
     try:
         lv0, st0 = g.bfs([0])
         assert st0["schedule_count"][4] > 0  # the default rule pulls on this graph
-        for alpha, beta in ((0, 20), (1, 1), (1000, 1000), (4, 5)):
+        for alpha, beta, gamma in ((0, 20, 16), (1, 1, 0), (1000, 1000, 0), (4, 5, 1000), (15, 20, 1)):
             gpu_ctx.set_tunable("bfs_alpha", alpha)
             gpu_ctx.set_tunable("bfs_beta", beta)
+            gpu_ctx.set_tunable("bfs_gamma", gamma)
             lv, st = g.bfs([0])
             np.testing.assert_array_equal(lv, lv0)
             if alpha == 0:
@@ -78,3 +80,4 @@ def test_bfs_rule_tunables_keep_levels(gpu_ctx):
         g.close()
         gpu_ctx.set_tunable("bfs_alpha", -1)
         gpu_ctx.set_tunable("bfs_beta", -1)
+        gpu_ctx.set_tunable("bfs_gamma", -1)
