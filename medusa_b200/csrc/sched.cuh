@@ -52,23 +52,19 @@ __host__ __device__ inline void make_features(float *f, float n, float m, float 
 // Inference by one full warp; returns the argmax in every lane.  Schedules
 // whose bit is clear in `allowed` are never picked.  Latency matters (it
 // runs between supersteps), so every weight load is issued first, all of
-// them independent and coalesced: lane j holds column j of each weight row,
-// and a row's dot product with the previous layer (lane j holding unit j)
-// is a warp all-reduce.  ~50 loads per lane in flight at once, then ~40
-// butterfly reductions.
-__device__ __forceinline__ float warp_allsum_f(float x) {
-#pragma unroll
-    for (int off = 16; off; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-    return x;
-}
-
-// The MLP's weights as one warp holds them (per lane: column `lane` of
-// every weight row, its own biases).
+// them independent: lane i holds row i of W1 and W2 and row i mod 8 of W3
+// (16-byte loads), and computes unit i from the previous layer's units,
+// which arrive by one shuffle each -- 32 shuffles and FMAs per layer instead
+// of a 5-step all-reduce per unit.
+// The MLP's weights as one warp holds them (per lane i: row i of W1 and W2,
+// row i mod kOut of W3, its own biases).
 struct MlpRegs {
-    float w1r[kFeat], w2r[kHid], w3r[kOut];
+    float w1r[kFeat], w2r[kHid], w3r[kHid];
     float bias1, bias2, bias3;
     float lo, hi;  // lane i < kFeat: training range of feature i
 };
+static_assert(MlpLayout::w2 % 4 == 0 && MlpLayout::w3 % 4 == 0 && kHid % 4 == 0,
+              "W2 and W3 rows are read as float4");
 
 // Issue every weight load (independent, coalesced); callers start this
 // before other work so the loads' latency overlaps it.
@@ -76,10 +72,20 @@ __device__ __forceinline__ void mlp_load_warp(const float *__restrict__ P, MlpRe
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int i = 0; i < kFeat; i++) r.w1r[i] = __ldg(&P[MlpLayout::w1 + lane * kFeat + i]);
+    const float4 *w2 = reinterpret_cast<const float4 *>(P + MlpLayout::w2 + lane * kHid);
+    const float4 *w3 = reinterpret_cast<const float4 *>(P + MlpLayout::w3 + (lane % kOut) * kHid);
 #pragma unroll
-    for (int i = 0; i < kHid; i++) r.w2r[i] = __ldg(&P[MlpLayout::w2 + i * kHid + lane]);
-#pragma unroll
-    for (int k = 0; k < kOut; k++) r.w3r[k] = __ldg(&P[MlpLayout::w3 + k * kHid + lane]);
+    for (int q = 0; q < kHid / 4; q++) {
+        const float4 x = __ldg(&w2[q]), y = __ldg(&w3[q]);
+        r.w2r[4 * q] = x.x;
+        r.w2r[4 * q + 1] = x.y;
+        r.w2r[4 * q + 2] = x.z;
+        r.w2r[4 * q + 3] = x.w;
+        r.w3r[4 * q] = y.x;
+        r.w3r[4 * q + 1] = y.y;
+        r.w3r[4 * q + 2] = y.z;
+        r.w3r[4 * q + 3] = y.w;
+    }
     r.bias1 = __ldg(&P[MlpLayout::b1 + lane]);
     r.bias2 = __ldg(&P[MlpLayout::b2 + lane]);
     r.bias3 = __ldg(&P[MlpLayout::b3 + (lane < kOut ? lane : 0)]);
@@ -101,21 +107,25 @@ __device__ inline int mlp_decide_warp(const MlpRegs &r, const float *f, unsigned
 #pragma unroll
     for (int i = 0; i < kFeat; i++) h1 = fmaf(r.w1r[i], f[i], h1);
     h1 = fmaxf(h1, 0.f);
-    // layer 2: unit i = sum over lanes j of w2[i][j] * h1[j]; lane i keeps it
-    float h2 = 0.f;
+    // layer 2: lane i computes unit i = sum_j w2[i][j] * h1[j], h1[j] from
+    // lane j (two accumulators halve the dependent FMA chain)
+    float s0 = r.bias2, s1 = 0.f;
 #pragma unroll
-    for (int i = 0; i < kHid; i++) {
-        const float sum = warp_allsum_f(r.w2r[i] * h1);
-        if (lane == i) h2 = sum;
+    for (int j = 0; j < kHid; j += 2) {
+        s0 = fmaf(r.w2r[j], __shfl_sync(0xffffffffu, h1, j), s0);
+        s1 = fmaf(r.w2r[j + 1], __shfl_sync(0xffffffffu, h1, j + 1), s1);
     }
-    h2 = fmaxf(h2 + r.bias2, 0.f);
-    float o = 0.f;
+    const float h2 = fmaxf(s0 + s1, 0.f);
+    // layer 3: lane k < kOut computes output k (the other lanes' values are
+    // discarded below)
+    s0 = r.bias3;
+    s1 = 0.f;
 #pragma unroll
-    for (int k = 0; k < kOut; k++) {
-        const float sum = warp_allsum_f(r.w3r[k] * h2);
-        if (lane == k) o = sum;
+    for (int j = 0; j < kHid; j += 2) {
+        s0 = fmaf(r.w3r[j], __shfl_sync(0xffffffffu, h2, j), s0);
+        s1 = fmaf(r.w3r[j + 1], __shfl_sync(0xffffffffu, h2, j + 1), s1);
     }
-    o += r.bias3;
+    float o = s0 + s1;
     const float o_fb = __shfl_sync(0xffffffffu, o, fallback >= 0 ? (fallback & 31) : 0);
     if (lane >= kOut || !((allowed >> lane) & 1u)) o = -3.0e38f;
     int best = lane < kOut ? lane : kOut;
