@@ -36,6 +36,16 @@ def test_library_exports_every_declared_symbol(api):
     assert not missing, missing
 
 
+def test_tunable_ids_match_the_header(api):
+    """api.TUNABLES names every MB_TUNE_* of include/medusa_b200.h with the
+    same id, and nothing else."""
+    text = open(os.path.join(ROOT, "include", "medusa_b200.h")).read()
+    ids = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"#define MB_TUNE_(\w+) (\d+)", text)}
+    count = int(re.search(r"#define MB_NUM_TUNABLES (\d+)", text).group(1))
+    assert ids == api.TUNABLES
+    assert sorted(ids.values()) == list(range(count))
+
+
 def test_version(api):
     assert "sm_100a" in api.version()
 
