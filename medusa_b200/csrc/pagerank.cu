@@ -12,13 +12,15 @@
 // The sum runs in the fixed order of pr_order.cuh, the same for every
 // schedule, so schedules never change a bit of the result.  Work mapping:
 //   light vertices (in-degree <= kPrLight): their in-edge sources are copied
-//     once per graph into a compacted list; one warp per 128 consecutive
-//     light vertices streams their in-edges through a shared-memory window
-//     (coalesced) and each lane folds its own vertices (k_pr_light; the
-//     message-reading schedule uses k_pr_pull over the full reverse CSR);
+//     once per graph into a compacted list; one warp per 32 x VPL (1, 2 or
+//     4) consecutive light vertices streams their in-edges through a
+//     shared-memory window (coalesced) and each lane folds its own vertices
+//     (k_pr_light; the message-reading schedule uses k_pr_pull over the
+//     full reverse CSR);
 //   heavier vertices: their kPrBlock-edge blocks form a work list built once
 //     per graph, one 16-byte item per block (edge range, vertex, slot); one
-//     warp per item (k_heavy_blocks).  A vertex with a single block is
+//     warp per long item, or 1, 2 or 4 short items per warp
+//     (k_heavy_blocks).  A vertex with a single block is
 //     finished there (update and next contribution); a hub's blocks write
 //     block sums that k_hub_finalize folds in order -- so hubs and the long
 //     tail of R-MAT's hundreds-to-thousands in-degrees spread over every SM
@@ -190,7 +192,8 @@ __global__ void k_hub_finalize(PrArgs a) {
     }
 }
 
-// Main combine+update: one warp per 32 consecutive vertices.  The warp
+// Combine+update over the full reverse CSR (the message-reading schedule and
+// the reference's MEG order): one warp per 32 consecutive vertices.  The warp
 // streams the group's in-edges (contiguous in reverse-CSR order) through a
 // shared-memory window, coalesced; each lane then folds its own vertex's
 // part of the window in order.  kAllLight (the reference's MEG order): every
