@@ -1,0 +1,43 @@
+"""The autotuner's search on the host (no GPU): coordinate descent over a
+fake context whose run time is a known function of the settings."""
+from medusa_b200 import autotune
+
+
+class FakeCtx:
+    def __init__(self):
+        self.t = {"a": -1, "b": -1}
+        self.sssp_delta = 0.0
+
+    def get_tunable(self, name):
+        return self.t[name]
+
+    def set_tunable(self, name, value):
+        self.t[name] = value
+
+    def set_sssp_delta(self, value):
+        self.sssp_delta = value
+
+
+def cost(ctx):
+    # best at a = 4, b = 16, delta = 100, separable
+    a = 8 if ctx.t["a"] == -1 else ctx.t["a"]
+    b = 32 if ctx.t["b"] == -1 else ctx.t["b"]
+    return {"device_ms": abs(a - 4) + abs(b - 16) / 4 + abs(ctx.sssp_delta - 100) / 100 + 1.0}
+
+
+def test_coordinate_descent_finds_the_separable_optimum_and_leaves_it_set():
+    ctx = FakeCtx()
+    space = {"a": [-1, 2, 4, 6], "b": [-1, 8, 16], "sssp_delta": [0.0, 100.0, 1000.0]}
+    best, table = autotune.tune(ctx, lambda: cost(ctx), space, reps=1)
+    assert best == {"a": 4, "b": 16, "sssp_delta": 100.0}
+    assert ctx.t == {"a": 4, "b": 16} and ctx.sssp_delta == 100.0
+    # the default setting, then every other candidate of every tunable once
+    assert len(table) == 1 + 3 + 2 + 2
+    assert min(ms for _, ms in table) == cost(ctx)["device_ms"]
+
+
+def test_a_worse_candidate_is_never_kept():
+    ctx = FakeCtx()
+    ctx.t["a"] = 4
+    best, _ = autotune.tune(ctx, lambda: cost(ctx), {"a": [-1, 0, 100]}, reps=3)
+    assert best["a"] == 4 and ctx.t["a"] == 4
