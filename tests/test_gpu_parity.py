@@ -275,7 +275,7 @@ def test_bad_arguments_fail_loudly(gpu_ctx, api):
     g.close()
 
 
-# ---- full-size property checks (BASELINE sizes) --------------------------------
+# ---- full-size property checks (R-MAT 2^20 / 2^24, 1448^2 grid) ---------------
 
 def bfs_certificate(V, src, dst, lv, s):
     """Levels are BFS levels iff: lv[s]=0; every edge from a reached vertex
