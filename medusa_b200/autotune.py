@@ -65,7 +65,7 @@ def tune_sssp(ctx, g, source=0, reps=3):
 
 def tune_bfs(ctx, g, source=0, reps=3):
     """Persistent-tail size and the push / per-vertex grids for BFS on g."""
-    space = {"tail_edges": [-1, 2048, 4096, 6144],
+    space = {"tail_edges": [-1, 0, 2048, 4096, 6144],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
@@ -86,7 +86,7 @@ def tune_traversals(ctx, g, source=0, reps=3):
 
     space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "sssp_delta": [0.0, -1.0, 100.0, 1000.0, 10000.0],
-             "tail_edges": [-1, 2048, 4096],
+             "tail_edges": [-1, 0, 2048, 4096],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
