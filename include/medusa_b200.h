@@ -124,7 +124,7 @@ int mb_set_schedule_replay(mb_ctx *ctx, const int8_t *schedules, int32_t n);
  * reference relaxes every edge every superstep, SSSP/CPUFunctorHoster.cpp:58-99). */
 int mb_set_sssp_delta(mb_ctx *ctx, float delta);
 /* 1 (default): supersteps of schedule 0 whose queue frontier is small (at
- * most 2048 vertices and 16384 out-edges) run in one persistent CTA, several
+ * most 2048 vertices and 8192 out-edges, MB_TUNE_TAIL_EDGES) run in one persistent CTA, several
  * supersteps per launch; 0: every superstep is a grid-wide launch.  Results
  * are identical either way. */
 int mb_set_persistent_tail(mb_ctx *ctx, int enable);
