@@ -60,6 +60,7 @@ SEED = 1
 C2 = dict(scale=20, num_edges=1 << 24, a=0.45, b=0.15, c=0.15, wmin=1, wmax=1000)
 C1 = dict(num_vertices=1 << 18, num_edges=1 << 22)
 PR_ITERS = 10
+C3_SAMPLE_SIDE = 512  # the C3 CPU baseline's grid side (a bounded sample)
 TRAIN_SCALES = (14, 17, 20)  # log2 vertices of the scheduler's trace graphs
 TRAIN_ROUNDS = 3  # trace collections: fixed-rule trajectories, then the learned policy's
 METRIC = "BFS/SSSP GTEPS (R-MAT 2^20 V / 2^24 E, source 0)"
@@ -83,6 +84,19 @@ def c2_params(api):
 
 def c1_params(api):
     return api.uniform_params(C1["num_vertices"], C1["num_edges"], seed=SEED)
+
+
+def host_edges(kind, **params):
+    """A workload's edge list made on the CPU by the oracle's generator (the
+    same edges the product's generator makes; the CPU legs load nothing from
+    the product library)."""
+    from oracle import oracle as O
+    return O.generate(kind, **params)
+
+
+def c2_edges():
+    return host_edges("rmat", scale=C2["scale"], num_edges=C2["num_edges"], a=C2["a"], b=C2["b"],
+                      c=C2["c"], seed=SEED, wmin=C2["wmin"], wmax=C2["wmax"])
 
 
 class ClockSampler:
@@ -477,6 +491,13 @@ def bench_configs(ctx, api, args, flush):
                       "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk),
                       "autotuned": {k: float(v) for k, v in tuned3.items()}}
     g.close()
+    if not args.no_cpu_baseline:
+        out["c3_grid"]["cpu_baseline"] = cpu_baseline_traversals(
+            host_edges("grid", rows=C3_SAMPLE_SIDE, cols=C3_SAMPLE_SIDE, drop_frac=0.1,
+                       shortcut_frac=0.005, seed=SEED, wmin=1, wmax=100),
+            "one BFS + one SSSP from the corner of a %dx%d grid of the same generator (the "
+            "1448x1448 grid's reference run takes minutes: its edge-centric sweeps scale with the "
+            "diameter)" % (C3_SAMPLE_SIDE, C3_SAMPLE_SIDE))
     reset_tunables(ctx, api)
     del lv, dd
     # C4a: 64 BFS + 32 SSSP sources on R-MAT 2^22 / 2^26, batched vs one loop per source
@@ -535,21 +556,25 @@ def bench_configs(ctx, api, args, flush):
         r = scheduler.evaluate(ctx, X, T, F, model)
         per_step[name] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
     c5["per_superstep"] = per_step
-    if not args.no_autotune:
-        tuned5.update(autotune.tune_pagerank(ctx, g, 20, reps=2, out=rk)[0])
-    g.pagerank(20, 1.0 / V, out=rk)
-    mp, sp = _timed(lambda: g.pagerank(20, 1.0 / V, out=rk)[1], reps, flush)
-    per = mp / 20
-    b = 8 * E + 16 * V + 4
-    c5["pagerank"] = {"ms_per_superstep": round(per, 4),
-                      "edges_per_s": round(E / (per / 1e3), 1),
-                      "roofline": {"achieved_gbs": round(b / (per / 1e3) / 1e9, 1),
-                                   "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}}
     c5["autotuned"] = {k: float(v) for k, v in tuned5.items()}
-    out["c5_scale"] = c5
-    g.close()
     reset_tunables(ctx, api)
+    pres, pranks = time_pagerank_orders(ctx, api, g, 20, flush, reps, not args.no_autotune, rk)
+    b = 8 * E + 16 * V + 4
+    for name in pres:
+        per = pres[name]["ms_per_superstep"]
+        pres[name]["roofline"] = {"achieved_gbs": round(b / (per / 1e3) / 1e9, 1),
+                                  "frac": round(b / (per / 1e3) / 1e9 / pk, 4)}
+    c5["pagerank"] = dict(pres["reference_order"])
+    c5["pagerank"]["summation_order"] = "the reference's (MEG slots, sequential float fold), default"
+    c5["pagerank"]["fixed_order"] = pres["fixed_order"]
+    g.close()
     del lv, dd, rk
+    if not args.no_cpu_baseline:
+        V_, s_, d_, _ = host_edges("rmat", scale=24, num_edges=1 << 28, a=0.57, b=0.19, c=0.19,
+                                   seed=SEED)
+        c5["pagerank"]["accuracy"] = pr_accuracy(V_, s_, d_, 20, pranks)
+        del s_, d_
+    out["c5_scale"] = c5
     out["c4b_many_graphs"] = bench_many_graphs(ctx, api, reps, not args.no_autotune)
     return out
 
@@ -603,37 +628,123 @@ def bench_many_graphs(ctx, api, reps, tune=True):
     return res
 
 
+def pr_accuracy(V, src, dst, iters, ranks):
+    """PageRank errors, per run: each result's max relative error per vertex
+    against the reference's FP32 ranks (the oracle's sequential fold in the
+    reference's MEG order, bit-identical to the reference's CPU code on the
+    golden graphs) and its L1 error against the FP64 oracle (absolute, and
+    relative to the FP64 ranks' sum).  ranks: {name: float32 array}."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    aa = O.AAGraph(V, src, dst)
+    ref = O.pagerank(V, aa, None, iters, 1.0 / V).astype(np.float64)
+    r64 = O.pagerank(V, aa, None, iters, 1.0 / V, fp64=True)
+    del aa
+    out = {"reference_fp32_l1_vs_fp64": float(np.abs(ref - r64).sum()),
+           "fp64_rank_sum": float(r64.sum())}
+    for name, r in ranks.items():
+        r = r.astype(np.float64)
+        out[name] = {"max_rel_vs_reference": float((np.abs(r - ref) / ref).max()),
+                     "vertices_above_1e-5": int(((np.abs(r - ref) / ref) > 1e-5).sum()),
+                     "bit_identical_to_reference": bool(np.array_equal(r, ref)),
+                     "l1_vs_fp64": float(np.abs(r - r64).sum()),
+                     "l1_vs_fp64_relative": float(np.abs(r - r64).sum() / r64.sum())}
+    out["oracle_seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
+def time_pagerank_orders(ctx, api, g, iters, flush, reps, tune, out):
+    """Device ms per superstep and the ranks of both summation orders: the
+    reference's (default; autotuned hub threshold and light packing) and the
+    fixed parallel order (autotuned light packing and short-block pairing)."""
+    from medusa_b200 import autotune
+    res, ranks = {}, {}
+    for name, order in (("reference_order", api.MB_PR_ORDER_REFERENCE),
+                        ("fixed_order", api.MB_PR_ORDER_FIXED)):
+        ctx.set_pagerank_order(order)
+        tuned = {}
+        if tune:
+            tuned = autotune.tune_pagerank(ctx, g, iters, reps=2, out=out)[0]
+        g.pagerank(iters, 1.0 / g.V, out=out)
+        ms, st = _timed(lambda: g.pagerank(iters, 1.0 / g.V, out=out)[1], reps, flush)
+        ranks[name] = out.cpu().numpy().copy()
+        res[name] = {"ms_per_superstep": round(ms / iters, 5),
+                     "edges_per_s": round(g.E / (ms / iters / 1e3), 1),
+                     "kernel_launches": st["kernel_launches"],
+                     "autotuned": {k: float(v) for k, v in tuned.items()}}
+        for k in tuned:
+            ctx.set_tunable(k, -1)
+    ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
+    return res, ranks
+
+
 def bench_pagerank(ctx, api, args, flush):
+    """C1: uniform 2^18 / 2^22, 10 supersteps from 1/N, both summation orders
+    with their errors, and the reference's own CPU PageRank on the same graph."""
     import torch
     p = c1_params(api)
     g = ctx.generate(p)
     V, E = g.V, g.E
     r = torch.empty(V, dtype=torch.float32, device="cuda")
-    tuned = {}
-    if not args.no_autotune:
-        from medusa_b200 import autotune
-        tuned = autotune.tune_pagerank(ctx, g, PR_ITERS, reps=3, out=r)[0]
-    for _ in range(max(args.warmup, 1)):
-        g.pagerank(PR_ITERS, 1.0 / V, out=r)
-    ms = 0.0
-    for _ in range(args.steps):
-        flush_l2(flush)
-        torch.cuda.synchronize()
-        _, st = g.pagerank(PR_ITERS, 1.0 / V, out=r)
-        ms += st["device_ms"]
-    per_iter_ms = ms / args.steps / PR_ITERS
+    res, ranks = time_pagerank_orders(ctx, api, g, PR_ITERS, flush, max(args.steps, 3),
+                                      not args.no_autotune, r)
+    g.close()
     pk, _ = peaks()
     b = 8 * E + 16 * V + 4
+    per_iter_ms = res["reference_order"]["ms_per_superstep"]
     ach = b / (per_iter_ms / 1e3) / 1e9
-    g.close()
-    for k in tuned:
-        ctx.set_tunable(k, -1)
-    return {"workload": "uniform 2^18 vertices, 2^22 edges, seed 1, 10 supersteps from 1/N",
-            "autotuned": {k: float(v) for k, v in tuned.items()},
-            "edges_per_s": round(E / (per_iter_ms / 1e3), 1), "ms_per_superstep": round(per_iter_ms, 5),
-            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": pk, "unit": "GB/s",
-                         "frac": round(ach / pk, 4),
-                         "bytes_per_superstep": b, "formula": "8*E + 16*V + 4"}}
+    out = {"workload": "uniform 2^18 vertices, 2^22 edges, seed 1, 10 supersteps from 1/N",
+           "edges_per_s": round(E / (per_iter_ms / 1e3), 1), "ms_per_superstep": per_iter_ms,
+           "summation_order": "the reference's (MEG slots, sequential float fold), default",
+           "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": pk, "unit": "GB/s",
+                        "frac": round(ach / pk, 4),
+                        "bytes_per_superstep": b, "formula": "8*E + 16*V + 4"},
+           "orders": res}
+    if not args.no_cpu_baseline:
+        V_, s_, d_, _ = host_edges("uniform", num_vertices=C1["num_vertices"],
+                                   num_edges=C1["num_edges"], seed=SEED)
+        out["accuracy"] = pr_accuracy(V_, s_, d_, PR_ITERS, ranks)
+        out["cpu_baseline"] = cpu_baseline_pagerank(V_, s_, d_, PR_ITERS)
+    return out
+
+
+def cpu_baseline_pagerank(V, src, dst, iters):
+    """The reference's own CPU PageRank (oracle/_ref: MPG's sortByDegree +
+    buildMEG + its per-vertex send/update functions, OpenMP) on the graph."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref not built"}
+    nthr = min(os.cpu_count() or 1, 24)
+    rp = O.RefGraph("pr", V, src, dst)
+    ms = []
+    for _ in range(3):
+        _, m = rp.pagerank(iters, 1.0 / V, nthr)
+        ms.append(m)
+    rp.close()
+    per = float(np.median(ms)) / iters
+    return {"value": round(len(src) / (per / 1e3), 1), "unit": "edges/s per superstep",
+            "ms_per_superstep": round(per, 3), "cores": nthr, "kind": "reference",
+            "sample": "%d supersteps on the full C1 graph, median of 3 runs" % iters}
+
+
+def cpu_baseline_traversals(edges, sample):
+    """The reference's CPU BFS and SSSP (oracle/_ref, OpenMP) from vertex 0 of
+    the graph `edges` = (V, src, dst, w)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"unavailable": "oracle/_ref not built"}
+    V, s, d, w = edges
+    nthr = min(os.cpu_count() or 1, 24)
+    gb = O.RefGraph("bfs", V, s, d)
+    lv, ms_b = gb.bfs(0, nthr)
+    gb.close()
+    gs = O.RefGraph("sssp", V, s, d, w)
+    dd, ms_s = gs.sssp(0, nthr)
+    gs.close()
+    outdeg = np.bincount(s, minlength=V)
+    er = int(outdeg[lv >= 0].sum()) + int(outdeg[dd < 1e9].sum())
+    return {"value": round(er / ((ms_b + ms_s) / 1e3) / 1e9, 5), "unit": "GTEPS", "cores": nthr,
+            "kind": "reference", "sample": sample, "bfs_ms": round(ms_b, 2), "sssp_ms": round(ms_s, 2)}
 
 
 def cpu_baseline(api, args):
@@ -641,7 +752,7 @@ def cpu_baseline(api, args):
     from oracle import oracle as O
     if not O.ref_available():
         return {"unavailable": "oracle/_ref not built"}
-    V, s, d, w = api.generate_edges_host(c2_params(api))
+    V, s, d, w = c2_edges()
     nthr = min(os.cpu_count() or 1, 24)
     gb = O.RefGraph("bfs", V, s, d)
     lv, ms_b = gb.bfs(0, nthr)
@@ -662,12 +773,11 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from medusa_b200 import api
     from oracle import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
         return
-    V, s, d, w = api.generate_edges_host(c2_params(api))
+    V, s, d, w = c2_edges()
     nthr = min(os.cpu_count() or 1, 24)
     gb = O.RefGraph("bfs", V, s, d)
     gs = O.RefGraph("sssp", V, s, d, w)

@@ -16,14 +16,38 @@
  *   while (exe) { ResetToExecute(); Medusa_Exec(); exe = RetriveToExecute();
  *                 MGLOBAL::super_step++; }    // SSSP/main.cu:369-382
  *
- * and that code keeps its shape here.  What changes is where application
- * data lives: the reference generates per-application SoA arrays and device
- * proxies with accessors (get_distance / set_distance, SSSP/DeviceDataStructure.h)
- * from the app's Vertex/Edge structs; here an application keeps its vertex
- * and edge attributes in medusa::DeviceArray<T> and its functors index them
- * with v.index / e.index.  The graph itself (CSR in the reference's AA edge
- * order, the reverse CSR whose positions are the message slots msgDstID) is
- * the library's (mb_graph_device_view).
+ * and that code keeps its shape here.  The reference generates, per
+ * application, SoA arrays and device proxies with accessors (get_distance /
+ * set_distance, SSSP/DeviceDataStructure.h:160-246) from the app's Vertex and
+ * Edge structs.  Here the application lists its attributes once, before
+ * including this header, and the same accessors, host arrays and device
+ * arrays are generated from the list:
+ *
+ *   #define MEDUSA_VERTEX_FIELDS(F) F(MVT, distance) F(bool, updated)
+ *   #define MEDUSA_EDGE_FIELDS(F)   // none: weight is the graph's own
+ *   #include <medusa/medusa.h>
+ *
+ * gives D_Vertex::get_distance() / set_distance(x) / get_updated() /
+ * set_updated(b), the host arrays MGLOBAL::gpu_def[0].vertexArray.distance[i]
+ * (sized by InitHostDS, uploaded by InitDeviceDS) and
+ * MGLOBAL::gpu_def[0].d_vertexArray.Dump(vertexArray) to read them back, as in
+ * the reference's main.cu files.  The structural attributes (edge_count,
+ * msg_index, edge_index, the edge's endpoints and weight) come from the
+ * graph and are not listed.  An application may instead keep attributes in
+ * medusa::DeviceArray<T> and index them with v.index / e.index.
+ *
+ * The graph itself (CSR in the reference's AA edge order, the reverse CSR
+ * whose positions are the message slots msgDstID) is the library's
+ * (mb_graph_device_view).
+ *
+ * The reference's own three apps can route their whole loop to the
+ * library's hand-written kernels: one line after the functor declares that
+ * the functor IS the reference's BFS, SSSP or PageRank send over the named
+ * fields (MEDUSA_BUILTIN_BFS / _SSSP / _PAGERANK below), and
+ * FunctorHolder<EDGE>::Run then calls mb_bfs / mb_sssp / mb_pagerank_from on
+ * those fields instead of the generic functor kernels, when the fields hold
+ * the state the reference's main.cu sets up (checked at the call; otherwise
+ * the generic kernels run).
  *
  * Every name below is compiled into the including translation unit (nvcc,
  * -std=c++17); the functor kernels are templates instantiated for the app's
@@ -39,6 +63,7 @@
 #include <stdio.h>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -61,7 +86,7 @@ enum MessageMode { EDGE_MESSAGE, VERTEX_MESSAGE, NO_MESSAGE };
 enum CombinerOperator { CUDPP_ADD, CUDPP_MULTIPLY, CUDPP_MIN, CUDPP_MAX };
 enum CombinerDatatype { CUDPP_INT, CUDPP_UINT, CUDPP_FLOAT };
 /* MultipleGPU/MultiAPIHoster.h: the functor kinds of FunctorHolder */
-enum FunctorType { VERTEX, EDGE, EDGELIST, MESSAGE };
+enum FunctorType { VERTEX, EDGE, EDGELIST, MESSAGE, EDGE_HT };
 
 namespace medusa {
 
@@ -90,6 +115,34 @@ struct RunView {
 /* One copy per translation unit (internal linkage), as the functor kernels. */
 static __constant__ medusa::RunView medusa_run;
 
+/* ---- application attributes from a field list --------------------------- */
+#ifndef MEDUSA_VERTEX_FIELDS
+#define MEDUSA_VERTEX_FIELDS(F)
+#endif
+#ifndef MEDUSA_EDGE_FIELDS
+#define MEDUSA_EDGE_FIELDS(F)
+#endif
+#define MEDUSA_FIELD_PTR(T, name) T *name;
+namespace medusa {
+/* device addresses of the listed attributes (one array per field) */
+struct VertexFieldPtrs {
+    MEDUSA_VERTEX_FIELDS(MEDUSA_FIELD_PTR)
+    char unused_;
+};
+struct EdgeFieldPtrs {
+    MEDUSA_EDGE_FIELDS(MEDUSA_FIELD_PTR)
+    char unused_;
+};
+}  // namespace medusa
+static __constant__ medusa::VertexFieldPtrs medusa_vfields;
+static __constant__ medusa::EdgeFieldPtrs medusa_efields;
+#define MEDUSA_VERTEX_ACCESSORS(T, name)                                                  \
+    __device__ T get_##name() const { return medusa_vfields.name[index]; }              \
+    __device__ void set_##name(T value) const { medusa_vfields.name[index] = value; }
+#define MEDUSA_EDGE_ACCESSORS(T, name)                                                    \
+    __device__ T get_##name() const { return medusa_efields.name[index]; }              \
+    __device__ void set_##name(T value) const { medusa_efields.name[index] = value; }
+
 /* ---- device proxies ------------------------------------------------------ */
 
 /* MedusaRT/SystemLibGPU.h */
@@ -112,6 +165,7 @@ struct D_Edge {
     __device__ int get_msgDstID() const { return medusa_run.g.mslot[index]; }
     /* send a message along this edge: into the destination's slot msgDstID */
     __device__ void sendMsg(MVT v) const { medusa_run.msg[medusa_run.g.mslot[index]] = v; }
+    MEDUSA_EDGE_FIELDS(MEDUSA_EDGE_ACCESSORS)
 };
 
 /* The out-edges of one vertex (SSSP/DeviceDataStructure.h:70-80). */
@@ -134,6 +188,7 @@ struct D_Vertex {
     /* the combiner's result for this vertex (SSSP/DeviceDataStructure.h:221-235);
      * a vertex without messages gets the buffer's initial value */
     __device__ MVT get_combined_msg() const { return medusa_run.combined[index]; }
+    MEDUSA_VERTEX_FIELDS(MEDUSA_VERTEX_ACCESSORS)
 };
 
 namespace medusa {
@@ -204,6 +259,20 @@ struct DeviceArray {
     explicit DeviceArray(int64_t count) { resize(count); }
     DeviceArray(const DeviceArray &) = delete;
     DeviceArray &operator=(const DeviceArray &) = delete;
+    DeviceArray(DeviceArray &&o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DeviceArray &operator=(DeviceArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
     ~DeviceArray() { release(); }
     void resize(int64_t count) {
         release();
@@ -227,6 +296,92 @@ struct DeviceArray {
         if (n) upload(h.data());
     }
     T *data() const { return p; }
+};
+
+/* Host array of one attribute (bool-safe, unlike std::vector<bool>). */
+template <class T>
+struct HostArray {
+    std::unique_ptr<T[]> p;
+    int64_t n = 0;
+    void resize(int64_t count) {
+        p.reset(new T[(size_t)(count > 0 ? count : 1)]());
+        n = count;
+    }
+    T &operator[](int64_t i) { return p[(size_t)i]; }
+    const T &operator[](int64_t i) const { return p[(size_t)i]; }
+    T *data() const { return p.get(); }
+};
+
+/* The listed attributes as host arrays (the reference's VertexArray /
+ * EdgeArray, SSSP/VertexDataType.h, SSSP/EdgeDataType.h) and device arrays
+ * (D_VertexArray / D_EdgeArray, with Fill and Dump). */
+#define MEDUSA_HOST_FIELD(T, name) HostArray<T> name;
+#define MEDUSA_DEV_FIELD(T, name) DeviceArray<T> name;
+#define MEDUSA_RESIZE_FIELD(T, name) name.resize(count);
+#define MEDUSA_FILL_FIELD(T, name) \
+    name.resize(h.size);           \
+    if (h.size) name.upload(h.name.data());
+#define MEDUSA_DUMP_FIELD(T, name) \
+    if (size) name.download(h.name.data());
+#define MEDUSA_PTR_FIELD(T, name) out.name = name.p;
+struct VertexArray {
+    int size = 0;
+    MEDUSA_VERTEX_FIELDS(MEDUSA_HOST_FIELD)
+    void resize(int count) {
+        size = count;
+        MEDUSA_VERTEX_FIELDS(MEDUSA_RESIZE_FIELD)
+    }
+};
+struct D_VertexArray {
+    int size = 0;
+    MEDUSA_VERTEX_FIELDS(MEDUSA_DEV_FIELD)
+    void Fill(const VertexArray &h) {
+        size = h.size;
+        MEDUSA_VERTEX_FIELDS(MEDUSA_FILL_FIELD)
+    }
+    void Dump(VertexArray &h) const {
+        if (h.size != size) h.resize(size);
+        MEDUSA_VERTEX_FIELDS(MEDUSA_DUMP_FIELD)
+    }
+    VertexFieldPtrs ptrs() const {
+        VertexFieldPtrs out{};
+        MEDUSA_VERTEX_FIELDS(MEDUSA_PTR_FIELD)
+        return out;
+    }
+};
+struct EdgeArray {
+    int size = 0;
+    MEDUSA_EDGE_FIELDS(MEDUSA_HOST_FIELD)
+    void resize(int count) {
+        size = count;
+        MEDUSA_EDGE_FIELDS(MEDUSA_RESIZE_FIELD)
+    }
+};
+struct D_EdgeArray {
+    int size = 0;
+    MEDUSA_EDGE_FIELDS(MEDUSA_DEV_FIELD)
+    void Fill(const EdgeArray &h) {
+        size = h.size;
+        MEDUSA_EDGE_FIELDS(MEDUSA_FILL_FIELD)
+    }
+    void Dump(EdgeArray &h) const {
+        if (h.size != size) h.resize(size);
+        MEDUSA_EDGE_FIELDS(MEDUSA_DUMP_FIELD)
+    }
+    EdgeFieldPtrs ptrs() const {
+        EdgeFieldPtrs out{};
+        MEDUSA_EDGE_FIELDS(MEDUSA_PTR_FIELD)
+        return out;
+    }
+};
+/* One GPU's share of the application data (MultipleGPU/MultiGraphStorage.h's
+ * gpu_def[i]; one GPU here).  Edge attributes are indexed by the edge's
+ * position in the AA order (D_Edge::index). */
+struct GPUDef {
+    VertexArray vertexArray;
+    D_VertexArray d_vertexArray;
+    EdgeArray edgeArray;
+    D_EdgeArray d_edgeArray;
 };
 
 /* ---- graph construction ------------------------------------------------------ */
@@ -271,6 +426,9 @@ namespace medusa {
 struct Combiner {
     void combineAllDevice();
 };
+/* Which built-in path ran the last superstep (MEDUSA_BUILTIN_*), with the
+ * library's statistics of that call. */
+enum BuiltinApp { BUILTIN_NONE = 0, BUILTIN_BFS = 1, BUILTIN_SSSP = 2, BUILTIN_PAGERANK = 3 };
 struct Runtime {
     mb_ctx *ctx = nullptr;
     mb_graph *graph = nullptr;
@@ -278,6 +436,12 @@ struct Runtime {
     DeviceArray<MVT> msg, combined;
     DeviceArray<int> flag;
     MVT init_msg = (MVT)0;
+    bool fill_pending = false;      /* InitMessageBuffer ran; the fill waits for a reader */
+    int skip_step = -1;             /* a built-in path finished this superstep */
+    bool builtin_enabled = true;    /* route MEDUSA_BUILTIN_* functors to the library */
+    int64_t generic_launches = 0;   /* functor / combiner kernels launched */
+    BuiltinApp last_builtin = BUILTIN_NONE;
+    mb_stats builtin_stats{};
     int num_sms = 148;
     cudaStream_t stream = 0;
     void sync_view() {
@@ -295,6 +459,7 @@ struct Runtime {
         if (b > (int64_t)num_sms * 8) b = (int64_t)num_sms * 8;
         return (int)b;
     }
+    void fill_messages();
 };
 }  // namespace medusa
 
@@ -307,6 +472,7 @@ inline CombinerDatatype combiner_datatype = CUDPP_FLOAT;
 inline bool toExecute = false;
 inline medusa::Combiner com;
 inline medusa::Runtime rt;
+inline medusa::GPUDef gpu_def[1];
 }  // namespace MGLOBAL
 
 /* MultipleGPU/MultiPublicAPI.h:15-35.  gpu_num must be "1" (one GPU). */
@@ -323,6 +489,17 @@ inline void InitConfig(const char *gpu_num, const char *max_hop, MessageMode mm,
     MGLOBAL::rt.num_sms = prop.multiProcessorCount;
 }
 
+namespace medusa {
+/* After the graph is built: the application's host arrays are sized to it. */
+inline void graph_ready() {
+    auto &rt = MGLOBAL::rt;
+    medusa::check_mb(mb_graph_device_view(rt.graph, &rt.view), rt.ctx, "mb_graph_device_view");
+    medusa::check(cudaDeviceSynchronize(), "graph build");  // the library builds on its own stream
+    MGLOBAL::gpu_def[0].vertexArray.resize(rt.view.num_vertices);
+    MGLOBAL::gpu_def[0].edgeArray.resize((int)rt.view.num_edges);
+}
+}  // namespace medusa
+
 /* MultipleGPU/MultiPublicAPI.h:42-100: build the graph storage from the IR. */
 inline void InitHostDS(const medusa::GraphIR &ir) {
     auto &rt = MGLOBAL::rt;
@@ -332,8 +509,7 @@ inline void InitHostDS(const medusa::GraphIR &ir) {
     medusa::check_mb(mb_graph_from_edges(rt.ctx, ir.vertexNum, (int64_t)ir.src.size(), ir.src.data(),
                                          ir.dst.data(), ir.weight.data(), MB_ORDER_REFERENCE, &rt.graph),
                      rt.ctx, "mb_graph_from_edges");
-    medusa::check_mb(mb_graph_device_view(rt.graph, &rt.view), rt.ctx, "mb_graph_device_view");
-    medusa::check(cudaDeviceSynchronize(), "graph build");  // the library builds on its own stream
+    medusa::graph_ready();
 }
 
 /* The same from GTgraph text (parsed on the GPU), the reference's file format. */
@@ -348,11 +524,25 @@ inline void InitHostDSFromGTGraph(const std::string &path) {
     medusa::check_mb(mb_graph_from_gtgraph(rt.ctx, text.data(), (int64_t)text.size(), MB_ORDER_REFERENCE,
                                            &rt.graph),
                      rt.ctx, "mb_graph_from_gtgraph");
-    medusa::check_mb(mb_graph_device_view(rt.graph, &rt.view), rt.ctx, "mb_graph_device_view");
-    medusa::check(cudaDeviceSynchronize(), "graph build");
+    medusa::graph_ready();
 }
 
-/* MultipleGPU/MultiPublicAPI.h:145-265: message buffers and the flag. */
+namespace medusa {
+/* The application's attributes to the device, and their addresses to the
+ * functors' constant bank. */
+inline void upload_fields() {
+    auto &d = MGLOBAL::gpu_def[0];
+    d.d_vertexArray.Fill(d.vertexArray);
+    d.d_edgeArray.Fill(d.edgeArray);
+    const VertexFieldPtrs vp = d.d_vertexArray.ptrs();
+    const EdgeFieldPtrs ep = d.d_edgeArray.ptrs();
+    check(cudaMemcpyToSymbol(medusa_vfields, &vp, sizeof(vp)), "vertex fields");
+    check(cudaMemcpyToSymbol(medusa_efields, &ep, sizeof(ep)), "edge fields");
+}
+}  // namespace medusa
+
+/* MultipleGPU/MultiPublicAPI.h:145-265: message buffers, the flag, and the
+ * application's attributes (the reference's D_VertexArray::Fill). */
 inline void InitDeviceDS() {
     auto &rt = MGLOBAL::rt;
     int64_t n = 0;
@@ -361,10 +551,20 @@ inline void InitDeviceDS() {
     rt.msg.resize(n);
     rt.combined.resize(rt.view.num_vertices);
     rt.flag.resize(1);
+    rt.fill_pending = false;
+    rt.skip_step = -1;
     MGLOBAL::super_step = 0;
     rt.sync_view();
+    medusa::upload_fields();
+    int v = MGLOBAL::toExecute ? 1 : 0;  // the flag starts as InitConfig's exe
+    medusa::check(cudaMemcpy(rt.flag.p, &v, sizeof(int), cudaMemcpyHostToDevice), "InitDeviceDS");
 }
-inline void ResetGraphData() { MGLOBAL::super_step = 0; }
+/* Back to the state the host arrays hold, for another run. */
+inline void ResetGraphData() {
+    MGLOBAL::super_step = 0;
+    MGLOBAL::rt.skip_step = -1;
+    medusa::upload_fields();
+}
 
 /* MultipleGPU/MultiUtilities.h:48-69 */
 inline void ResetToExecute() {
@@ -377,18 +577,33 @@ inline bool RetriveToExecute() {
     return v != 0;
 }
 
-/* MultipleGPU/MultiPublicAPI.h:344-376: every message slot := init_val. */
+namespace medusa {
+inline bool skipping() { return MGLOBAL::rt.skip_step == MGLOBAL::super_step; }
+inline void Runtime::fill_messages() {
+    if (!fill_pending) return;
+    fill_pending = false;
+    k_fill_msg<<<grid(msg.n), 256>>>(msg.p, msg.n, init_msg);
+    generic_launches++;
+    check(cudaGetLastError(), "InitMessageBuffer");
+}
+}  // namespace medusa
+
+/* MultipleGPU/MultiPublicAPI.h:344-376: every message slot := init_val.  The
+ * fill itself runs when a functor or the combiner first reads the buffer (a
+ * superstep that a built-in path runs whole never needs it). */
 template <class Message>
 inline void InitMessageBuffer(const Message &init_val) {
     auto &rt = MGLOBAL::rt;
+    if (medusa::skipping()) return;
     rt.init_msg = (MVT)init_val.val;
     rt.sync_view();
-    medusa::k_fill_msg<<<rt.grid(rt.msg.n), 256>>>(rt.msg.p, rt.msg.n, rt.init_msg);
-    medusa::check(cudaGetLastError(), "InitMessageBuffer");
+    rt.fill_pending = true;
 }
 
 inline void medusa::Combiner::combineAllDevice() {
     auto &rt = MGLOBAL::rt;
+    if (skipping()) return;
+    rt.fill_messages();
     const int g = rt.grid(rt.view.num_vertices);
     switch (MGLOBAL::combiner_operator) {
         case CUDPP_ADD: k_combine<CUDPP_ADD><<<g, 256>>>(rt.combined.p); break;
@@ -396,8 +611,167 @@ inline void medusa::Combiner::combineAllDevice() {
         case CUDPP_MIN: k_combine<CUDPP_MIN><<<g, 256>>>(rt.combined.p); break;
         default: k_combine<CUDPP_MAX><<<g, 256>>>(rt.combined.p); break;
     }
+    rt.generic_launches++;
     check(cudaGetLastError(), "combineAllDevice");
 }
+
+/* ---- the reference's three apps on the library's kernels ------------------- */
+/* An application declares, after its edge functor, that the functor is the
+ * reference's BFS, SSSP or PageRank send over the named vertex fields:
+ *
+ *   MEDUSA_BUILTIN_BFS(UpdateLevel, level)            Algorithm/UserOperators.h:17-35
+ *   MEDUSA_BUILTIN_SSSP(SendMsg, distance, updated)   SSSP/UserOperators.h:151-189
+ *   MEDUSA_BUILTIN_PAGERANK(SendMsg, level)           MPG/UserOperators.h:16-43
+ *
+ * FunctorHolder<EDGE>::Run(op) then hands the superstep to the library:
+ *   BFS: at superstep 0, with level 0 at the roots and MVT_Init_Value (-1)
+ *     elsewhere, the whole traversal runs in mb_bfs (levels of several roots
+ *     are combined by minimum) and the loop's flag is left clear;
+ *   SSSP: at superstep 0, with updated set exactly on the vertices at
+ *     distance 0 and MEDUSA_MAX elsewhere, the whole traversal runs in
+ *     mb_sssp, every vertex ends not updated, and the flag is left clear;
+ *   PageRank: each superstep is mb_pagerank_from(1 superstep) from the rank
+ *     field into the rank field (send rank/edge_count, sum, 0.15 + 0.85 sum).
+ * The rest of that superstep's Medusa_Exec (InitMessageBuffer, the combiner,
+ * the vertex functor) then does nothing.  When the fields hold anything else
+ * the generic functor kernels run as usual.  MGLOBAL::rt.last_builtin and
+ * builtin_stats say what ran (kernel launches, schedules per superstep). */
+namespace medusa {
+template <class Op>
+struct Builtin {
+    static constexpr BuiltinApp app = BUILTIN_NONE;
+    static int *level() { return nullptr; }
+    static float *dist() { return nullptr; }
+    static bool *updated() { return nullptr; }
+    static float *rank() { return nullptr; }
+};
+
+static __global__ void k_min_levels(const int32_t *lv, int32_t nsrc, int64_t V, int *out) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+        int best = -1;
+        for (int32_t s = 0; s < nsrc; s++) {
+            const int x = lv[s * V + v];
+            if (x >= 0 && (best < 0 || x < best)) best = x;
+        }
+        out[v] = best;
+    }
+}
+static __global__ void k_min_dist(const float *d, int32_t nsrc, int64_t V, float *out) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+        float best = d[v];
+        for (int32_t s = 1; s < nsrc; s++) best = fminf(best, d[s * V + v]);
+        out[v] = best;
+    }
+}
+
+/* Levels (or distances) of several roots, combined by minimum. */
+inline bool builtin_bfs(int *level) {
+    auto &rt = MGLOBAL::rt;
+    const int64_t V = rt.view.num_vertices;
+    if (MGLOBAL::super_step != 0 || !level) return false;
+    std::vector<int> h((size_t)V);
+    if (V) check(cudaMemcpy(h.data(), level, sizeof(int) * (size_t)V, cudaMemcpyDeviceToHost), "BFS roots");
+    std::vector<int32_t> roots;
+    for (int64_t v = 0; v < V; v++) {
+        if (h[v] == 0) roots.push_back((int32_t)v);
+        else if (h[v] != -1) return false;
+    }
+    if (roots.empty()) return false;
+    if (roots.size() == 1) {
+        check_mb(mb_bfs(rt.ctx, rt.graph, roots.data(), 1, level, &rt.builtin_stats), rt.ctx, "mb_bfs");
+    } else {
+        DeviceArray<int32_t> all((int64_t)roots.size() * V);
+        check_mb(mb_bfs(rt.ctx, rt.graph, roots.data(), (int32_t)roots.size(), all.p, &rt.builtin_stats),
+                 rt.ctx, "mb_bfs");
+        k_min_levels<<<rt.grid(V), 256>>>(all.p, (int32_t)roots.size(), V, level);
+        check(cudaDeviceSynchronize(), "BFS roots combined");
+    }
+    return true;
+}
+
+inline bool builtin_sssp(float *dist, bool *updated) {
+    auto &rt = MGLOBAL::rt;
+    const int64_t V = rt.view.num_vertices;
+    if (MGLOBAL::super_step != 0 || !dist || !updated) return false;
+    std::vector<float> hd((size_t)V);
+    std::unique_ptr<bool[]> hu(new bool[(size_t)(V > 0 ? V : 1)]);
+    if (V) {
+        check(cudaMemcpy(hd.data(), dist, sizeof(float) * (size_t)V, cudaMemcpyDeviceToHost), "SSSP state");
+        check(cudaMemcpy(hu.get(), updated, sizeof(bool) * (size_t)V, cudaMemcpyDeviceToHost), "SSSP state");
+    }
+    std::vector<int32_t> roots;
+    for (int64_t v = 0; v < V; v++) {
+        if (hu[v] && hd[v] == 0.0f) roots.push_back((int32_t)v);
+        else if (hu[v] || hd[v] != (float)MEDUSA_MAX) return false;
+    }
+    if (roots.empty()) return false;
+    if (roots.size() == 1) {
+        check_mb(mb_sssp(rt.ctx, rt.graph, roots.data(), 1, dist, &rt.builtin_stats), rt.ctx, "mb_sssp");
+    } else {
+        DeviceArray<float> all((int64_t)roots.size() * V);
+        check_mb(mb_sssp(rt.ctx, rt.graph, roots.data(), (int32_t)roots.size(), all.p, &rt.builtin_stats),
+                 rt.ctx, "mb_sssp");
+        k_min_dist<<<rt.grid(V), 256>>>(all.p, (int32_t)roots.size(), V, dist);
+    }
+    check(cudaMemset(updated, 0, sizeof(bool) * (size_t)V), "SSSP updated");
+    check(cudaDeviceSynchronize(), "SSSP");
+    return true;
+}
+
+inline bool builtin_pagerank(float *rank) {
+    auto &rt = MGLOBAL::rt;
+    if (!rank || MGLOBAL::combiner_operator != CUDPP_ADD) return false;
+    check_mb(mb_pagerank_from(rt.ctx, rt.graph, 1, rank, rank, &rt.builtin_stats), rt.ctx, "mb_pagerank_from");
+    return true;
+}
+
+template <class Op>
+inline bool run_builtin() {
+    auto &rt = MGLOBAL::rt;
+    using B = Builtin<Op>;
+    bool ran = false;
+    if (B::app == BUILTIN_BFS) ran = builtin_bfs(B::level());
+    else if (B::app == BUILTIN_SSSP) ran = builtin_sssp(B::dist(), B::updated());
+    else if (B::app == BUILTIN_PAGERANK) ran = builtin_pagerank(B::rank());
+    if (!ran) return false;
+    if (B::app != BUILTIN_PAGERANK) {  // the traversal is complete: no further superstep
+        const int zero = 0;
+        check(cudaMemcpy(rt.flag.p, &zero, sizeof(int), cudaMemcpyHostToDevice), "flag");
+    }
+    rt.fill_pending = false;
+    rt.skip_step = MGLOBAL::super_step;
+    rt.last_builtin = B::app;
+    return true;
+}
+}  // namespace medusa
+
+#define MEDUSA_BUILTIN_BFS(Functor, level_field)                                                   \
+    template <>                                                                                     \
+    struct medusa::Builtin<Functor> {                                                               \
+        static constexpr medusa::BuiltinApp app = medusa::BUILTIN_BFS;                              \
+        static int *level() { return (int *)MGLOBAL::gpu_def[0].d_vertexArray.level_field.p; }      \
+        static float *dist() { return nullptr; }                                                    \
+        static bool *updated() { return nullptr; }                                                  \
+        static float *rank() { return nullptr; }                                                    \
+    };
+#define MEDUSA_BUILTIN_SSSP(Functor, dist_field, updated_field)                                    \
+    template <>                                                                                     \
+    struct medusa::Builtin<Functor> {                                                               \
+        static constexpr medusa::BuiltinApp app = medusa::BUILTIN_SSSP;                             \
+        static int *level() { return nullptr; }                                                     \
+        static float *dist() { return (float *)MGLOBAL::gpu_def[0].d_vertexArray.dist_field.p; }    \
+        static bool *updated() { return (bool *)MGLOBAL::gpu_def[0].d_vertexArray.updated_field.p; } \
+        static float *rank() { return nullptr; }                                                    \
+    };
+#define MEDUSA_BUILTIN_PAGERANK(Functor, rank_field)                                               \
+    template <>                                                                                     \
+    struct medusa::Builtin<Functor> {                                                               \
+        static constexpr medusa::BuiltinApp app = medusa::BUILTIN_PAGERANK;                         \
+        static int *level() { return nullptr; }                                                     \
+        static float *dist() { return nullptr; }                                                    \
+        static bool *updated() { return nullptr; }                                                  \
+        static float *rank() { return (float *)MGLOBAL::gpu_def[0].d_vertexArray.rank_field.p; }    \
+    };
 
 /* MultipleGPU/MultiAPIHoster.h:653-735 */
 template <FunctorType T>
@@ -407,7 +781,9 @@ struct FunctorHolder<VERTEX> {
     template <class Op>
     static void Run(Op op) {
         auto &rt = MGLOBAL::rt;
+        if (medusa::skipping()) return;
         medusa::k_vertex<<<rt.grid(rt.view.num_vertices), 256>>>(op, MGLOBAL::super_step);
+        rt.generic_launches++;
         medusa::check(cudaGetLastError(), "FunctorHolder<VERTEX>");
     }
 };
@@ -416,8 +792,28 @@ struct FunctorHolder<EDGE> {
     template <class Op>
     static void Run(Op op) {
         auto &rt = MGLOBAL::rt;
+        if (medusa::skipping()) return;
+        if (medusa::Builtin<Op>::app != medusa::BUILTIN_NONE && rt.builtin_enabled && medusa::run_builtin<Op>())
+            return;
+        rt.fill_messages();
         medusa::k_edge<<<rt.grid(rt.view.num_edges), 256>>>(op, MGLOBAL::super_step);
+        rt.generic_launches++;
         medusa::check(cudaGetLastError(), "FunctorHolder<EDGE>");
+    }
+};
+/* The edge functor on a fixed small grid, one CTA per SM, each thread
+ * walking many edges (the reference's hash-table variant, 60 x 256 threads,
+ * MultipleGPU/MultiAPIHoster.h:682-703, MedusaRT/APIKernelWrappers.h:185-193). */
+template <>
+struct FunctorHolder<EDGE_HT> {
+    template <class Op>
+    static void Run(Op op) {
+        auto &rt = MGLOBAL::rt;
+        if (medusa::skipping()) return;
+        rt.fill_messages();
+        medusa::k_edge<<<rt.num_sms, 256>>>(op, MGLOBAL::super_step);
+        rt.generic_launches++;
+        medusa::check(cudaGetLastError(), "FunctorHolder<EDGE_HT>");
     }
 };
 template <>
@@ -425,7 +821,10 @@ struct FunctorHolder<EDGELIST> {
     template <class Op>
     static void Run(Op op) {
         auto &rt = MGLOBAL::rt;
+        if (medusa::skipping()) return;
+        rt.fill_messages();
         medusa::k_edgelist<<<rt.grid(rt.view.num_vertices), 256>>>(op, MGLOBAL::super_step);
+        rt.generic_launches++;
         medusa::check(cudaGetLastError(), "FunctorHolder<EDGELIST>");
     }
 };
@@ -434,7 +833,10 @@ struct FunctorHolder<MESSAGE> {
     template <class Op>
     static void Run(Op op) {
         auto &rt = MGLOBAL::rt;
+        if (medusa::skipping()) return;
+        rt.fill_messages();
         medusa::k_message<<<rt.grid(rt.msg.n), 256>>>(op, MGLOBAL::super_step, rt.msg.n);
+        rt.generic_launches++;
         medusa::check(cudaGetLastError(), "FunctorHolder<MESSAGE>");
     }
 };
@@ -445,6 +847,8 @@ inline void MedusaShutdown() {
     rt.msg.release();
     rt.combined.release();
     rt.flag.release();
+    MGLOBAL::gpu_def[0].d_vertexArray = medusa::D_VertexArray{};
+    MGLOBAL::gpu_def[0].d_edgeArray = medusa::D_EdgeArray{};
     if (rt.graph) mb_graph_destroy(rt.graph);
     rt.graph = nullptr;
     if (rt.ctx) mb_destroy(rt.ctx);

@@ -193,15 +193,30 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *g, const int32_t *sources, int32_t nsrc
  * (MPG/main.cu:148-169, MPG/UserOperators.h:16-43,119-144,175-270). */
 int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
                 float *rank_out, mb_stats *stats);
-/* PageRank summation order.  MB_PR_ORDER_FIXED (default): a fixed order
- * the same for every schedule -- a sequential fold in message-slot order up
- * to 64 in-edges (the reference's CPU fold over the AA layout), 4096-edge
- * warp blocks above; within 1e-5 of the reference on graphs without hubs.
- * MB_PR_ORDER_REFERENCE: the reference's own MEG layout (vertices sorted by
- * out-degree with std::sort, column-major edge slots, MedusaRT/GraphConverter.cu
- * :136-165, MPG/EdgeDataType.cu:45-131) folded sequentially -- the reference's
- * FP32 result bit for bit, at the cost of serial folds on hubs; the ordering
- * is built on first use per graph (a host sort of V out-degrees). */
+/* The same from an initial rank per vertex, init_ranks[V] (host or device):
+ * the first superstep sends init_ranks[u] / outdeg[u].  This is what one
+ * superstep of the reference's PageRank loop does to the rank attribute it
+ * holds (MPG/UserOperators.h:16-43, SendMsg + combiner + UpdateVertex), so a
+ * loop of single supersteps gives the same bits as one call of many. */
+int mb_pagerank_from(mb_ctx *ctx, const mb_graph *g, int32_t iters, const float *init_ranks,
+                     float *rank_out, mb_stats *stats);
+/* PageRank summation order.
+ * MB_PR_ORDER_REFERENCE (default): the reference's own MEG layout (vertices
+ * sorted by out-degree with std::sort, column-major edge slots,
+ * MedusaRT/GraphConverter.cu:136-165, MPG/EdgeDataType.cu:45-131), every
+ * vertex's messages folded sequentially in float as the reference's combiner
+ * does -- the reference's FP32 result bit for bit.  The fused schedule computes
+ * those sequential sums in parallel (an exact integer scan within each binade
+ * of the running sum, float adds only where the sum changes binade or meets a
+ * rounding tie); the message-reading schedule folds each vertex serially.  The
+ * ordering is built on first use per graph (a host sort of V out-degrees).
+ * MB_PR_ORDER_FIXED: a fixed parallel order, the same for every schedule -- a
+ * sequential fold in AA message-slot order up to 64 in-edges, 4096-edge warp
+ * blocks above.  Faster on graphs with large hubs; more accurate than the
+ * reference's sequential float sums there, and therefore up to ~2e-4 away
+ * from the reference's ranks on a vertex with 3.7e5 in-edges (within 1e-5
+ * only on graphs without large hubs).  mb_batch_run and mb_pagerank_noalloc
+ * use this order. */
 #define MB_PR_ORDER_FIXED 0
 #define MB_PR_ORDER_REFERENCE 1
 int mb_set_pagerank_order(mb_ctx *ctx, int32_t order);
@@ -309,7 +324,19 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                  TMA engine, 0 by the threads' loads (default 0) */
 #define MB_TUNE_BFS_GAMMA 11 /* BFS fixed rule: bottom-up only while the frontier has
                                 at least E / gamma out-edges (default 16; 0: no floor) */
-#define MB_NUM_TUNABLES 12
+#define MB_TUNE_PR_HUB_MIN 12 /* PageRank in the reference's order: in-degree above
+                                which one CTA sums a vertex by the parallel
+                                integer scan (default 2048; at least 64) */
+#define MB_TUNE_WAIT_POLLS 13 /* polls before a bounded device wait gives up -- the grid
+                                barrier of the persistent kernels, the team barrier of the
+                                many-graph kernel, the bulk-copy wait of the staged push
+                                (defaults 2^22, 2^24, 2^22); the run then fails with
+                                MB_ERR_TIMEOUT.  0 gives up at once: a way to drive the
+                                error path.  A bulk copy whose wait gave up is still
+                                waited for with the full budget before the CTA moves on */
+#define MB_TUNE_STEP_CAP 14 /* superstep cap of the BFS / SSSP loops (default V+4 for BFS,
+                              4V+16 for SSSP, V+8 batched BFS); past it MB_ERR_TIMEOUT */
+#define MB_NUM_TUNABLES 15
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 
@@ -375,10 +402,18 @@ int mb_scheduler_pick(mb_ctx *ctx, int32_t model, const float *features,
  * destination (the reverse CSR), rank_out[V].  Same arithmetic and bits as
  * mb_pagerank.  Scratch is one fixed device array in the library (8 MiB per
  * GPU, held until exit), so num_vertices <= 1048576 (larger: MB_ERR_UNSUPPORTED).
- * The first call on a device looks up that array's address; make it before
- * any stream capture.  Runs asynchronously on `stream` (a cudaStream_t; NULL
- * = the default stream).  All calls on a device share the scratch: calls that
- * overlap on the GPU race.  Errors: mb_last_error(NULL). */
+ * The arrays must belong to the current device (managed memory is also
+ * accepted); another GPU's memory is MB_ERR_INVALID.  The scratch belongs to
+ * the context current at the call: every call looks its address up there
+ * (no allocation), and the first call in a context also loads the library's
+ * device code, so make that first call before any stream capture.  Runs
+ * asynchronously on `stream` (a cudaStream_t; NULL = the default stream).
+ * All calls on a device share the scratch: calls that overlap on the GPU
+ * race.  One warp sums each vertex with more than 64 in-edges, block after
+ * block, so a vertex with millions of in-edges makes each superstep as long
+ * as that warp's sum (mb_pagerank spreads such a vertex over many warps).
+ * A CUDA error left pending by the caller's earlier calls on this thread is
+ * cleared on entry; the call reports its own.  Errors: mb_last_error(NULL). */
 int mb_pagerank_noalloc(const int32_t *row, const int32_t *rrow, const int32_t *rcol,
                         int32_t num_vertices, int64_t num_edges, int32_t iters, float init,
                         float *rank_out, void *stream);

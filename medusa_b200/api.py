@@ -25,11 +25,13 @@ MB_PR_ORDER_FIXED, MB_PR_ORDER_REFERENCE = 0, 1
 MB_TUNE_SSSP_BM_PUSH_MIN, MB_TUNE_PUSH_BLOCKS_PER_SM, MB_TUNE_VERTEX_BLOCKS_PER_SM, \
     MB_TUNE_TAIL_EDGES, MB_TUNE_BATCH_THREADS, MB_TUNE_BATCH_EDGES_PER_CTA, \
     MB_TUNE_PR_LIGHT_VPL, MB_TUNE_PR_SHORT_PAIR, MB_TUNE_BFS_ALPHA, MB_TUNE_BFS_BETA, \
-    MB_TUNE_BULK_STAGE, MB_TUNE_BFS_GAMMA = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11
+    MB_TUNE_BULK_STAGE, MB_TUNE_BFS_GAMMA, MB_TUNE_PR_HUB_MIN, MB_TUNE_WAIT_POLLS, \
+    MB_TUNE_STEP_CAP = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14
 TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_sm": 2,
             "tail_edges": 3, "batch_threads": 4, "batch_edges_per_cta": 5,
             "pr_light_vpl": 6, "pr_short_pair": 7, "bfs_alpha": 8, "bfs_beta": 9,
-            "bulk_stage": 10, "bfs_gamma": 11}
+            "bulk_stage": 10, "bfs_gamma": 11, "pr_hub_min": 12, "wait_polls": 13,
+            "step_cap": 14}
 NUM_SCHEDULES = 8
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
@@ -99,6 +101,7 @@ def _load():
         "mb_sssp": (ctypes.c_int, [P, P, P, I32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank_noalloc": (ctypes.c_int, [P, P, P, I32, I64, I32, F32, P, P]),
+        "mb_pagerank_from": (ctypes.c_int, [P, P, I32, P, P, ctypes.POINTER(Stats)]),
         "mb_scheduler_collect": (ctypes.c_int, [P, P, I32, I32, P, P, P, I32, ctypes.POINTER(I32)]),
         "mb_scheduler_train": (ctypes.c_int, [P, I32, P, P, I32, I32, F32, ctypes.c_uint64,
                                               ctypes.POINTER(F32)]),
@@ -283,6 +286,21 @@ class Graph:
         return out, st.as_dict()
 
 
+def _pagerank_from(self, iters, init_ranks, out=None):
+    """`iters` supersteps from a rank per vertex (mb_pagerank_from)."""
+    if not hasattr(init_ranks, "data_ptr"):
+        init_ranks = np.ascontiguousarray(init_ranks, np.float32)
+    if out is None:
+        out = np.empty(self.V, np.float32)
+    st = Stats()
+    _check(lib.mb_pagerank_from(self.ctx.h, self.h, int(iters), _ptr(init_ranks), _ptr(out),
+                                ctypes.byref(st)), self.ctx.h)
+    return out, st.as_dict()
+
+
+Graph.pagerank_from = _pagerank_from
+
+
 class Batch:
     """Many independent graphs run together (mb_batch_*)."""
 
@@ -351,6 +369,7 @@ class Context:
         self.h = h
         self.policy = (MB_POLICY_FIXED, 0)
         self.sssp_delta = 0.0
+        self.pr_order = MB_PR_ORDER_REFERENCE
 
     def close(self):
         if self.h:
@@ -477,9 +496,10 @@ class Context:
         return out[:n.value].copy()
 
     def set_pagerank_order(self, order):
-        """MB_PR_ORDER_FIXED (fast, fixed order) or MB_PR_ORDER_REFERENCE (the
-        reference's MEG order, its FP32 result bit for bit)."""
+        """MB_PR_ORDER_REFERENCE (default: the reference's MEG order, its FP32
+        result bit for bit) or MB_PR_ORDER_FIXED (a fixed parallel order)."""
         _check(lib.mb_set_pagerank_order(self.h, int(order)), self.h)
+        self.pr_order = int(order)
 
     def set_batching(self, enable):
         _check(lib.mb_set_batching(self.h, 1 if enable else 0), self.h)

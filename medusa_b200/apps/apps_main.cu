@@ -1,6 +1,6 @@
 // apps_main.cu -- command-line driver of the operator-API apps:
 //
-//   medusa_apps bfs|sssp|pr <gtgraph file> <source | supersteps> <output file>
+//   medusa_apps bfs|sssp|pr|prmsg <gtgraph file> <source | supersteps> <output file>
 //
 // Reads the graph with InitHostDSFromGTGraph (GPU GTgraph parser), runs the
 // app through the generic functor kernels of include/medusa/medusa.h and
@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include "bfs_ops.cuh"
+#include "msg_ops.cuh"
 #include "pagerank_ops.cuh"
 #include "sssp_ops.cuh"
 
@@ -21,7 +22,7 @@ static void write_out(const char *path, const std::vector<T> &v) {
 
 int main(int argc, char **argv) {
     if (argc != 5) {
-        std::fprintf(stderr, "usage: medusa_apps bfs|sssp|pr <gtgraph file> <source|supersteps> <out>\n");
+        std::fprintf(stderr, "usage: medusa_apps bfs|sssp|pr|prmsg <gtgraph file> <source|supersteps> <out>\n");
         return 2;
     }
     try {
@@ -32,6 +33,7 @@ int main(int argc, char **argv) {
         if (app == "bfs") write_out(argv[4], bfs_app::run(arg));
         else if (app == "sssp") write_out(argv[4], sssp_app::run(arg));
         else if (app == "pr") write_out(argv[4], pagerank_app::run(arg));
+        else if (app == "prmsg") write_out(argv[4], msg_app::run(arg));
         else throw std::runtime_error("unknown app " + app);
         std::printf("%s done: %d supersteps\n", app.c_str(), MGLOBAL::super_step);
         MedusaShutdown();

@@ -97,10 +97,17 @@ def tune_traversals(ctx, g, source=0, reps=3):
 
 
 def tune_pagerank(ctx, g, iters=10, reps=3, out=None):
-    """Light vertices per lane of the fused pull and short heavy blocks per
-    warp, timing `iters` PageRank supersteps on g (out: a rank buffer to
-    reuse, e.g. a device tensor)."""
-    space = {"pr_light_vpl": [-1, 1, 2, 4], "pr_short_pair": [-1, 1, 2]}
+    """Light vertices per lane of the fused pull, and, in the reference's
+    order, the in-degree above which a vertex is summed by one CTA's integer
+    scan (else short heavy blocks per warp of the fixed order), timing
+    `iters` PageRank supersteps on g (out: a rank buffer to reuse, e.g. a
+    device tensor)."""
+    from medusa_b200 import api
+    space = {"pr_light_vpl": [-1, 1, 2, 4]}
+    if getattr(ctx, "pr_order", api.MB_PR_ORDER_REFERENCE) == api.MB_PR_ORDER_REFERENCE:
+        space["pr_hub_min"] = [-1, 256, 512, 1024, 4096]
+    else:
+        space["pr_short_pair"] = [-1, 1, 2]
     return tune(ctx, lambda: g.pagerank(iters, 1.0 / g.V, out=out)[1], space, reps)
 
 

@@ -104,7 +104,40 @@ def build_apps(force=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("apps build failed:\n%s" % r.stderr[-6000:])
+    build_dropin(force)
     return APPS_BIN
+
+
+DROPIN_DIR = os.path.join(APPS_DIR, "dropin")
+DROPIN_APPS = ("bfs", "sssp", "pagerank")
+
+
+def dropin_bin(app):
+    return os.path.join(DROPIN_DIR, "medusa_dropin_" + app)
+
+
+def build_dropin(force=False):
+    """The reference's apps in their own shape (medusa_b200/apps/dropin), one
+    binary each (each app generates its own vertex field list)."""
+    common = glob.glob(os.path.join(DROPIN_DIR, "*.h")) + [LIB] + \
+        glob.glob(os.path.join(ROOT, "include", "medusa", "*.h"))
+    jobs = []
+    for app in DROPIN_APPS:
+        src = os.path.join(DROPIN_DIR, "dropin_%s.cu" % app)
+        if force or _stale(dropin_bin(app), [src] + common):
+            jobs.append([NVCC, "-std=c++17", "-O3", "-lineinfo"] + ARCH +
+                        ["-I", os.path.join(ROOT, "include"), "-I", DROPIN_DIR, src,
+                         "-o", dropin_bin(app), "-L", HERE, "-lmedusa_b200",
+                         "-Xlinker", "-rpath,$ORIGIN/../.."])
+
+    def run(cmd):
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("drop-in app build failed:\n%s" % r.stderr[-6000:])
+
+    if jobs:
+        with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+            list(ex.map(run, jobs))
 
 
 def main(argv=None):

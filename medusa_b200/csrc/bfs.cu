@@ -564,7 +564,7 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
     sp.st = &st;
     sp.fa = a.f;
     sp.app = APP_BFS;
-    sp.cap = g.V + 4;
+    sp.cap = step_cap(ctx, (int64_t)g.V + 4);
     sp.name = "bfs";
     sp.prologue = [&](cudaStream_t s) {
         MB_CUDA(cudaMemsetAsync(a.level, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));

@@ -55,10 +55,10 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
-// Wait for the phase of parity `parity` to complete; false after kBulkSpins
-// polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kBulkSpins; i++) {
+// Wait for the phase of parity `parity` to complete; false after `polls`
+// polls (kBulkSpins by default).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t polls = kBulkSpins) {
+    for (uint32_t i = 0; i < polls; i++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

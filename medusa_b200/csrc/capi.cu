@@ -299,6 +299,8 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "BFS beta must be >= 1");
     if (which == MB_TUNE_BULK_STAGE && value > 1)
         return set_error(ctx, MB_ERR_INVALID, "bulk staging is 0 or 1");
+    if (which == MB_TUNE_PR_HUB_MIN && value != -1 && (value < 64 || value > 0x7fffffff))
+        return set_error(ctx, MB_ERR_INVALID, "PageRank hub threshold must be >= 64");
     ctx->c.tunable[which] = value;
     ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
     return MB_OK;
@@ -766,6 +768,31 @@ int mb_pagerank(mb_ctx *ctx, const mb_graph *gc, int32_t iters, float init, floa
         mb::run_pagerank(ctx->c, g->g, apps(g).pr, iters, init, sched, stats);
         MB_CUDA(cudaMemcpyAsync(rank_out, apps(g).pr.rank.p, sizeof(float) * (size_t)g->g.V,
                                 cudaMemcpyDefault, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int mb_pagerank_from(mb_ctx *ctx, const mb_graph *gc, int32_t iters, const float *init_ranks,
+                     float *rank_out, mb_stats *stats) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (iters < 0 || !rank_out || !init_ranks) mb::fail(MB_ERR_INVALID, "bad iters/input/output");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        const int sched = ctx->c.schedule_policy == MB_POLICY_FORCED ? ctx->c.fixed_schedule
+                                                                      : MB_SCHED_PUSH_EDGE_QUEUE;
+        // host ranks are staged into the PageRank state's own buffer, so a
+        // captured run keeps reading the same address
+        mb::PrState &pr = apps(g).pr;
+        const size_t bytes = sizeof(float) * (size_t)g->g.V;
+        const float *init_dev = init_ranks;
+        if (!mb::is_device_ptr(init_ranks)) {
+            pr.init_stage.reserve(std::max<size_t>(bytes, 1));
+            mb::copy_sync(ctx->c.stream, pr.init_stage.p, init_ranks, bytes);
+            init_dev = pr.init_stage.as<float>();
+        }
+        mb::run_pagerank(ctx->c, g->g, pr, iters, 0.f, sched, stats, init_dev);
+        MB_CUDA(cudaMemcpyAsync(rank_out, pr.rank.p, bytes, cudaMemcpyDefault, ctx->c.stream));
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
     });
 }

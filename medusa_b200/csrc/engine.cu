@@ -25,6 +25,7 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->tail_edges = ctx.tunable[MB_TUNE_TAIL_EDGES] >= 0
                         ? (uint32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_TAIL_EDGES], kTailEdges)
                         : kTailEdges;
+    p->wait_polls = ctx.tunable[MB_TUNE_WAIT_POLLS] >= 0 ? ctx.tunable[MB_TUNE_WAIT_POLLS] : -1;
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));

@@ -390,13 +390,15 @@ __device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
     }
 }
 
-// Count one loop iteration; past the cap the run stops with an error.
+// Count one loop iteration; past the cap the run stops with an error, and
+// so does a run in which a bounded wait gave up.
 __device__ inline void count_iteration(Ctrl *c, int cap) {
     c->iter++;
     if (c->iter > cap && !c->done) {
         c->err |= ERR_STEP_CAP;
         c->done = 1;
     }
+    if (c->err & (ERR_BARRIER | ERR_BULK)) c->done = 1;
 }
 
 // Top of every loop iteration (one warp): bookkeeping of the superstep that
@@ -439,8 +441,9 @@ static __global__ void k_select(FrontierArgs a, int app, int cap,
 }
 
 // Grid barrier of the persistent kernel (all blocks co-resident: cooperative
-// launch).  The wait is bounded: past kBarrierSpins polls it records
-// ERR_BARRIER and returns false, and the caller leaves its loop.
+// launch).  The wait is bounded: past kBarrierSpins polls (or the run's
+// wait_polls, when set) it records ERR_BARRIER and returns false, and the
+// caller leaves its loop.
 constexpr long kBarrierSpins = 1l << 22;
 __device__ inline bool grid_sync(Ctrl *c) {
     __shared__ int s_ok;
@@ -456,7 +459,8 @@ __device__ inline bool grid_sync(Ctrl *c) {
             atomicAdd(&c->bar_gen, 1u);
         } else {
             ok = 0;
-            for (long it = 0; it < kBarrierSpins; it++) {
+            const long spins = c->p.wait_polls >= 0 ? (long)c->p.wait_polls : kBarrierSpins;
+            for (long it = 0; it < spins; it++) {
                 if (ldg2(&c->bar_gen) != gen) {
                     ok = 1;
                     break;

@@ -134,9 +134,9 @@ struct Context {
     bool batching = true;          // several BFS sources: one masked traversal per 64
     bool replay_then_fixed = false;  // replay policy: fixed rule after the list
     int32_t max_step = -1;           // >= 0: runs stop after this superstep
-    int pr_order = MB_PR_ORDER_FIXED;  // PageRank summation order
+    int pr_order = MB_PR_ORDER_REFERENCE;  // PageRank summation order
     // launch and routing parameters (MB_TUNE_*); -1: the built-in default
-    int64_t tunable[MB_NUM_TUNABLES] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    int64_t tunable[MB_NUM_TUNABLES] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
     uint64_t tune_gen = 0;  // bumped on every change (loop graphs are rebuilt)
     int blocks_per_sm(int which, int dflt) const {
         return tunable[which] > 0 ? (int)tunable[which] : dflt;
@@ -161,6 +161,13 @@ struct Context {
         return pinned;
     }
 };
+
+// Superstep cap of a loop: the MB_TUNE_STEP_CAP tunable when set, else the
+// loop's own bound; past it a run stops with MB_ERR_TIMEOUT.
+inline int step_cap(const Context &ctx, int64_t dflt) {
+    const int64_t t = ctx.tunable[MB_TUNE_STEP_CAP];
+    return (int)std::min<int64_t>(t >= 0 ? t : dflt, 1 << 30);
+}
 
 // Blocking copy ordered with the library's stream.  The stream is
 // non-blocking, so a plain cudaMemcpy (legacy default stream) is not ordered

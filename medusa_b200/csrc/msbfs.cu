@@ -519,7 +519,7 @@ void run_msbfs(Context &ctx, Graph &g, MsBfsState &st, const int32_t *sources, i
     const size_t vb = (size_t)g.V;
     const int gv = ctx.num_sms * 8, gp = ctx.num_sms * 8;
     // every superstep reaches at least one new (vertex, source) pair
-    const int cap = (int)std::min<int64_t>((int64_t)g.V + 8, 1 << 30);
+    const int cap = step_cap(ctx, (int64_t)g.V + 8);
 
     auto prologue = [&](cudaStream_t cs) {
         MB_CUDA(cudaMemsetAsync(a.seen, 0, 8 * vb, cs));

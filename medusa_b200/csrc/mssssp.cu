@@ -304,7 +304,7 @@ void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources,
         MB_CHECK_LAUNCH();
         // every superstep lowers some distance; integer distances below 2^24
         // bound the count well below this cap
-        const int64_t cap = (int64_t)g.V * 4 + 16;
+        const int64_t cap = step_cap(ctx, (int64_t)g.V * 4 + 16);
         for (int64_t it = 0;; it++) {
             MB_CUDA(cudaMemcpyAsync(hc, a.c, sizeof(MsCtrl), cudaMemcpyDeviceToHost, s));
             MB_CUDA(cudaStreamSynchronize(s));

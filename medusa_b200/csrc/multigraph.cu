@@ -30,7 +30,7 @@ void graph_generate(Context &ctx, Graph &g, const mb_gen_params &p, uint32_t fla
 
 namespace {
 
-constexpr long kTeamSpins = 1l << 24;  // polls (64 ns apart) before a barrier gives up
+constexpr long kTeamSpins = 1l << 24;  // polls (64 ns apart) before a barrier gives up (default)
 
 struct MultiArgs {
     const GDesc *desc;
@@ -43,11 +43,12 @@ struct MultiArgs {
     float *rank;          // outputs, batch-wide
     int32_t *level;
     unsigned *work;       // [0] next entry, [1] error flag, [2] launches
+    long wait_polls;      // polls before a team barrier gives up
 };
 
 // Team barrier (all threads of the CTA call it).  False if it gave up or
 // another CTA reported an error.
-__device__ bool team_sync(TeamState *ts, int t, unsigned *err) {
+__device__ bool team_sync(TeamState *ts, int t, unsigned *err, long polls) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -62,7 +63,7 @@ __device__ bool team_sync(TeamState *ts, int t, unsigned *err) {
                 atomicAdd(&ts->bar_gen, 1u);
             } else {
                 ok = 0;
-                for (long it = 0; it < kTeamSpins; it++) {
+                for (long it = 0; it < polls; it++) {
                     if (__ldcg(&ts->bar_gen) != gen) {
                         ok = 1;
                         break;
@@ -106,7 +107,7 @@ __device__ bool pr_phase(const MultiArgs &a, const GDesc &d, TeamState *ts, cons
         c0[v] = deg > 0 ? init / (float)deg : 0.0f;
         if (a.pr_iters == 0) rank[v] = init;
     }
-    if (!team_sync(ts, m.t, &a.work[1])) return false;
+    if (!team_sync(ts, m.t, &a.work[1], a.wait_polls)) return false;
     const int lane = threadIdx.x & 31;
     const int64_t ngroups = ((int64_t)d.V + 31) / 32;
     for (int it = 0; it < a.pr_iters; it++) {
@@ -144,7 +145,7 @@ __device__ bool pr_phase(const MultiArgs &a, const GDesc &d, TeamState *ts, cons
                 cout[v] = deg > 0 ? r / (float)deg : 0.0f;
             }
         }
-        if (!team_sync(ts, m.t, &a.work[1])) return false;
+        if (!team_sync(ts, m.t, &a.work[1], a.wait_polls)) return false;
     }
     return true;
 }
@@ -153,13 +154,13 @@ __device__ bool bfs_phase(const MultiArgs &a, const GDesc &d, TeamState *ts, con
     int32_t *lv = a.level + d.vbase;
     int32_t *q[2] = {a.queue[0] + d.vbase, a.queue[1] + d.vbase};
     for (int64_t v = m.tid; v < d.V; v += m.nthr) lv[v] = -1;
-    if (!team_sync(ts, m.t, &a.work[1])) return false;
+    if (!team_sync(ts, m.t, &a.work[1], a.wait_polls)) return false;
     if (m.k == 0 && threadIdx.x == 0) {
         lv[d.source] = 0;
         q[0][0] = d.source;
         ts->qn[0] = 1;
     }
-    if (!team_sync(ts, m.t, &a.work[1])) return false;
+    if (!team_sync(ts, m.t, &a.work[1], a.wait_polls)) return false;
     const int lane = threadIdx.x & 31;
     for (int32_t L = 0;; L++) {
         const int cur = L % 3, nxt = (L + 1) % 3, clr = (L + 2) % 3;
@@ -215,7 +216,7 @@ __device__ bool bfs_phase(const MultiArgs &a, const GDesc &d, TeamState *ts, con
                 for (int32_t r = 0; r < maxd; r++) visit(r < sd, r < sd ? __ldg(&d.col[st + r]) : 0);
             }
         }
-        if (!team_sync(ts, m.t, &a.work[1])) return false;
+        if (!team_sync(ts, m.t, &a.work[1], a.wait_polls)) return false;
     }
     // reached vertices and their out-edges (the traversal count)
     unsigned long long nr = 0, er = 0;
@@ -341,6 +342,7 @@ void batch_run(Context &ctx, Batch &b, int32_t pr_iters, const int32_t *sources,
     a.rank = ranks_dev;
     a.level = levels_dev;
     a.work = b.work.as<unsigned>();
+    a.wait_polls = ctx.tunable[MB_TUNE_WAIT_POLLS] >= 0 ? (long)ctx.tunable[MB_TUNE_WAIT_POLLS] : kTeamSpins;
     cudaEvent_t e0, e1;
     MB_CUDA(cudaEventCreate(&e0));
     MB_CUDA(cudaEventCreate(&e1));

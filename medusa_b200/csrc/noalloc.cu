@@ -123,16 +123,19 @@ __global__ void __launch_bounds__(kNaWarps * 32) k_na_pull(NaArgs a) {
 }
 
 std::mutex g_mu;
-float *g_scratch_addr[kMaxDevices];
 int g_num_sms[kMaxDevices];
 
-bool is_device_memory(const void *p) {
+// Device memory of device `dev` (or managed memory, which every device
+// reaches).  Device memory of another GPU is refused: without peer access
+// the kernels would fault on it.
+bool is_device_memory(const void *p, int dev) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
 int na_fail(int code, const std::string &msg) {
@@ -155,37 +158,45 @@ extern "C" int mb_pagerank_noalloc(const int32_t *row, const int32_t *rrow, cons
     if (iters < 0) return na_fail(MB_ERR_INVALID, "iters must be >= 0");
     if (!row || !rrow || !rank_out || (num_edges > 0 && !rcol))
         return na_fail(MB_ERR_INVALID, "null array");
-    if (!is_device_memory(row) || !is_device_memory(rrow) || !is_device_memory(rank_out) ||
-        (num_edges > 0 && !is_device_memory(rcol)))
-        return na_fail(MB_ERR_INVALID, "every array must be device memory");
+    // an error left pending by the caller's earlier CUDA calls on this thread
+    // is cleared here, so that the check after the launches reports only
+    // this call's own errors
+    cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
         return na_fail(MB_ERR_CUDA, "no current CUDA device");
     }
+    if (!is_device_memory(row, dev) || !is_device_memory(rrow, dev) ||
+        !is_device_memory(rank_out, dev) || (num_edges > 0 && !is_device_memory(rcol, dev)))
+        return na_fail(MB_ERR_INVALID, "every array must be device memory of the current device");
+    // The scratch array's device address in the CURRENT context, looked up
+    // on every call (a lookup, no allocation): the host-side name
+    // g_pr_scratch is not a device address, and an address cached from an
+    // earlier context (before a cudaDeviceReset, or under another context
+    // the host made current through the driver API) would be stale.  The
+    // first call in a context also loads the library's device code there.
     float *scratch = nullptr;
+    {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_pr_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return na_fail(MB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        }
+        scratch = (float *)p;
+    }
     int sms = 0;
     {
-        // First call on a device: look up the scratch array's device address
-        // (the host-side name g_pr_scratch is not a device address).
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_addr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_pr_scratch);
+        if (!g_num_sms[dev]) {
+            const cudaError_t e = cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) {
                 cudaGetLastError();
-                return na_fail(MB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
-                                                cudaGetErrorString(e));
+                g_num_sms[dev] = 0;
+                return na_fail(MB_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
             }
-            e = cudaDeviceGetAttribute(&g_num_sms[dev], cudaDevAttrMultiProcessorCount, dev);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                return na_fail(MB_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") +
-                                                cudaGetErrorString(e));
-            }
-            g_scratch_addr[dev] = (float *)p;
         }
-        scratch = g_scratch_addr[dev];
         sms = g_num_sms[dev];
     }
     cudaStream_t s = (cudaStream_t)stream;

@@ -306,6 +306,244 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
     }
 }
 
+// ---- the reference's order (MB_PR_ORDER_REFERENCE), in parallel -------------
+// Every vertex's sum is the reference's sequential float fold over its MEG
+// slots, bit for bit (pr_order.cuh).  Three mappings by in-degree n:
+//   n <= kPrLight: k_pr_light over light lists copied from the MEG order;
+//   kPrLight < n <= hub_min: sliced ELL -- vertices sorted by in-degree, 32
+//     per group; row j of a group holds slot j of each of its vertices, so a
+//     warp reads a row with one coalesced load and lane l folds its own
+//     vertex in order (k_pr_sell);
+//   n > hub_min: one CTA per vertex, the parallel integer scan of
+//     pr_order.cuh (k_pr_hub_exact), run on a side stream beside the others.
+constexpr int kSellU = 16;                      // rows of a group in flight
+constexpr int kHubK = 16;                       // consecutive slots per thread
+constexpr int kHubBig = 16384;                  // in-degree above which a hub gets the big CTA
+constexpr int kHubMinDefault = 2048;
+
+struct ExactArgs {
+    const int32_t *rrow, *meg_src, *outdeg;
+    const float *contrib_in;
+    float *contrib_out, *rank_out;
+    const int32_t *sell_v;       // 32 vertices per group (-1: padding), sorted by in-degree
+    const int64_t *sell_base;    // first element of each group in sell_src
+    const int32_t *sell_rows;    // rows of each group (its largest in-degree)
+    const int32_t *sell_src;     // group g, row j, lane l at sell_base[g] + 32 j + l (-1: padding)
+    int32_t ngroups;
+    const int32_t *hub_v;        // hubs, largest in-degree first
+    int32_t nhub;
+};
+
+__device__ __forceinline__ void x_write(const ExactArgs &a, int32_t v, float sum, int32_t d) {
+    const float r = pr_update(sum);
+    a.rank_out[v] = r;
+    a.contrib_out[v] = d > 0 ? r / (float)d : 0.0f;
+}
+
+__device__ __forceinline__ int4 ld_stream4(const int4 *p) {
+    int4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+    return v;
+}
+
+// Sliced ELL: one warp per group, kSellU rows (coalesced index loads, then
+// the gathers) in flight; each lane folds its own vertex's slots in order.
+// Padding slots (-1) read 0, and s + 0 = s, so they change no bit.
+__global__ void __launch_bounds__(256) k_pr_sell(ExactArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < a.ngroups; g += warps) {
+        const int32_t v = __ldg(&a.sell_v[g * 32 + lane]);
+        const int32_t rows = __ldg(&a.sell_rows[g]);
+        const int32_t d = v >= 0 ? __ldg(&a.outdeg[v]) : 0;
+        const int32_t *src = a.sell_src + __ldg(&a.sell_base[g]) + lane;
+        float sum = 0.f;
+        // the next rows' indices load while this block's gathers are in flight
+        int32_t nxt[kSellU];
+#pragma unroll
+        for (int u = 0; u < kSellU; u++) nxt[u] = u < rows ? ld_stream(src + (int64_t)u * 32) : -1;
+        for (int32_t j0 = 0; j0 < rows; j0 += kSellU) {
+            int32_t idx[kSellU];
+#pragma unroll
+            for (int u = 0; u < kSellU; u++) idx[u] = nxt[u];
+#pragma unroll
+            for (int u = 0; u < kSellU; u++) {
+                const int32_t j = j0 + kSellU + u;
+                nxt[u] = j < rows ? ld_stream(src + (int64_t)j * 32) : -1;
+            }
+            float x[kSellU];
+#pragma unroll
+            for (int u = 0; u < kSellU; u++) x[u] = idx[u] >= 0 ? ld_gather(&a.contrib_in[idx[u]]) : 0.f;
+#pragma unroll
+            for (int u = 0; u < kSellU; u++) sum += x[u];
+        }
+        if (v >= 0) x_write(a, v, sum, d);
+    }
+}
+
+// The kHubK slot sources of thread `tid`'s part of the chunk at `pos`
+// (-1 past the vertex's end).  src + pos is 16-byte aligned.
+template <int kT>
+__device__ __forceinline__ void hub_idx(const int32_t *src, int32_t n, int32_t pos, int32_t (&idx)[kHubK]) {
+    const int32_t j0 = pos + (int32_t)threadIdx.x * kHubK;
+    if (j0 + kHubK <= n) {
+        const int4 *p4 = reinterpret_cast<const int4 *>(src + j0);
+#pragma unroll
+        for (int r = 0; r < kHubK / 4; r++) {
+            const int4 t4 = ld_stream4(p4 + r);
+            idx[4 * r] = t4.x;
+            idx[4 * r + 1] = t4.y;
+            idx[4 * r + 2] = t4.z;
+            idx[4 * r + 3] = t4.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kHubK; k++) idx[k] = j0 + k < n ? ld_stream(src + j0 + k) : -1;
+    }
+}
+
+__device__ __forceinline__ void hub_gather(const ExactArgs &a, const int32_t (&idx)[kHubK], float (&x)[kHubK]) {
+#pragma unroll
+    for (int k = 0; k < kHubK; k++) x[k] = idx[k] >= 0 ? ld_gather(&a.contrib_in[idx[k]]) : 0.f;
+}
+
+// Hubs [h0, h1) of the list: one CTA of kT threads per vertex.  The first
+// kHead slots (plus up to 3, so the rest starts on a 16-byte boundary) are
+// gathered by every thread and folded by thread 0; then chunks of kT * kHubK
+// slots, thread t owning kHubK consecutive ones, go through the integer
+// scan of pr_order.cuh.  The loads run ahead of the scans: each chunk's
+// sources load two chunks early and its contributions one chunk early.
+template <int kT, int kHead>
+__global__ void __launch_bounds__(kT) k_pr_hub_exact(ExactArgs a, int32_t h0, int32_t h1) {
+    constexpr int kW = kT / 32;
+    constexpr int kChunk = kT * kHubK;
+    __shared__ __align__(16) float head[kHead + 4];
+    __shared__ uint32_t wtot[kW];
+    __shared__ int32_t wbad[kW];
+    __shared__ float s_sh;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int32_t h = h0 + blockIdx.x; h < h1; h += gridDim.x) {
+        const int32_t v = __ldg(&a.hub_v[h]);
+        const int64_t b = __ldg(&a.rrow[v]);
+        const int32_t n = (int32_t)(__ldg(&a.rrow[v + 1]) - b);
+        const int32_t *src = a.meg_src + b;
+        const int32_t H = min(n, kHead + (int32_t)((4 - ((b + kHead) & 3)) & 3));
+        for (int i = tid; i < H; i += kT) head[i] = ld_gather(&a.contrib_in[ld_stream(src + i)]);
+        // the first two chunks' loads go out before the head is folded
+        int32_t idx[kHubK];
+        float x[kHubK], xn[kHubK];
+        hub_idx<kT>(src, n, H, idx);
+        hub_gather(a, idx, xn);
+        hub_idx<kT>(src, n, H + kChunk, idx);
+        __syncthreads();
+        if (tid == 0) {  // the adds chain; the shared loads run ahead, 4 at a time
+            float s0 = 0.f;
+            const float4 *h4 = reinterpret_cast<const float4 *>(head);
+            int i = 0;
+#pragma unroll 8
+            for (; i + 4 <= H; i += 4) {
+                const float4 t = h4[i >> 2];
+                s0 += t.x;
+                s0 += t.y;
+                s0 += t.z;
+                s0 += t.w;
+            }
+            for (; i < H; i++) s0 += head[i];
+            s_sh = s0;
+        }
+        __syncthreads();
+        float s = s_sh;
+        for (int32_t pos = H; pos < n; pos += kChunk) {
+#pragma unroll
+            for (int k = 0; k < kHubK; k++) x[k] = xn[k];
+            if (pos + kChunk < n) {
+                hub_gather(a, idx, xn);                       // chunk pos + kChunk
+                hub_idx<kT>(src, n, pos + 2 * kChunk, idx);   // chunk pos + 2 kChunk
+            }
+            int start = 0;  // threads before it have folded their slots
+            for (;;) {
+                const uint32_t bits = __float_as_uint(s);
+                const uint32_t ks = bits >> 23, base = (bits & 0x7fffffu) | 0x800000u;
+                uint32_t L = 0;
+                bool tie = false;
+                if (tid >= start) {
+#pragma unroll
+                    for (int k = 0; k < kHubK; k++) L += pr_units(x[k], ks, tie);
+                    L = min(L, 1u << 23);
+                }
+                // inclusive prefix over the CTA.  Up to the first bad thread it
+                // stays below 2^24 + 2^23; past it a sum may wrap around 2^32,
+                // which changes nothing: only the first bad thread is used
+                uint32_t I = L;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, I, off);
+                    if (lane >= off) I += y;
+                }
+                if (kW > 1) {
+                    if (lane == 31) wtot[wid] = I;
+                    __syncthreads();
+                }
+                uint32_t total = __shfl_sync(0xffffffffu, I, 31);
+                if (kW > 1) {
+                    total = 0;
+#pragma unroll
+                    for (int w = 0; w < kW; w++) {
+                        const uint32_t t = wtot[w];
+                        if (w < wid) I += t;
+                        total += t;
+                    }
+                }
+                const bool bad = tid >= start && (ks == 0 || ks == 255 || tie || base + I >= (1u << 24));
+                const unsigned bm = __ballot_sync(0xffffffffu, bad);
+                int c;
+                if (kW > 1) {
+                    if (lane == 0) wbad[wid] = bm ? wid * 32 + __ffs(bm) - 1 : kT;
+                    __syncthreads();
+                    c = kT;
+#pragma unroll
+                    for (int w = 0; w < kW; w++) c = min(c, wbad[w]);
+                } else {
+                    c = bm ? __ffs(bm) - 1 : kT;
+                }
+                if (c == kT) {  // the whole chunk stayed in the binade
+                    s = pr_make(ks, base + total);
+                    break;
+                }
+                if (tid == c) {  // the float path from the exact running sum
+                    float s2 = c == start ? s : pr_make(ks, base + I - L);
+#pragma unroll
+                    for (int k = 0; k < kHubK; k++) s2 += x[k];
+                    s_sh = s2;
+                }
+                __syncthreads();
+                s = s_sh;
+                start = c + 1;
+                if (start >= kT) break;
+                if (kW == 1) __syncthreads();  // s_sh is written again before the next read
+            }
+        }
+        if (tid == 0) x_write(a, v, s, __ldg(&a.outdeg[v]));
+        __syncthreads();  // head and s_sh are reused by the next hub
+    }
+}
+
+// Group g of the sliced ELL: row j, lane l <- slot j of the group's vertex l.
+__global__ void k_sell_fill(const int32_t *sell_v, const int64_t *sell_base, const int32_t *sell_rows,
+                            int32_t ngroups, const int32_t *rrow, const int32_t *meg_src, int32_t *sell_src) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += warps) {
+        const int32_t v = sell_v[g * 32 + lane];
+        const int32_t rows = sell_rows[g];
+        const int64_t b = v >= 0 ? rrow[v] : 0;
+        const int32_t n = v >= 0 ? rrow[v + 1] - (int32_t)b : 0;
+        int32_t *dst = sell_src + sell_base[g] + lane;
+        for (int32_t j = 0; j < rows; j++) dst[(int64_t)j * 32] = j < n ? meg_src[b + j] : -1;
+    }
+}
+
 // Copy each light vertex's in-edge sources out of the reverse CSR.
 __global__ void k_light_copy(const int32_t *light_v, const int32_t *light_row, int32_t nlight,
                              const int32_t *rrow, const int32_t *rcol, int32_t *light_col) {
@@ -333,6 +571,21 @@ __global__ void k_pr_init(const int32_t *outdeg, int32_t V, float init, float *c
         const int32_t d = outdeg[u];
         contrib[u] = d > 0 ? init / (float)d : 0.0f;
     }
+}
+
+// The first superstep's contributions from a given rank vector.
+__global__ void k_pr_init_vec(const int32_t *outdeg, int32_t V, const float *init, float *contrib) {
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < V;
+         u += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = outdeg[u];
+        contrib[u] = d > 0 ? init[u] / (float)d : 0.0f;
+    }
+}
+
+__global__ void k_copy(float *dst, const float *src, int32_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
 }
 
 __global__ void k_fill(float *x, int32_t n, float v) {
@@ -505,13 +758,105 @@ void PrState::ensure(Context &ctx, const Graph &g) {
     built = true;
 }
 
+void PrState::ensure_exact(Context &ctx, const Graph &g, int32_t hub_min) {
+    if (exact_built && x_hub_min == hub_min) return;
+    build_meg_order(ctx, *const_cast<Graph *>(&g), *this);
+    release_exact();
+    const int32_t V = g.V;
+    cudaStream_t s = ctx.stream;
+    std::vector<int32_t> rrow((size_t)V + 1);
+    copy_sync(s, rrow.data(), g.rrow.p, sizeof(int32_t) * ((size_t)V + 1));
+    // light vertices in id order, their sources copied out of the MEG order
+    std::vector<int32_t> lv, lr(1, 0);
+    // mid vertices by in-degree, largest first (ties in id order): a
+    // counting sort over in-degrees kPrLight+1 .. hub_min
+    std::vector<int64_t> cnt((size_t)hub_min + 2, 0);
+    std::vector<int32_t> hubs;
+    for (int32_t v = 0; v < V; v++) {
+        const int32_t d = rrow[v + 1] - rrow[v];
+        if (d <= kPrLight) {
+            lv.push_back(v);
+            lr.push_back(lr.back() + d);
+        } else if (d <= hub_min) {
+            cnt[d]++;
+        } else {
+            hubs.push_back(v);
+        }
+    }
+    std::stable_sort(hubs.begin(), hubs.end(), [&](int32_t x, int32_t y) {
+        return rrow[x + 1] - rrow[x] > rrow[y + 1] - rrow[y];
+    });
+    std::vector<int64_t> at((size_t)hub_min + 2, 0);
+    int64_t nmid = 0;
+    for (int32_t d = hub_min; d > kPrLight; d--) {
+        at[d] = nmid;
+        nmid += cnt[d];
+    }
+    std::vector<int32_t> mid((size_t)nmid);
+    for (int32_t v = 0; v < V; v++) {
+        const int32_t d = rrow[v + 1] - rrow[v];
+        if (d > kPrLight && d <= hub_min) mid[at[d]++] = v;
+    }
+    ngroups = (int32_t)((nmid + 31) / 32);
+    std::vector<int32_t> sv((size_t)ngroups * 32, -1), rows((size_t)ngroups);
+    std::vector<int64_t> sbase((size_t)ngroups);
+    int64_t total = 0;
+    for (int32_t gi = 0; gi < ngroups; gi++) {
+        for (int l = 0; l < 32 && (int64_t)gi * 32 + l < nmid; l++) sv[(size_t)gi * 32 + l] = mid[(size_t)gi * 32 + l];
+        const int32_t v0 = sv[(size_t)gi * 32];
+        rows[gi] = rrow[v0 + 1] - rrow[v0];
+        sbase[gi] = total;
+        total += (int64_t)rows[gi] * 32;
+    }
+    x_nlight = (int32_t)lv.size();
+    x_light_v.reserve(sizeof(int32_t) * std::max<size_t>(lv.size(), 1));
+    x_light_row.reserve(sizeof(int32_t) * lr.size());
+    x_light_col.reserve(sizeof(int32_t) * std::max<size_t>((size_t)lr.back(), 1));
+    sell_v.reserve(sizeof(int32_t) * std::max<size_t>(sv.size(), 1));
+    sell_rows.reserve(sizeof(int32_t) * std::max<size_t>(rows.size(), 1));
+    sell_base.reserve(sizeof(int64_t) * std::max<size_t>(sbase.size(), 1));
+    sell_src.reserve(sizeof(int32_t) * (size_t)std::max<int64_t>(total, 1));
+    x_nhub = (int32_t)hubs.size();
+    x_hub_v.reserve(sizeof(int32_t) * std::max<size_t>(hubs.size(), 1));
+    if (x_nlight) {
+        copy_sync(s, x_light_v.p, lv.data(), 4 * lv.size());
+        copy_sync(s, x_light_row.p, lr.data(), 4 * lr.size());
+        k_light_copy<<<grid_for(x_nlight, 256, ctx.num_sms * 16), 256, 0, s>>>(
+            x_light_v.as<int32_t>(), x_light_row.as<int32_t>(), x_nlight, g.rrow.as<int32_t>(),
+            meg_src.as<int32_t>(), x_light_col.as<int32_t>());
+        MB_CHECK_LAUNCH();
+    }
+    if (ngroups) {
+        copy_sync(s, sell_v.p, sv.data(), 4 * sv.size());
+        copy_sync(s, sell_rows.p, rows.data(), 4 * rows.size());
+        copy_sync(s, sell_base.p, sbase.data(), 8 * sbase.size());
+        k_sell_fill<<<grid_for((int64_t)ngroups * 32, 256, ctx.num_sms * 16), 256, 0, s>>>(
+            sell_v.as<int32_t>(), sell_base.as<int64_t>(), sell_rows.as<int32_t>(), ngroups,
+            g.rrow.as<int32_t>(), meg_src.as<int32_t>(), sell_src.as<int32_t>());
+        MB_CHECK_LAUNCH();
+    }
+    if (x_nhub) copy_sync(s, x_hub_v.p, hubs.data(), 4 * hubs.size());
+    x_nbig = 0;  // the hubs are sorted: the big ones come first
+    while (x_nbig < x_nhub && rrow[hubs[x_nbig] + 1] - rrow[hubs[x_nbig]] > kHubBig) x_nbig++;
+    MB_CUDA(cudaStreamSynchronize(s));
+    if (!side) MB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    if (!ev_fork) MB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if (!ev_join) MB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    x_hub_min = hub_min;
+    exact_built = true;
+}
+
 void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init, int sched,
-                  mb_stats *stats) {
+                  mb_stats *stats, const float *init_vec) {
     st.ensure(ctx, g);
     const bool ref_order = ctx.pr_order == MB_PR_ORDER_REFERENCE;
-    if (ref_order) build_meg_order(ctx, g, st);
-    cudaStream_t s = ctx.stream;
     const bool unfused = sched == MB_SCHED_PUSH_UNFUSED;
+    const int32_t hub_min = ctx.tunable[MB_TUNE_PR_HUB_MIN] > 0
+                                ? (int32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_PR_HUB_MIN], 0x7fffffff)
+                                : kHubMinDefault;
+    if (ref_order) build_meg_order(ctx, g, st);
+    if (ref_order && !unfused) st.ensure_exact(ctx, g, hub_min);
+    cudaStream_t s = ctx.stream;
     auto args = [&](int parity) {
         PrArgs a;
         a.V = g.V;
@@ -551,7 +896,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     if (vpl <= 0) {
         vpl = 2;
         const int64_t warps = (int64_t)resident((const void *)k_pr_light<1>, kPrThreads) * kPrWarps;
-        while (vpl > 1 && (int64_t)st.nlight < (int64_t)32 * vpl * 4 * warps) vpl >>= 1;
+        const int64_t nl = ref_order && !unfused ? st.x_nlight : st.nlight;
+        while (vpl > 1 && nl < (int64_t)32 * vpl * 4 * warps) vpl >>= 1;
     }
     const int pair = ctx.tunable[MB_TUNE_PR_SHORT_PAIR] > 0 ? (int)ctx.tunable[MB_TUNE_PR_SHORT_PAIR]
                                                              : kShortPairDefault;
@@ -578,16 +924,69 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         MB_CUDA(cudaLaunchKernel(light_fn[vi], grid_light, kPrThreads, params, 0, cs));
     };
     const int grid_vtx = ctx.num_sms * 8;
+    const int grid_sell = resident((const void *)k_pr_sell, 256);
+    const int grid_hub_small = resident((const void *)k_pr_hub_exact<128, 256>, 128);
+    const int grid_hub_big = resident((const void *)k_pr_hub_exact<512, 512>, 512);
+    auto exact_args = [&](const PrArgs &a) {
+        ExactArgs x;
+        x.rrow = g.rrow.as<int32_t>();
+        x.meg_src = st.meg_src.as<int32_t>();
+        x.outdeg = g.outdeg.as<int32_t>();
+        x.contrib_in = a.contrib_in;
+        x.contrib_out = a.contrib_out;
+        x.rank_out = a.rank_out;
+        x.sell_v = st.sell_v.as<int32_t>();
+        x.sell_base = st.sell_base.as<int64_t>();
+        x.sell_rows = st.sell_rows.as<int32_t>();
+        x.sell_src = st.sell_src.as<int32_t>();
+        x.ngroups = st.ngroups;
+        x.hub_v = st.x_hub_v.as<int32_t>();
+        x.nhub = st.x_nhub;
+        return x;
+    };
     auto emit = [&](cudaStream_t cs) {
-        k_pr_init<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init, st.contrib[0].as<float>());
+        if (init_vec)
+            k_pr_init_vec<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init_vec, st.contrib[0].as<float>());
+        else
+            k_pr_init<<<grid_vtx, 256, 0, cs>>>(g.outdeg.as<int32_t>(), g.V, init, st.contrib[0].as<float>());
         MB_CHECK_LAUNCH();
         for (int it = 0; it < iters; it++) {
             PrArgs a = args(it & 1);
-            if (ref_order) {
-                if (unfused) k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
-                if (unfused) k_pr_pull<true, true><<<grid_pull, kPrThreads, 0, cs>>>(a);
-                else k_pr_pull<false, true><<<grid_pull, kPrThreads, 0, cs>>>(a);
+            if (ref_order && unfused) {
+                // the reference's send -> combine split over the message array,
+                // each vertex folded serially in MEG order
+                k_pr_send<<<grid_vtx, 256, 0, cs>>>(a);
+                k_pr_pull<true, true><<<grid_pull, kPrThreads, 0, cs>>>(a);
                 MB_CHECK_LAUNCH();
+                continue;
+            }
+            if (ref_order) {
+                ExactArgs x = exact_args(a);
+                // the big hubs (the longest chains of scans) on the side
+                // stream, beside the rest
+                const int32_t nbig = st.x_nbig, nsmall = st.x_nhub - st.x_nbig;
+                if (nbig) {
+                    MB_CUDA(cudaEventRecord(st.ev_fork, cs));
+                    MB_CUDA(cudaStreamWaitEvent(st.side, st.ev_fork, 0));
+                    k_pr_hub_exact<512, 512><<<std::min(nbig, grid_hub_big), 512, 0, st.side>>>(x, 0, nbig);
+                    MB_CHECK_LAUNCH();
+                }
+                if (nsmall)
+                    k_pr_hub_exact<128, 256><<<std::min(nsmall, grid_hub_small), 128, 0, cs>>>(x, nbig, st.x_nhub);
+                if (st.ngroups) k_pr_sell<<<grid_sell, 256, 0, cs>>>(x);
+                if (st.x_nlight) {
+                    PrArgs la = a;
+                    la.light_v = st.x_light_v.as<int32_t>();
+                    la.light_row = st.x_light_row.as<int32_t>();
+                    la.light_col = st.x_light_col.as<int32_t>();
+                    la.nlight = st.x_nlight;
+                    light(cs, la);
+                }
+                MB_CHECK_LAUNCH();
+                if (nbig) {
+                    MB_CUDA(cudaEventRecord(st.ev_join, st.side));
+                    MB_CUDA(cudaStreamWaitEvent(cs, st.ev_join, 0));
+                }
                 continue;
             }
             if (unfused) {
@@ -602,7 +1001,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             MB_CHECK_LAUNCH();
         }
         if (iters == 0) {  // no superstep: the ranks are the initial ranks
-            k_fill<<<grid_vtx, 256, 0, cs>>>(st.rank.as<float>(), g.V, init);
+            if (init_vec) k_copy<<<grid_vtx, 256, 0, cs>>>(st.rank.as<float>(), init_vec, g.V);
+            else k_fill<<<grid_vtx, 256, 0, cs>>>(st.rank.as<float>(), g.V, init);
             MB_CHECK_LAUNCH();
         }
     };
@@ -611,7 +1011,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     MB_CUDA(cudaEventCreate(&e1));
     try {
         if (ctx.use_graphs) {
-            if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_sched != sched ||
+            if (!st.exec || st.g_iters != iters || st.g_init != init || st.g_init_vec != init_vec ||
+                st.g_sched != sched ||
                 st.g_order != ctx.pr_order || st.g_tune != ctx.tune_gen) {
                 if (st.exec) cudaGraphExecDestroy(st.exec);
                 st.exec = nullptr;
@@ -629,6 +1030,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                 MB_CUDA(e);
                 st.g_iters = iters;
                 st.g_init = init;
+                st.g_init_vec = init_vec;
                 st.g_sched = sched;
                 st.g_order = ctx.pr_order;
                 st.g_tune = ctx.tune_gen;
@@ -652,10 +1054,12 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             stats->device_ms = ms;
             stats->schedule_count[unfused ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE] = iters;
             stats->edges_scanned = (int64_t)iters * g.E;
-            stats->kernel_launches =
-                ref_order ? 1 + (int64_t)iters * (1 + unfused) + (iters == 0)
-                          : 1 + (int64_t)iters * ((unfused ? 2 : st.nlight > 0) + (st.nitems > 0) + (st.nhub > 0)) +
-                                (iters == 0);
+            int64_t per_step;
+            if (ref_order && unfused) per_step = 2;
+            else if (ref_order)
+                per_step = (st.x_nbig > 0) + (st.x_nhub > st.x_nbig) + (st.ngroups > 0) + (st.x_nlight > 0);
+            else per_step = (unfused ? 2 : st.nlight > 0) + (st.nitems > 0) + (st.nhub > 0);
+            stats->kernel_launches = 1 + (int64_t)iters * per_step + (iters == 0);
         }
     } catch (...) {
         cudaEventDestroy(e0);

@@ -9,6 +9,7 @@ struct PrState {
     int32_t V = 0;
     int64_t E = 0;
     DevBuf rank, contrib[2], msg, items, hub_v, hub_first, blk_sum;
+    DevBuf init_stage;  // host initial ranks of mb_pagerank_from, staged
     int32_t nitems = 0, nhub = 0;
     int32_t nlong = 0;  // items longer than kPrShortItem (the head of the list)
     // light vertices (in-degree <= kPrLight) in id order, with their in-edge
@@ -20,23 +21,53 @@ struct PrState {
     // destination in MEG slot order, and each CSR edge's slot in it
     bool meg_built = false;
     DevBuf meg_src, meg_slot;
+    // the reference's order computed in parallel (built on first use): light
+    // lists copied from the MEG order, the mid vertices' sliced ELL, the hubs
+    bool exact_built = false;
+    int32_t x_hub_min = 0;  // in-degree above which a vertex is a hub
+    DevBuf x_light_v, x_light_row, x_light_col;
+    int32_t x_nlight = 0;
+    DevBuf sell_v, sell_base, sell_rows, sell_src;
+    int32_t ngroups = 0;
+    DevBuf x_hub_v;
+    int32_t x_nhub = 0;
+    int32_t x_nbig = 0;  // hubs [0, x_nbig) have more than kHubBig in-edges
+    // the hub kernel runs on a side stream beside the others (fork / join)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t exec = nullptr;  // captured run (init + iters supersteps)
     int32_t g_iters = -1, g_sched = -1, g_order = -1;
     uint64_t g_tune = ~0ull;  // tunables generation of the captured run
     float g_init = 0.f;
+    const float *g_init_vec = nullptr;  // the initial rank vector the capture reads
     ~PrState() { release(); }
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         g_iters = -1;
         rank.release(); contrib[0].release(); contrib[1].release(); msg.release();
+        init_stage.release();
         items.release(); hub_v.release(); hub_first.release(); blk_sum.release();
         light_v.release(); light_row.release(); light_col.release();
         meg_src.release(); meg_slot.release();
         meg_built = false;
+        release_exact();
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
+        ev_fork = ev_join = nullptr;
+        side = nullptr;
         built = false;
     }
+    void release_exact() {
+        x_light_v.release(); x_light_row.release(); x_light_col.release();
+        sell_v.release(); sell_base.release(); sell_rows.release(); sell_src.release();
+        x_hub_v.release();
+        exact_built = false;
+    }
     void ensure(Context &ctx, const Graph &g);
+    // the structures of the parallel reference-order sum (meg order included)
+    void ensure_exact(Context &ctx, const Graph &g, int32_t hub_min);
 };
 
 // The reference's MEG message order (GraphIR::sortByDegree +
@@ -46,9 +77,11 @@ void build_meg_order(Context &ctx, const Graph &g, PrState &st);
 // `iters` supersteps from a uniform initial rank; the ranks are left in
 // st.rank (device).  sched: MB_SCHED_PUSH_UNFUSED runs the reference's
 // send/combine split, anything else the fused pull; both give identical bits.
-// ctx.pr_order MB_PR_ORDER_REFERENCE: every vertex folds its messages
-// sequentially in the reference's MEG slot order (slower on hubs).
+// ctx.pr_order MB_PR_ORDER_REFERENCE: every vertex's sum is the reference's
+// sequential fold over its MEG slots, bit for bit (the fused pull computes
+// it in parallel; the message-reading schedule folds each vertex serially).
+// init_vec (device, nullable): initial ranks per vertex instead of `init`.
 void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init, int sched,
-                  mb_stats *stats);
+                  mb_stats *stats, const float *init_vec = nullptr);
 
 }  // namespace mb

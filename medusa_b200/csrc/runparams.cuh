@@ -32,6 +32,7 @@ struct RunParams {
                                 // exceed the unvisited out-edges (0: never)
     int32_t bfs_beta;           // BFS fixed rule: back to top-down below V / beta frontier vertices
     int32_t bfs_gamma;          // BFS fixed rule: bottom-up only from E / gamma frontier out-edges (0: any)
+    int64_t wait_polls;         // polls before a bounded device wait gives up (-1: each wait's default)
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 

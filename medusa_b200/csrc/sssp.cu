@@ -134,6 +134,7 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
     const uint32_t *qo = pick(a.f.qo, cur);
     const int32_t *tf = pick(a.f.tf, cur);
     const uint32_t tiles = (m + kTile - 1) / kTile;
+    const uint32_t bulk_polls = c->p.wait_polls >= 0 ? (uint32_t)min(c->p.wait_polls, (int64_t)kBulkSpins) : kBulkSpins;
     uint32_t cn = 0;
     bool stop = false;  // block-uniform: a bulk copy timed out
     for (uint32_t t = blockIdx.x; t < tiles && !stop; t += gridDim.x) {
@@ -152,9 +153,11 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
             bulk_g2s(sm.qo_st, qo + a0, bytes, &sm.bar);
             bulk_g2s(sm.qv_st, qv + a0, bytes, &sm.bar);
         }
-        const bool staged = !kBulk || mbar_wait(&sm.bar, parity);  // the same for every thread
-        if (!staged) {  // never seen: record it, give the copies one more
-            // bounded wait, and relax nothing more
+        // the same for every thread
+        const bool staged = !kBulk || mbar_wait(&sm.bar, parity, bulk_polls);
+        if (!staged) {  // record it, let the copies finish (a wait with the
+            // full budget: no copy may still be landing when the CTA moves
+            // on), and relax nothing more
             if (threadIdx.x == 0) atomicOr(&c->err, ERR_BULK);
             mbar_wait(&sm.bar, parity);
             k = 0;
@@ -1079,7 +1082,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     // each superstep lowers some distance; with integer distances below 2^24
     // a run cannot need more supersteps than this
     sp.app = APP_SSSP;
-    sp.cap = (int)std::min<int64_t>((int64_t)g.V * 4 + 16, 1 << 30);
+    sp.cap = step_cap(ctx, (int64_t)g.V * 4 + 16);
     sp.name = "sssp";
     sp.prologue = [&](cudaStream_t s) {
         k_fill_dist<<<grid_vtx, 256, 0, s>>>(a);

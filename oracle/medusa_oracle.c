@@ -196,13 +196,17 @@ int orc_pagerank_f32(int32_t V, int64_t E, const int32_t *e_src,
 {
     float *msg = (float *)malloc(sizeof(float) * (size_t)(E > 0 ? E : 1));
     if (!msg) return -1;
+    /* Every slot and every vertex is written by one OpenMP thread, and each
+     * vertex's fold runs in one thread in its own order, so the bits do not
+     * depend on the thread count. */
     for (int it = 0; it < iters; it++) {
-        for (int64_t e = 0; e < E; e++) msg[e] = 0.0f;
+#pragma omp parallel for schedule(static)
         for (int64_t e = 0; e < E; e++) {
             int32_t s = e_src[e];
             int32_t cnt = edge_index[s + 1] - edge_index[s];
             msg[msg_dst[e]] = rank[s] / (float)cnt;
         }
+#pragma omp parallel for schedule(dynamic, 4096)
         for (int32_t v = 0; v < V; v++) {
             float sum = 0.0f;
             if (order == 1) {
@@ -219,7 +223,10 @@ int orc_pagerank_f32(int32_t V, int64_t E, const int32_t *e_src,
 }
 
 /* The same PageRank in FP64 throughout: the accuracy yardstick for both the
- * reference FP32 result and the GPU FP32 result. */
+ * reference FP32 result and the GPU FP32 result.  The scatter and the
+ * per-vertex sums are split over OpenMP threads (each message slot and each
+ * vertex is written by one thread, so the result does not depend on the
+ * thread count). */
 int orc_pagerank_f64(int32_t V, int64_t E, const int32_t *e_src,
                      const int32_t *msg_dst, const int32_t *msg_index,
                      const int32_t *edge_index, int iters, double *rank)
@@ -227,11 +234,12 @@ int orc_pagerank_f64(int32_t V, int64_t E, const int32_t *e_src,
     double *msg = (double *)malloc(sizeof(double) * (size_t)(E > 0 ? E : 1));
     if (!msg) return -1;
     for (int it = 0; it < iters; it++) {
-        for (int64_t e = 0; e < E; e++) msg[e] = 0.0;
+#pragma omp parallel for schedule(static)
         for (int64_t e = 0; e < E; e++) {
             int32_t s = e_src[e];
             msg[msg_dst[e]] = rank[s] / (double)(edge_index[s + 1] - edge_index[s]);
         }
+#pragma omp parallel for schedule(dynamic, 4096)
         for (int32_t v = 0; v < V; v++) {
             double sum = 0.0;
             for (int32_t i = msg_index[v]; i < msg_index[v + 1]; i++) sum += msg[i];

@@ -45,39 +45,23 @@ def test_tune_batch(gpu_ctx):
 
 
 def test_tune_pagerank_keeps_results(gpu_ctx):
+    """Both summation orders: the tuned launch shapes (hub threshold in the
+    reference's order, short-block pairing in the fixed order) change no bit."""
     from medusa_b200 import api, autotune
     g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.57, 0.19, 0.19, seed=3))
     try:
-        r0, _ = g.pagerank(5, 1.0 / g.V)
-        best, table = autotune.tune_pagerank(gpu_ctx, g, 5, reps=1)
-        assert set(best) == {"pr_light_vpl", "pr_short_pair"} and len(table) >= 5
-        r1, _ = g.pagerank(5, 1.0 / g.V)
-        np.testing.assert_array_equal(r0.view(np.uint32), r1.view(np.uint32))
+        for order, keys in ((api.MB_PR_ORDER_REFERENCE, {"pr_light_vpl", "pr_hub_min"}),
+                            (api.MB_PR_ORDER_FIXED, {"pr_light_vpl", "pr_short_pair"})):
+            gpu_ctx.set_pagerank_order(order)
+            r0, _ = g.pagerank(5, 1.0 / g.V)
+            best, table = autotune.tune_pagerank(gpu_ctx, g, 5, reps=1)
+            assert set(best) == keys and len(table) >= 5
+            r1, _ = g.pagerank(5, 1.0 / g.V)
+            np.testing.assert_array_equal(r0.view(np.uint32), r1.view(np.uint32))
+            for k in keys:
+                gpu_ctx.set_tunable(k, -1)
     finally:
+        gpu_ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
         g.close()
-        gpu_ctx.set_tunable("pr_light_vpl", -1)
-        gpu_ctx.set_tunable("pr_short_pair", -1)
-
-
-def test_bfs_rule_tunables_keep_levels(gpu_ctx):
-    """The direction-optimising rule's alpha (0: never bottom-up), beta and
-    gamma (the frontier-size floor for bottom-up) change only which schedule
-    runs: levels stay those of the default rule."""
-    from medusa_b200 import api
-    g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.45, 0.15, 0.15, seed=5))
-    try:
-        lv0, st0 = g.bfs([0])
-        assert st0["schedule_count"][4] > 0  # the default rule pulls on this graph
-        for alpha, beta, gamma in ((0, 20, 16), (1, 1, 0), (1000, 1000, 0), (4, 5, 1000), (15, 20, 1)):
-            gpu_ctx.set_tunable("bfs_alpha", alpha)
-            gpu_ctx.set_tunable("bfs_beta", beta)
-            gpu_ctx.set_tunable("bfs_gamma", gamma)
-            lv, st = g.bfs([0])
-            np.testing.assert_array_equal(lv, lv0)
-            if alpha == 0:
-                assert st["schedule_count"][4] == 0
-    finally:
-        g.close()
-        gpu_ctx.set_tunable("bfs_alpha", -1)
-        gpu_ctx.set_tunable("bfs_beta", -1)
-        gpu_ctx.set_tunable("bfs_gamma", -1)
+        for k in ("pr_light_vpl", "pr_short_pair", "pr_hub_min"):
+            gpu_ctx.set_tunable(k, -1)

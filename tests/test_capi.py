@@ -117,3 +117,17 @@ def test_generator_rejects_bad_params(api):
     for p in bad:
         with pytest.raises(api.MedusaError):
             api.generate_edges_host(p)
+
+
+def test_pagerank_noalloc_rejects_bad_sizes_without_touching_memory(api):
+    """Size and null checks come before any CUDA call: an oversize graph is
+    MB_ERR_UNSUPPORTED with the limit in the message, a null array or a
+    negative count MB_ERR_INVALID (no GPU needed)."""
+    lib = api.lib
+    rc = lib.mb_pagerank_noalloc(None, None, None, (1 << 20) + 1, 10, 1, 0.5, None, None)
+    assert rc == api.MB_ERR_UNSUPPORTED
+    assert b"limit" in lib.mb_last_error(None)
+    assert lib.mb_pagerank_noalloc(None, None, None, 4, 10, 1, 0.5, None, None) == api.MB_ERR_INVALID
+    assert lib.mb_pagerank_noalloc(None, None, None, 0, 10, 1, 0.5, None, None) == api.MB_ERR_INVALID
+    assert lib.mb_pagerank_noalloc(None, None, None, 4, -1, 1, 0.5, None, None) == api.MB_ERR_INVALID
+    assert lib.mb_pagerank_noalloc(None, None, None, 4, 10, -1, 0.5, None, None) == api.MB_ERR_INVALID

@@ -89,24 +89,32 @@ def test_sssp_bulk_staged_push_matches_reference(ctx, api, name):
         g.close()
 
 
-def check_pagerank(got, ref, r64, indeg, tol=1e-5, hub=2048):
-    from test_oracle import check_pagerank as chk
-    chk(got, ref, r64, indeg, tol, hub)
-
-
 @pytest.mark.parametrize("name", golden_names())
-def test_pagerank_matches_reference(ctx, name):
+def test_pagerank_matches_reference(ctx, api, name):
+    """The default order is the reference's: its FP32 ranks bit for bit (the
+    1e-5 rule with 0 error), and the oracle's MEG-order fold equally.  The
+    fixed parallel order equals the oracle run in that order bit for bit and
+    stays within the FP32 summation bound of the FP64 ranks."""
+    from test_oracle import check_pagerank
     c = load_golden(name)
     g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
-    r, st = g.pagerank(c["pr_iters"], 1.0 / c["V"])
-    aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
-    indeg = np.diff(aa.msg_index)
-    r64 = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], fp64=True)
-    check_pagerank(r, c["pr_rank"], r64, indeg)
-    # bit for bit against the oracle run in the kernels' summation order
-    ro = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], order="device")
-    np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
-    g.close()
+    try:
+        r, st = g.pagerank(c["pr_iters"], 1.0 / c["V"])
+        np.testing.assert_array_equal(r.view(np.uint32), c["pr_rank"].view(np.uint32))
+        assert check_pagerank(r, c["pr_rank"]) == 0.0
+        aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+        ro = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"])
+        np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
+        ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
+        rf, _ = g.pagerank(c["pr_iters"], 1.0 / c["V"])
+        rd = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], order="device")
+        np.testing.assert_array_equal(rf.view(np.uint32), rd.view(np.uint32))
+        r64 = O.pagerank(c["V"], aa, None, c["pr_iters"], 1.0 / c["V"], fp64=True)
+        bound = (float(np.diff(aa.msg_index).max(initial=0)) + 8) * 2.0 ** -24 * 4
+        assert (np.abs(rf - r64) / r64).max(initial=0) <= bound
+    finally:
+        ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
+        g.close()
 
 
 def test_pagerank_launch_shapes_keep_every_bit(ctx, api):
@@ -122,6 +130,7 @@ def test_pagerank_launch_shapes_keep_every_bit(ctx, api):
     aa = O.AAGraph(V, src, dst, None)
     ro = O.pagerank(V, aa, None, 5, 1.0 / V, order="device")
     g = ctx.graph_from_edges(V, src, dst, None)
+    ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
     try:
         for vpl in (1, 2, 4):
             for pair in (1, 2, 4):
@@ -134,6 +143,7 @@ def test_pagerank_launch_shapes_keep_every_bit(ctx, api):
                                                   err_msg="vpl %d pair %d schedule %d" % (vpl, pair, sched))
     finally:
         ctx.set_policy(api.MB_POLICY_FIXED)
+        ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
         ctx.set_tunable("pr_light_vpl", -1)
         ctx.set_tunable("pr_short_pair", -1)
         g.close()
@@ -156,7 +166,6 @@ def test_pagerank_reference_order_is_the_reference_bit_for_bit(ctx, api, name):
                                           err_msg="schedule %d" % sched)
     finally:
         ctx.set_policy(api.MB_POLICY_FIXED)
-        ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
         g.close()
 
 
@@ -337,9 +346,18 @@ def test_full_size_pagerank_c1_against_oracle(gpu_ctx, api):
     r, st = g.pagerank(10, 1.0 / V)
     aa = O.AAGraph(V, s_, d_)
     ro = O.pagerank(V, aa, None, 10, 1.0 / V)
-    # in-degrees are all <= 64: the kernels' order is the reference's fold
-    assert np.diff(aa.msg_index).max() <= 64
+    # the reference's MEG-order fold, bit for bit
     np.testing.assert_array_equal(r.view(np.uint32), ro.view(np.uint32))
+    # the fixed order: in-degrees are all <= 64, so it is the sequential
+    # fold in AA slot order
+    assert np.diff(aa.msg_index).max() <= 64
+    gpu_ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
+    try:
+        rf, _ = g.pagerank(10, 1.0 / V)
+    finally:
+        gpu_ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
+    ra = O.pagerank(V, aa, None, 10, 1.0 / V, order="aa")
+    np.testing.assert_array_equal(rf.view(np.uint32), ra.view(np.uint32))
     g.close()
 
 

@@ -20,31 +20,44 @@ def test_oracle_bfs_sssp_match_reference_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", golden_names())
-def test_oracle_pagerank_within_tolerance(name):
+def test_oracle_pagerank_is_the_reference_bit_for_bit(name):
+    """The oracle folds each vertex's messages in the reference's MEG slot
+    order: its FP32 ranks are the reference's own, hubs included; and they
+    meet the per-vertex 1e-5 rule against the reference with nothing to
+    spare (0).  The FP64 oracle is the accuracy yardstick for both."""
     c = load_golden(name)
     g = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
     r = O.pagerank(c["V"], g, None, c["pr_iters"], 1.0 / c["V"])
+    np.testing.assert_array_equal(r.view(np.uint32), c["pr_rank"].view(np.uint32))
+    check_pagerank(r, c["pr_rank"])
     r64 = O.pagerank(c["V"], g, None, c["pr_iters"], 1.0 / c["V"], fp64=True)
-    check_pagerank(r, c["pr_rank"], r64, np.diff(g.msg_index))
+    # the reference's FP32 sums are within a few ulp per in-edge of exact
+    indeg = np.diff(g.msg_index)
+    bound = (float(indeg.max(initial=0)) + 8) * 2.0 ** -24 * 4
+    assert (np.abs(r - r64) / r64).max(initial=0) <= bound
 
 
-def check_pagerank(got, ref, r64, indeg, tol=1e-5, hub=2048):
-    """The PageRank parity rule.  The reference sums each vertex's messages in
-    FP32 in its MEG slot order; another order rounds differently.  A graph
-    whose in-degrees are all <= `hub`: every vertex within `tol` relative of
-    the reference.  A graph with larger in-degrees: a hub's FP32 sum can
-    differ by up to (n-1)*2^-24 relative between two orders, and that error
-    flows to the hub's out-neighbours, so both results are held to that
-    summation bound (x4 for the supersteps' carry) against the FP64 oracle."""
+def check_pagerank(got, ref, tol=1e-5):
+    """The PageRank parity rule: every vertex within `tol` relative of the
+    reference's FP32 rank."""
     got = got.astype(np.float64)
     ref = ref.astype(np.float64)
-    if indeg.max(initial=0) <= hub:
-        rel = np.abs(got - ref) / np.abs(ref)
-        assert rel.max(initial=0) <= tol, rel.max()
-        return
-    bound = (float(indeg.max()) + 8) * 2.0 ** -24 * 4
-    assert (np.abs(got - r64) / r64).max() <= bound
-    assert (np.abs(ref - r64) / r64).max() <= bound
+    rel = np.abs(got - ref) / np.abs(ref)
+    assert rel.max(initial=0) <= tol, rel.max()
+    return float(rel.max(initial=0))
+
+
+def test_other_orders_break_the_rule_on_a_hub():
+    """Why only the reference's own order is used for the rule: on the golden
+    graph with a 5000-in-edge hub, the same sequential fold over the AA slot
+    order, and the fixed parallel order, both land more than 1e-5 from the
+    reference's FP32 ranks (the reference itself is about 1.7e-5 from exact)."""
+    c = load_golden("hub")
+    g = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
+    ref = c["pr_rank"].astype(np.float64)
+    for order in ("aa", "device"):
+        r = O.pagerank(c["V"], g, None, c["pr_iters"], 1.0 / c["V"], order=order)
+        assert (np.abs(r - ref) / ref).max() > 1e-5, order
 
 
 def _butterfly_fold(m):
@@ -96,7 +109,7 @@ def test_oracle_device_order_on_a_star(n):
     want = np.float32(0.15 + np.float64(np.float32(np.float64(sm) * 0.85)))
     assert r[0] == want
     if n <= 64:
-        assert r[0] == O.pagerank(V, g, None, 1, init)[0]
+        assert r[0] == O.pagerank(V, g, None, 1, init, order="aa")[0]
 
 
 def test_oracle_layout_matches_reference_builders():
@@ -137,4 +150,35 @@ def test_oracle_equals_reference_random(seed):
     r = O.pagerank(V, src, dst, 10, 1.0 / V)
     rp = O.RefGraph("pr", V, src, dst)
     ref = rp.pagerank(10, 1.0 / V)[0]
-    assert (np.abs(r - ref) / ref).max() <= 1e-5
+    np.testing.assert_array_equal(r.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("kind,params", [
+    ("rmat", dict(scale=12, num_edges=50000, a=0.45, b=0.15, c=0.15, seed=3, wmin=1, wmax=1000)),
+    ("rmat", dict(scale=11, num_edges=30001, a=0.57, b=0.19, c=0.19, seed=9)),
+    ("uniform", dict(num_vertices=3000, num_edges=20000, seed=5, wmin=1, wmax=100)),
+    ("grid", dict(rows=37, cols=41, drop_frac=0.1, shortcut_frac=0.005, seed=2, wmin=1, wmax=100)),
+])
+def test_oracle_generator_equals_the_products(kind, params):
+    """The oracle's own generator (gen.c) makes exactly the product's edge
+    lists, so CPU-side inputs need nothing from the product library."""
+    from medusa_b200 import api
+    V, s, d, w = O.generate(kind, **params)
+    p = dict(params)
+    if kind == "rmat":
+        gp = api.rmat_params(p["scale"], p["num_edges"], p["a"], p["b"], p["c"], seed=p["seed"],
+                             wmin=p.get("wmin", 0), wmax=p.get("wmax", 0))
+    elif kind == "uniform":
+        gp = api.uniform_params(p["num_vertices"], p["num_edges"], seed=p["seed"], wmin=p["wmin"],
+                                wmax=p["wmax"])
+    else:
+        gp = api.grid_params(p["rows"], p["cols"], p["drop_frac"], p["shortcut_frac"], seed=p["seed"],
+                             wmin=p["wmin"], wmax=p["wmax"])
+    V2, s2, d2, w2 = api.generate_edges_host(gp)
+    assert V == V2
+    np.testing.assert_array_equal(s, s2)
+    np.testing.assert_array_equal(d, d2)
+    if w2 is None:
+        assert w is None
+    else:
+        np.testing.assert_array_equal(w.view(np.uint32), w2.view(np.uint32))
