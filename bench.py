@@ -60,7 +60,6 @@ SEED = 1
 C2 = dict(scale=20, num_edges=1 << 24, a=0.45, b=0.15, c=0.15, wmin=1, wmax=1000)
 C1 = dict(num_vertices=1 << 18, num_edges=1 << 22)
 PR_ITERS = 10
-C3_SAMPLE_SIDE = 512  # the C3 CPU baseline's grid side (a bounded sample)
 TRAIN_SCALES = (14, 17, 20)  # log2 vertices of the scheduler's trace graphs
 TRAIN_ROUNDS = 3  # trace collections: fixed-rule trajectories, then the learned policy's
 METRIC = "BFS/SSSP GTEPS (R-MAT 2^20 V / 2^24 E, source 0)"
@@ -493,11 +492,10 @@ def bench_configs(ctx, api, args, flush):
     g.close()
     if not args.no_cpu_baseline:
         out["c3_grid"]["cpu_baseline"] = cpu_baseline_traversals(
-            host_edges("grid", rows=C3_SAMPLE_SIDE, cols=C3_SAMPLE_SIDE, drop_frac=0.1,
-                       shortcut_frac=0.005, seed=SEED, wmin=1, wmax=100),
-            "one BFS + one SSSP from the corner of a %dx%d grid of the same generator (the "
-            "1448x1448 grid's reference run takes minutes: its edge-centric sweeps scale with the "
-            "diameter)" % (C3_SAMPLE_SIDE, C3_SAMPLE_SIDE))
+            host_edges("grid", rows=1448, cols=1448, drop_frac=0.1, shortcut_frac=0.005,
+                       seed=SEED, wmin=1, wmax=100),
+            "one BFS + one SSSP from the corner on the full C3 graph (reference Medusa_Exec_CPU, "
+            "OpenMP)")
     reset_tunables(ctx, api)
     del lv, dd
     # C4a: 64 BFS + 32 SSSP sources on R-MAT 2^22 / 2^26, batched vs one loop per source
@@ -599,7 +597,9 @@ def bench_many_graphs(ctx, api, reps, tune=True):
     one = float(np.median(ms))
     r_all = ranks.cpu().numpy()
     l_all = levels.cpu().numpy()
-    # the same work one graph at a time through mb_pagerank / mb_bfs
+    # the same work one graph at a time through mb_pagerank / mb_bfs (the
+    # many-graph kernel sums in the fixed order)
+    ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED)
     seq_ms, same = 0.0, True
     for i, p in enumerate(ps):
         g = ctx.generate(p)
@@ -609,6 +609,7 @@ def bench_many_graphs(ctx, api, reps, tune=True):
         same &= bool(np.array_equal(r.view(np.uint32), r_all[b.vbase[i]:b.vbase[i + 1]].view(np.uint32))
                      and np.array_equal(lv[0], l_all[b.vbase[i]:b.vbase[i + 1]]))
         g.close()
+    ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
     edges = st["edges_traversed"]
     res = {"workload": "256 R-MAT graphs, (0.45,0.15,0.15,0.25), vertices 2^10..2^18 log-uniform, "
                        "average degree uniform [4,32], seed 1; 20 PageRank supersteps + one BFS "

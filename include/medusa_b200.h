@@ -261,7 +261,8 @@ int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *l
 /* ---- many graphs in one launch (no reference counterpart) ----------------- */
 /* A batch of independent graphs (reference order), e.g. 256 R-MAT graphs of
  * uneven sizes.  mb_batch_run runs, for every graph, `pr_iters` PageRank
- * supersteps from 1/V (as mb_pagerank) and then one BFS (as mb_bfs) from
+ * supersteps from 1/V (as mb_pagerank in MB_PR_ORDER_FIXED, bit for bit) and
+ * then one BFS (as mb_bfs) from
  * sources[i] (nullable: vertex 0), all in ONE persistent cooperative launch
  * fed by a device work queue; each graph is worked by a team of CTAs sized
  * by its edge count.  Outputs are concatenated: graph i's ranks and levels
