@@ -169,7 +169,8 @@ def sssp_bytes(st, V):
 
 
 BRANCH_KERNELS = {0: "k_push_edge_q", 1: "k_push_warp_q", 4: "k_pull_stream", 5: "k_pull_warp",
-                  6: "reference split", 7: "full pull", 17: "k_tail", 19: "k_push_edge_bm + k_nbm2q"}
+                  6: "reference split", 7: "full pull", 17: "k_tail", 19: "k_push_edge_bm + k_nbm2q",
+                  20: "k_push_edge_q (two CTAs per SM)"}
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dominant_kernel_traffic.md")
 
 

@@ -337,7 +337,11 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 waited for with the full budget before the CTA moves on */
 #define MB_TUNE_STEP_CAP 14 /* superstep cap of the BFS / SSSP loops (default V+4 for BFS,
                               4V+16 for SSSP, V+8 batched BFS); past it MB_ERR_TIMEOUT */
-#define MB_NUM_TUNABLES 15
+#define MB_TUNE_SMALL_PUSH_EDGES 15 /* frontier out-edges up to which schedule 0 (above the
+                                      persistent tail's limits) runs on a grid of two CTAs
+                                      per SM instead of the full push grid (default
+                                      2 x SMs x 512; 0: never) */
+#define MB_NUM_TUNABLES 16
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

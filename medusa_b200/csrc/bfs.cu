@@ -575,6 +575,11 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
     sp.branch = [&](int branch, cudaStream_t s) {
         // BFS never routes to the bitmap-output push (bm_push_min is 0)
         if (branch == kBranchPushBm) branch = MB_SCHED_PUSH_EDGE_QUEUE;
+        if (branch == kBranchPushSmall) {
+            k_push_edge_q<<<ctx.num_sms * kSmallPushPerSm, kPushThreads, 0, s>>>(a);
+            MB_CHECK_LAUNCH();
+            return;
+        }
         if (branch == kBranchTail) {
             k_tail<<<1, kTailThreads, 0, s>>>(a, sp.cap);
             MB_CHECK_LAUNCH();

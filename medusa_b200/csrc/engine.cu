@@ -26,6 +26,10 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
                         ? (uint32_t)std::min<int64_t>(ctx.tunable[MB_TUNE_TAIL_EDGES], kTailEdges)
                         : kTailEdges;
     p->wait_polls = ctx.tunable[MB_TUNE_WAIT_POLLS] >= 0 ? ctx.tunable[MB_TUNE_WAIT_POLLS] : -1;
+    p->small_push_max = (uint32_t)std::min<int64_t>(
+        ctx.tunable[MB_TUNE_SMALL_PUSH_EDGES] >= 0 ? ctx.tunable[MB_TUNE_SMALL_PUSH_EDGES]
+                                                   : (int64_t)ctx.num_sms * kSmallPushPerSm * kTile,
+        0xffffffffll);
     for (int i = 0; i < p->nreplay; i++) p->replay[i] = ctx.replay[i];
     const size_t bytes = offsetof(RunParams, replay) + (size_t)p->nreplay;
     MB_CUDA(cudaMemcpyAsync(ctrl_dev, p, bytes, cudaMemcpyHostToDevice, ctx.stream));

@@ -38,7 +38,12 @@ constexpr int kBranchPersist = kBranchTail + 1;
 // a next-frontier bitmap with fire-and-forget atomics (no per-vertex claim
 // round trip), and a compaction pass turns the bitmap into the next queue.
 constexpr int kBranchPushBm = kBranchPersist + 1;
-constexpr int kNumBranches = kBranchPushBm + 1;
+// Schedule 0 on a medium queue frontier (above the tail's limits, at most
+// p.small_push_max out-edges): the same push on a grid of two CTAs per SM,
+// which dispatches and retires faster than the full grid.
+constexpr int kBranchPushSmall = kBranchPushBm + 1;
+constexpr int kNumBranches = kBranchPushSmall + 1;
+constexpr int kSmallPushPerSm = 2;  // CTAs per SM of the small-grid push
 constexpr int kTailThreads = 1024;
 constexpr uint32_t kTailEntries = 2048, kTailEdges = 8192;
 // The SSSP tail keeps its frontier in shared memory: room for kSTailCap
@@ -154,6 +159,8 @@ __device__ inline int route(const Ctrl *c, int s) {
     if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.bm_push_min &&
         c->front_m >= c->p.bm_push_min)
         return kBranchPushBm;
+    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->front_m <= c->p.small_push_max)
+        return kBranchPushSmall;
     return branch_of(s, c->mode);
 }
 
@@ -269,15 +276,44 @@ __device__ inline void finish_superstep(Ctrl *c, int app, int32_t V, int64_t E, 
 // memory only).  Called by every thread of the CTA.
 static_assert(sizeof(Ctrl) % 8 == 0, "control block copied in 8-byte words");
 static_assert(offsetof(Ctrl, q) % 8 == 0, "the select kernel writes back from q on, in 8-byte words");
+// The replay list (4 KB of the run parameters) is copied only for the
+// replay policy, and every thread issues all of its loads before its stores:
+// one L2 round trip per pass instead of one per word.
+static_assert(offsetof(Ctrl, p) == 0 && offsetof(RunParams, replay) % 8 == 0 && kMaxReplay % 8 == 0,
+              "the replay list is skipped in 8-byte words");
+constexpr int kCtrlWords = (int)(sizeof(Ctrl) / 8);
+constexpr int kReplayW0 = (int)(offsetof(RunParams, replay) / 8);
+constexpr int kReplayW1 = kReplayW0 + kMaxReplay / 8;
+constexpr int kHotWords = kReplayW0 + (kCtrlWords - kReplayW1);  // words outside the replay list
+__device__ __forceinline__ int hot_word(int i) { return i < kReplayW0 ? i : i - kReplayW0 + kReplayW1; }
 __device__ inline void ctrl_shadow_in(Ctrl *s, const Ctrl *g) {
-    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x)
-        reinterpret_cast<unsigned long long *>(s)[i] = reinterpret_cast<const unsigned long long *>(g)[i];
+    const auto *gw = reinterpret_cast<const unsigned long long *>(g);
+    auto *sw = reinterpret_cast<unsigned long long *>(s);
+    for (int base = 0; base < kHotWords; base += 4 * (int)blockDim.x) {
+        unsigned long long v[4];
+        int w[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = base + r * (int)blockDim.x + (int)threadIdx.x;
+            w[r] = i < kHotWords ? hot_word(i) : -1;
+            v[r] = w[r] >= 0 ? __ldcg(&gw[w[r]]) : 0ull;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            if (w[r] >= 0) sw[w[r]] = v[r];
+    }
     __syncthreads();
+    if (s->p.policy == MB_POLICY_ORACLE_BEST) {
+        for (int i = kReplayW0 + (int)threadIdx.x; i < kReplayW1; i += (int)blockDim.x) sw[i] = __ldcg(&gw[i]);
+        __syncthreads();
+    }
 }
 __device__ inline void ctrl_shadow_out(Ctrl *g, const Ctrl *s) {
     __syncthreads();
-    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x)
-        reinterpret_cast<unsigned long long *>(g)[i] = reinterpret_cast<const unsigned long long *>(s)[i];
+    for (int i = threadIdx.x; i < kHotWords; i += blockDim.x) {
+        const int w = hot_word(i);
+        reinterpret_cast<unsigned long long *>(g)[w] = reinterpret_cast<const unsigned long long *>(s)[w];
+    }
     __threadfence();
 }
 

@@ -33,6 +33,8 @@ struct RunParams {
     int32_t bfs_beta;           // BFS fixed rule: back to top-down below V / beta frontier vertices
     int32_t bfs_gamma;          // BFS fixed rule: bottom-up only from E / gamma frontier out-edges (0: any)
     int64_t wait_polls;         // polls before a bounded device wait gives up (-1: each wait's default)
+    uint32_t small_push_max;    // schedule 0 frontiers up to this many out-edges use the small grid
+    uint32_t pad_;
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 

@@ -105,6 +105,11 @@ struct PushSmem {
 #ifndef MB_SSSP_MATCH
 #define MB_SSSP_MATCH 0
 #endif
+// 128-bit col/wt loads in the edge-balanced push (needs 4 edges per thread:
+// MB_TILE_EDGES=1024).  Measured against the scalar loads; off.
+#ifndef MB_PUSH_VEC4
+#define MB_PUSH_VEC4 0
+#endif
 
 // kBmOut: instead of claiming each improved vertex (an atomic with a
 // result) and appending it to the next queue, set its bit in a.nbm with a
@@ -190,6 +195,26 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
         {
             const uint32_t e0 = c0 + threadIdx.x * kTileItems;
             int j = e0 < c1 ? upper_bound_minus1(s_off, k, e0) : 0;
+#if MB_PUSH_VEC4
+            // 128-bit loads of col and wt where the thread's 4 edges lie in one
+            // vertex's list and start on a 16-byte boundary; scalar elsewhere
+            static_assert(kTileItems == 4, "MB_PUSH_VEC4 needs 4 edges per thread");
+            bool vec_done = false;
+            if (e0 + 3 < c1 && (j + 1 >= k || s_off[j + 1] > e0 + 3)) {
+                const int32_t e = s_row[j] + (int32_t)(e0 - s_off[j]);
+                if ((e & 3) == 0) {
+                    const int4 c4 = __ldg(reinterpret_cast<const int4 *>(a.col + e));
+                    const float4 w4 = __ldg(reinterpret_cast<const float4 *>(a.wt + e));
+                    const float du = s_du[j];
+                    v[0] = c4.x; v[1] = c4.y; v[2] = c4.z; v[3] = c4.w;
+                    nd[0] = du + w4.x; nd[1] = du + w4.y; nd[2] = du + w4.z; nd[3] = du + w4.w;
+#pragma unroll
+                    for (int r = 0; r < 4; r++) ok[r] = true;
+                    vec_done = true;
+                }
+            }
+            if (!vec_done)
+#endif
 #pragma unroll
             for (int r = 0; r < kTileItems; r++) {
                 const uint32_t e_idx = e0 + r;
@@ -1105,6 +1130,13 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         }
         if (branch == kBranchPersist) {
             launch_cooperative((const void *)k_persist, persist_grid, kPushThreads, s, a, sp.cap);
+            return;
+        }
+        if (branch == kBranchPushSmall) {
+            const int grid_small = ctx.num_sms * kSmallPushPerSm;
+            if (bulk) k_push_edge_q<true><<<grid_small, kPushThreads, 0, s>>>(a);
+            else k_push_edge_q<false><<<grid_small, kPushThreads, 0, s>>>(a);
+            MB_CHECK_LAUNCH();
             return;
         }
         if (branch == kBranchPushBm) {
