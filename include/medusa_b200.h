@@ -341,7 +341,10 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                       persistent tail's limits) runs on a grid of two CTAs
                                       per SM instead of the full push grid (default
                                       2 x SMs x 512; 0: never) */
-#define MB_NUM_TUNABLES 16
+#define MB_TUNE_PR_HUB_CTAS 16 /* PageRank in the reference's order: CTAs of the scans of
+                                 the hubs above 16384 in-edges, which run beside the other
+                                 kernels (default SMs / 4) */
+#define MB_NUM_TUNABLES 17
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

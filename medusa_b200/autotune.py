@@ -106,6 +106,7 @@ def tune_pagerank(ctx, g, iters=10, reps=3, out=None):
     space = {"pr_light_vpl": [-1, 1, 2, 4]}
     if getattr(ctx, "pr_order", api.MB_PR_ORDER_REFERENCE) == api.MB_PR_ORDER_REFERENCE:
         space["pr_hub_min"] = [-1, 256, 512, 1024, 4096]
+        space["pr_hub_ctas"] = [-1, 148, 592]
     else:
         space["pr_short_pair"] = [-1, 1, 2]
     return tune(ctx, lambda: g.pagerank(iters, 1.0 / g.V, out=out)[1], space, reps)

@@ -314,8 +314,10 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
 //     per group; row j of a group holds slot j of each of its vertices, so a
 //     warp reads a row with one coalesced load and lane l folds its own
 //     vertex in order (k_pr_sell);
-//   n > hub_min: one CTA per vertex, the parallel integer scan of
-//     pr_order.cuh (k_pr_hub_exact), run on a side stream beside the others.
+//   n > hub_min: the contributions staged by every SM into one contiguous run
+//     per vertex (k_pr_hub_stage), then one CTA per vertex runs the parallel
+//     integer scan of pr_order.cuh over it (k_pr_hub_exact), on a side
+//     stream beside the others.
 constexpr int kSellU = 16;                      // rows of a group in flight
 constexpr int kHubK = 16;                       // consecutive slots per thread
 constexpr int kHubBig = 16384;                  // in-degree above which a hub gets the big CTA
@@ -332,19 +334,16 @@ struct ExactArgs {
     int32_t ngroups;
     const int32_t *hub_v;        // hubs, largest in-degree first
     int32_t nhub;
+    float *x_stage;              // every hub's contributions, in MEG slot order
+    const int64_t *stage_off;    // where hub h's run starts (16-byte aligned)
+    const int4 *stage_items;     // staging work: {stage offset, meg_src offset, length, 0}
+    int32_t nstage_items;
 };
 
 __device__ __forceinline__ void x_write(const ExactArgs &a, int32_t v, float sum, int32_t d) {
     const float r = pr_update(sum);
     a.rank_out[v] = r;
     a.contrib_out[v] = d > 0 ? r / (float)d : 0.0f;
-}
-
-__device__ __forceinline__ int4 ld_stream4(const int4 *p) {
-    int4 v;
-    asm("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
-    return v;
 }
 
 // Sliced ELL: one warp per group, kSellU rows (coalesced index loads, then
@@ -382,60 +381,80 @@ __global__ void __launch_bounds__(256) k_pr_sell(ExactArgs a) {
     }
 }
 
-// The kHubK slot sources of thread `tid`'s part of the chunk at `pos`
-// (-1 past the vertex's end).  src + pos is 16-byte aligned.
-template <int kT>
-__device__ __forceinline__ void hub_idx(const int32_t *src, int32_t n, int32_t pos, int32_t (&idx)[kHubK]) {
-    const int32_t j0 = pos + (int32_t)threadIdx.x * kHubK;
-    if (j0 + kHubK <= n) {
-        const int4 *p4 = reinterpret_cast<const int4 *>(src + j0);
+// Staging: every hub's contributions gathered, in MEG slot order, into one
+// contiguous run per hub (x_stage), by all SMs at once: one warp per item of
+// at most kStageItem slots, kStageU loads of each lane in flight.  The
+// scans below then read coalesced data instead of each hub's CTA gathering
+// at one SM's rate.
+constexpr int kStageItem = 4096;
+constexpr int kStageU = 8;
+__global__ void __launch_bounds__(256) k_pr_hub_stage(ExactArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t it = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < a.nstage_items; it += warps) {
+        const int4 item = __ldg(&a.stage_items[it]);
+        float *dst = a.x_stage + (uint32_t)item.x;
+        const int32_t *src = a.meg_src + (uint32_t)item.y;
+        for (int32_t k0 = 0; k0 < item.z; k0 += 32 * kStageU) {
+            float x[kStageU];
 #pragma unroll
-        for (int r = 0; r < kHubK / 4; r++) {
-            const int4 t4 = ld_stream4(p4 + r);
-            idx[4 * r] = t4.x;
-            idx[4 * r + 1] = t4.y;
-            idx[4 * r + 2] = t4.z;
-            idx[4 * r + 3] = t4.w;
+            for (int u = 0; u < kStageU; u++) {
+                const int32_t k = k0 + 32 * u + lane;
+                x[u] = k < item.z ? ld_gather(&a.contrib_in[ld_stream(src + k)]) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kStageU; u++) {
+                const int32_t k = k0 + 32 * u + lane;
+                if (k < item.z) dst[k] = x[u];
+            }
         }
-    } else {
-#pragma unroll
-        for (int k = 0; k < kHubK; k++) idx[k] = j0 + k < n ? ld_stream(src + j0 + k) : -1;
     }
 }
 
-__device__ __forceinline__ void hub_gather(const ExactArgs &a, const int32_t (&idx)[kHubK], float (&x)[kHubK]) {
+// Scan thread t's kHubK consecutive staged values of the chunk at `pos`
+// (0 past the vertex's end).  run + pos is 16-byte aligned.
+__device__ __forceinline__ void hub_load(const float *run, int32_t n, int32_t pos, int t, float (&x)[kHubK]) {
+    const int32_t j0 = pos + t * kHubK;
+    if (j0 + kHubK <= n) {
+        const float4 *p4 = reinterpret_cast<const float4 *>(run + j0);
 #pragma unroll
-    for (int k = 0; k < kHubK; k++) x[k] = idx[k] >= 0 ? ld_gather(&a.contrib_in[idx[k]]) : 0.f;
+        for (int r = 0; r < kHubK / 4; r++) {
+            const float4 t4 = __ldcs(p4 + r);
+            x[4 * r] = t4.x;
+            x[4 * r + 1] = t4.y;
+            x[4 * r + 2] = t4.z;
+            x[4 * r + 3] = t4.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kHubK; k++) x[k] = j0 + k < n ? __ldcs(run + j0 + k) : 0.f;
+    }
 }
 
-// Hubs [h0, h1) of the list: one CTA of kT threads per vertex.  The first
-// kHead slots (plus up to 3, so the rest starts on a 16-byte boundary) are
-// gathered by every thread and folded by thread 0; then chunks of kT * kHubK
-// slots, thread t owning kHubK consecutive ones, go through the integer
-// scan of pr_order.cuh.  The loads run ahead of the scans: each chunk's
-// sources load two chunks early and its contributions one chunk early.
+// Hubs [h0, h1) of the list: one CTA of kT threads per vertex, over its
+// staged run.  The first kHead values are folded by thread 0 (a multiple of
+// 4, so the chunks that follow start 16-byte aligned); then chunks of
+// kT * kHubK values, thread t owning kHubK consecutive ones, go through the
+// integer scan of pr_order.cuh.  Each chunk's loads are issued one chunk
+// ahead of its scan.
 template <int kT, int kHead>
 __global__ void __launch_bounds__(kT) k_pr_hub_exact(ExactArgs a, int32_t h0, int32_t h1) {
+    static_assert(kHead % 4 == 0, "chunks start 16-byte aligned");
     constexpr int kW = kT / 32;
     constexpr int kChunk = kT * kHubK;
-    __shared__ __align__(16) float head[kHead + 4];
+    __shared__ __align__(16) float head[kHead];
     __shared__ uint32_t wtot[kW];
     __shared__ int32_t wbad[kW];
     __shared__ float s_sh;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int32_t h = h0 + blockIdx.x; h < h1; h += gridDim.x) {
         const int32_t v = __ldg(&a.hub_v[h]);
-        const int64_t b = __ldg(&a.rrow[v]);
-        const int32_t n = (int32_t)(__ldg(&a.rrow[v + 1]) - b);
-        const int32_t *src = a.meg_src + b;
-        const int32_t H = min(n, kHead + (int32_t)((4 - ((b + kHead) & 3)) & 3));
-        for (int i = tid; i < H; i += kT) head[i] = ld_gather(&a.contrib_in[ld_stream(src + i)]);
-        // the first two chunks' loads go out before the head is folded
-        int32_t idx[kHubK];
+        const int32_t n = __ldg(&a.rrow[v + 1]) - __ldg(&a.rrow[v]);
+        const float *run = a.x_stage + __ldg(&a.stage_off[h]);
+        const int32_t H = min(n, kHead);
+        for (int i = tid; i < H; i += kT) head[i] = __ldcs(run + i);
         float x[kHubK], xn[kHubK];
-        hub_idx<kT>(src, n, H, idx);
-        hub_gather(a, idx, xn);
-        hub_idx<kT>(src, n, H + kChunk, idx);
+        hub_load(run, n, H, tid, xn);  // the first chunk's loads go out before the head is folded
         __syncthreads();
         if (tid == 0) {  // the adds chain; the shared loads run ahead, 4 at a time
             float s0 = 0.f;
@@ -457,10 +476,7 @@ __global__ void __launch_bounds__(kT) k_pr_hub_exact(ExactArgs a, int32_t h0, in
         for (int32_t pos = H; pos < n; pos += kChunk) {
 #pragma unroll
             for (int k = 0; k < kHubK; k++) x[k] = xn[k];
-            if (pos + kChunk < n) {
-                hub_gather(a, idx, xn);                       // chunk pos + kChunk
-                hub_idx<kT>(src, n, pos + 2 * kChunk, idx);   // chunk pos + 2 kChunk
-            }
+            if (pos + kChunk < n) hub_load(run, n, pos + kChunk, tid, xn);
             int start = 0;  // threads before it have folded their slots
             for (;;) {
                 const uint32_t bits = __float_as_uint(s);
@@ -481,32 +497,22 @@ __global__ void __launch_bounds__(kT) k_pr_hub_exact(ExactArgs a, int32_t h0, in
                     const uint32_t y = __shfl_up_sync(0xffffffffu, I, off);
                     if (lane >= off) I += y;
                 }
-                if (kW > 1) {
-                    if (lane == 31) wtot[wid] = I;
-                    __syncthreads();
-                }
-                uint32_t total = __shfl_sync(0xffffffffu, I, 31);
-                if (kW > 1) {
-                    total = 0;
+                if (lane == 31) wtot[wid] = I;
+                __syncthreads();
+                uint32_t total = 0;
 #pragma unroll
-                    for (int w = 0; w < kW; w++) {
-                        const uint32_t t = wtot[w];
-                        if (w < wid) I += t;
-                        total += t;
-                    }
+                for (int w = 0; w < kW; w++) {
+                    const uint32_t t = wtot[w];
+                    if (w < wid) I += t;
+                    total += t;
                 }
                 const bool bad = tid >= start && (ks == 0 || ks == 255 || tie || base + I >= (1u << 24));
                 const unsigned bm = __ballot_sync(0xffffffffu, bad);
-                int c;
-                if (kW > 1) {
-                    if (lane == 0) wbad[wid] = bm ? wid * 32 + __ffs(bm) - 1 : kT;
-                    __syncthreads();
-                    c = kT;
+                if (lane == 0) wbad[wid] = bm ? wid * 32 + __ffs(bm) - 1 : kT;
+                __syncthreads();
+                int c = kT;
 #pragma unroll
-                    for (int w = 0; w < kW; w++) c = min(c, wbad[w]);
-                } else {
-                    c = bm ? __ffs(bm) - 1 : kT;
-                }
+                for (int w = 0; w < kW; w++) c = min(c, wbad[w]);
                 if (c == kT) {  // the whole chunk stayed in the binade
                     s = pr_make(ks, base + total);
                     break;
@@ -521,11 +527,75 @@ __global__ void __launch_bounds__(kT) k_pr_hub_exact(ExactArgs a, int32_t h0, in
                 s = s_sh;
                 start = c + 1;
                 if (start >= kT) break;
-                if (kW == 1) __syncthreads();  // s_sh is written again before the next read
             }
         }
         if (tid == 0) x_write(a, v, s, __ldg(&a.outdeg[v]));
         __syncthreads();  // head and s_sh are reused by the next hub
+    }
+}
+
+// Hubs [h0, h1) of the list: one WARP per vertex over its staged run --
+// the integer scan of pr_order.cuh with shuffles only (no CTA barrier), so
+// a SM keeps dozens of hubs in flight.  Every lane first folds the first
+// kWarpHead values itself (each value broadcast by a shuffle, the same adds
+// in every lane); then chunks of 32 * kHubK values, lane l owning kHubK
+// consecutive ones, loaded one chunk ahead of their scan.
+constexpr int kWarpHead = 64;
+__global__ void __launch_bounds__(256) k_pr_hub_warp(ExactArgs a, int32_t h0, int32_t h1) {
+    constexpr int kChunk = 32 * kHubK;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t h = h0 + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); h < h1; h += warps) {
+        const int32_t v = __ldg(&a.hub_v[h]);
+        const int32_t n = __ldg(&a.rrow[v + 1]) - __ldg(&a.rrow[v]);
+        const float *run = a.x_stage + __ldg(&a.stage_off[h]);
+        const int32_t H = min(n, kWarpHead);
+        const float h_lo = lane < H ? __ldcs(run + lane) : 0.f;
+        const float h_hi = lane + 32 < H ? __ldcs(run + lane + 32) : 0.f;
+        float x[kHubK], xn[kHubK];
+        hub_load(run, n, H, lane, xn);  // the first chunk's loads go out before the head is folded
+        float s = 0.f;
+        for (int i = 0; i < H; i++) s += __shfl_sync(0xffffffffu, i < 32 ? h_lo : h_hi, i & 31);
+        for (int32_t pos = H; pos < n; pos += kChunk) {
+#pragma unroll
+            for (int k = 0; k < kHubK; k++) x[k] = xn[k];
+            if (pos + kChunk < n) hub_load(run, n, pos + kChunk, lane, xn);
+            int start = 0;  // lanes before it have folded their values
+            for (;;) {
+                const uint32_t bits = __float_as_uint(s);
+                const uint32_t ks = bits >> 23, base = (bits & 0x7fffffu) | 0x800000u;
+                uint32_t L = 0;
+                bool tie = false;
+                if (lane >= start) {
+#pragma unroll
+                    for (int k = 0; k < kHubK; k++) L += pr_units(x[k], ks, tie);
+                    L = min(L, 1u << 23);
+                }
+                uint32_t I = L;  // inclusive prefix (< 2^28: 32 lanes of at most 2^23)
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, I, off);
+                    if (lane >= off) I += y;
+                }
+                const uint32_t total = __shfl_sync(0xffffffffu, I, 31);
+                const bool bad = lane >= start && (ks == 0 || ks == 255 || tie || base + I >= (1u << 24));
+                const unsigned bm = __ballot_sync(0xffffffffu, bad);
+                if (!bm) {  // the whole chunk stayed in the binade
+                    s = pr_make(ks, base + total);
+                    break;
+                }
+                const int c = __ffs(bm) - 1;
+                float s2 = c == start ? s : pr_make(ks, base + I - L);
+                if (lane == c) {  // the float path from the exact running sum
+#pragma unroll
+                    for (int k = 0; k < kHubK; k++) s2 += x[k];
+                }
+                s = __shfl_sync(0xffffffffu, s2, c);
+                start = c + 1;
+                if (start >= 32) break;
+            }
+        }
+        if (lane == 0) x_write(a, v, s, __ldg(&a.outdeg[v]));
     }
 }
 
@@ -838,6 +908,25 @@ void PrState::ensure_exact(Context &ctx, const Graph &g, int32_t hub_min) {
     if (x_nhub) copy_sync(s, x_hub_v.p, hubs.data(), 4 * hubs.size());
     x_nbig = 0;  // the hubs are sorted: the big ones come first
     while (x_nbig < x_nhub && rrow[hubs[x_nbig] + 1] - rrow[hubs[x_nbig]] > kHubBig) x_nbig++;
+    // staging: hub h's run at a multiple of 4 floats, items of kStageItem slots
+    std::vector<int64_t> soff((size_t)std::max<int32_t>(x_nhub, 1), 0);
+    std::vector<int4> items;
+    int64_t staged = 0;
+    for (int32_t h = 0; h < x_nhub; h++) {
+        const int32_t v = hubs[h];
+        const int32_t n = rrow[v + 1] - rrow[v];
+        soff[h] = staged;
+        for (int32_t j0 = 0; j0 < n; j0 += kStageItem)
+            items.push_back(make_int4((int32_t)(staged + j0), rrow[v] + j0, std::min(kStageItem, n - j0), 0));
+        staged += ((int64_t)n + 3) & ~(int64_t)3;
+    }
+    if (staged > 0x7fffffffll) fail(MB_ERR_UNSUPPORTED, "PageRank: hub staging exceeds 2^31 slots");
+    nstage_items = (int32_t)items.size();
+    x_stage.reserve(sizeof(float) * (size_t)std::max<int64_t>(staged, 1));
+    stage_off.reserve(sizeof(int64_t) * soff.size());
+    stage_items.reserve(sizeof(int4) * std::max<size_t>(items.size(), 1));
+    copy_sync(s, stage_off.p, soff.data(), 8 * soff.size());
+    if (nstage_items) copy_sync(s, stage_items.p, items.data(), sizeof(int4) * items.size());
     MB_CUDA(cudaStreamSynchronize(s));
     if (!side) MB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     if (!ev_fork) MB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -925,8 +1014,11 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     };
     const int grid_vtx = ctx.num_sms * 8;
     const int grid_sell = resident((const void *)k_pr_sell, 256);
-    const int grid_hub_small = resident((const void *)k_pr_hub_exact<128, 256>, 128);
-    const int grid_hub_big = resident((const void *)k_pr_hub_exact<512, 512>, 512);
+    const int hub_ctas = ctx.tunable[MB_TUNE_PR_HUB_CTAS] > 0 ? (int)ctx.tunable[MB_TUNE_PR_HUB_CTAS]
+                                                               : std::max(ctx.num_sms / 4, 1);
+    const int grid_hub_warp = resident((const void *)k_pr_hub_warp, 256);
+    const int grid_stage = resident((const void *)k_pr_hub_stage, 256);
+    const int grid_hub_big = std::min(resident((const void *)k_pr_hub_exact<512, 512>, 512), hub_ctas);
     auto exact_args = [&](const PrArgs &a) {
         ExactArgs x;
         x.rrow = g.rrow.as<int32_t>();
@@ -942,6 +1034,10 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
         x.ngroups = st.ngroups;
         x.hub_v = st.x_hub_v.as<int32_t>();
         x.nhub = st.x_nhub;
+        x.x_stage = st.x_stage.as<float>();
+        x.stage_off = st.stage_off.as<int64_t>();
+        x.stage_items = st.stage_items.as<int4>();
+        x.nstage_items = st.nstage_items;
         return x;
     };
     auto emit = [&](cudaStream_t cs) {
@@ -962,17 +1058,24 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             }
             if (ref_order) {
                 ExactArgs x = exact_args(a);
-                // the big hubs (the longest chains of scans) on the side
-                // stream, beside the rest
+                // the hubs' contributions staged by every SM, then their
+                // scans on the side stream beside the rest
                 const int32_t nbig = st.x_nbig, nsmall = st.x_nhub - st.x_nbig;
-                if (nbig) {
+                if (st.x_nhub) {
+                    k_pr_hub_stage<<<grid_stage, 256, 0, cs>>>(x);
+                    MB_CHECK_LAUNCH();
                     MB_CUDA(cudaEventRecord(st.ev_fork, cs));
                     MB_CUDA(cudaStreamWaitEvent(st.side, st.ev_fork, 0));
-                    k_pr_hub_exact<512, 512><<<std::min(nbig, grid_hub_big), 512, 0, st.side>>>(x, 0, nbig);
+                    // the big hubs' CTA scans beside the rest, on few CTAs
+                    if (nbig)
+                        k_pr_hub_exact<512, 512><<<std::min(nbig, grid_hub_big), 512, 0, st.side>>>(x, 0, nbig);
                     MB_CHECK_LAUNCH();
                 }
-                if (nsmall)
-                    k_pr_hub_exact<128, 256><<<std::min(nsmall, grid_hub_small), 128, 0, cs>>>(x, nbig, st.x_nhub);
+                if (nsmall) {  // one warp per hub
+                    k_pr_hub_warp<<<grid_for((int64_t)nsmall * 32, 256, grid_hub_warp), 256, 0, cs>>>(
+                        x, nbig, st.x_nhub);
+                    MB_CHECK_LAUNCH();
+                }
                 if (st.ngroups) k_pr_sell<<<grid_sell, 256, 0, cs>>>(x);
                 if (st.x_nlight) {
                     PrArgs la = a;
@@ -983,7 +1086,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                     light(cs, la);
                 }
                 MB_CHECK_LAUNCH();
-                if (nbig) {
+                if (st.x_nhub) {
                     MB_CUDA(cudaEventRecord(st.ev_join, st.side));
                     MB_CUDA(cudaStreamWaitEvent(cs, st.ev_join, 0));
                 }
@@ -1057,7 +1160,8 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
             int64_t per_step;
             if (ref_order && unfused) per_step = 2;
             else if (ref_order)
-                per_step = (st.x_nbig > 0) + (st.x_nhub > st.x_nbig) + (st.ngroups > 0) + (st.x_nlight > 0);
+                per_step = (st.x_nhub > 0) + (st.x_nbig > 0) + (st.x_nhub > st.x_nbig) + (st.ngroups > 0) +
+                           (st.x_nlight > 0);
             else per_step = (unfused ? 2 : st.nlight > 0) + (st.nitems > 0) + (st.nhub > 0);
             stats->kernel_launches = 1 + (int64_t)iters * per_step + (iters == 0);
         }

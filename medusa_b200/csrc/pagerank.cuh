@@ -32,6 +32,8 @@ struct PrState {
     DevBuf x_hub_v;
     int32_t x_nhub = 0;
     int32_t x_nbig = 0;  // hubs [0, x_nbig) have more than kHubBig in-edges
+    DevBuf x_stage, stage_off, stage_items;  // the hubs' staged contributions
+    int32_t nstage_items = 0;
     // the hub kernel runs on a side stream beside the others (fork / join)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -63,6 +65,7 @@ struct PrState {
         x_light_v.release(); x_light_row.release(); x_light_col.release();
         sell_v.release(); sell_base.release(); sell_rows.release(); sell_src.release();
         x_hub_v.release();
+        x_stage.release(); stage_off.release(); stage_items.release();
         exact_built = false;
     }
     void ensure(Context &ctx, const Graph &g);

@@ -9,13 +9,19 @@ graph, SSSP from sources 0..31 in one batched traversal), c4a-msssp (R-MAT
 2^18 / 2^22, 10 supersteps), c5-bfs, c5-sssp (R-MAT 2^24 / 2^28,
 (0.57,0.19,0.19,0.05)), c5-pr (20 supersteps), c3-bfs, c3-sssp (1448^2
 grid), c5s-bfs, c5s-sssp, c5s-pr (the C5 generator at 2^21 / 2^25: a case
-small enough for full ncu captures).  Prints one line per repetition with
+small enough for full ncu captures), path-bfs, path-sssp (a directed path
+of 200 vertices, persistent tail off: every superstep is one select kernel
+and one push over a one-vertex frontier -- the fixed cost of a superstep).
+--pr-order fixed|reference picks PageRank's summation order (default: the
+library's, the reference's).  Prints one line per repetition with
 the library's device time.  --hostloop runs the host-driven loop (kernels in
 conditional-node graphs are invisible to ncu); --trace prints each superstep
 of the last repetition (BFS 8 B per frontier out-edge + 20 B per frontier
 vertex, SSSP 12 + 20, as algorithmic bytes)."""
 import argparse
 import sys
+
+import numpy as np
 
 from . import api
 
@@ -45,11 +51,21 @@ def main(argv=None):
     ap.add_argument("--hostloop", action="store_true")
     ap.add_argument("--trace", action="store_true",
                     help="print every superstep (branch, frontier, CUDA-event ms) of the last rep")
+    ap.add_argument("--pr-order", choices=["fixed", "reference"], default=None)
     args = ap.parse_args(argv)
     ctx = api.Context(0)
     if args.hostloop:
         ctx.set_graph_capture(False)
-    g = ctx.generate(params(args.case))
+    if args.pr_order:
+        ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED if args.pr_order == "fixed"
+                               else api.MB_PR_ORDER_REFERENCE)
+    if args.case.startswith("path"):
+        n = 200
+        src = np.arange(n - 1, dtype=np.int32)
+        g = ctx.graph_from_edges(n, src, src + 1, np.ones(n - 1, np.float32))
+        ctx.set_persistent_tail(False)
+    else:
+        g = ctx.generate(params(args.case))
     kind = args.case.split("-")[1]
     for i in range(args.reps):
         if args.trace and i == args.reps - 1:
