@@ -200,6 +200,26 @@ int mb_pagerank(mb_ctx *ctx, const mb_graph *g, int32_t iters, float init,
  * loop of single supersteps gives the same bits as one call of many. */
 int mb_pagerank_from(mb_ctx *ctx, const mb_graph *g, int32_t iters, const float *init_ranks,
                      float *rank_out, mb_stats *stats);
+/* One BSP superstep of a built-in app, for a host that drives the loop
+ * itself as the reference's main.cu does (ResetToExecute; Medusa_Exec;
+ * exe = RetriveToExecute; super_step++: SSSP/main.cu:369-382,
+ * Algorithm/main.cu:284-300, MPG/main.cu:148-169).  app: MB_APP_BFS,
+ * MB_APP_SSSP or MB_APP_PAGERANK.  step 0 starts a run (BFS/SSSP from
+ * `source`; PageRank from 1/V) and runs its first superstep; each later call
+ * runs the next one.  schedule: -1 for the context's policy, else that
+ * schedule for this superstep (PageRank: 0 or 6).  *continue_out = 1 while
+ * the traversal needs another superstep (PageRank: always 1; the host stops
+ * it).  mb_superstep_result then copies the levels (int32), distances or
+ * ranks (float) into out[V] (host or device) with the run's statistics and
+ * ends the run.  A stepped run holds the graph's state of that app: any
+ * whole-run call on the graph (mb_bfs, ...) ends it.  Results are those of
+ * the whole-run calls bit for bit, whatever schedules are forced. */
+#define MB_APP_BFS 0
+#define MB_APP_SSSP 1
+#define MB_APP_PAGERANK 2
+int mb_superstep(mb_ctx *ctx, const mb_graph *g, int32_t app, int32_t step, int32_t source,
+                 int32_t schedule, int32_t *continue_out);
+int mb_superstep_result(mb_ctx *ctx, const mb_graph *g, int32_t app, void *out, mb_stats *stats);
 /* PageRank summation order.
  * MB_PR_ORDER_REFERENCE (default): the reference's own MEG layout (vertices
  * sorted by out-degree with std::sort, column-major edge slots,

@@ -103,6 +103,8 @@ def _load():
         "mb_pagerank": (ctypes.c_int, [P, P, I32, F32, P, ctypes.POINTER(Stats)]),
         "mb_pagerank_noalloc": (ctypes.c_int, [P, P, P, I32, I64, I32, F32, P, P]),
         "mb_pagerank_from": (ctypes.c_int, [P, P, I32, P, P, ctypes.POINTER(Stats)]),
+        "mb_superstep": (ctypes.c_int, [P, P, I32, I32, I32, I32, ctypes.POINTER(I32)]),
+        "mb_superstep_result": (ctypes.c_int, [P, P, I32, P, ctypes.POINTER(Stats)]),
         "mb_scheduler_collect": (ctypes.c_int, [P, P, I32, I32, P, P, P, I32, ctypes.POINTER(I32)]),
         "mb_scheduler_train": (ctypes.c_int, [P, I32, P, P, I32, I32, F32, ctypes.c_uint64,
                                               ctypes.POINTER(F32)]),
@@ -300,6 +302,30 @@ def _pagerank_from(self, iters, init_ranks, out=None):
 
 
 Graph.pagerank_from = _pagerank_from
+
+MB_APP_BFS, MB_APP_SSSP, MB_APP_PAGERANK = 0, 1, 2
+
+
+def _superstep(self, app, step, source=0, schedule=-1):
+    """One superstep of a stepped run (mb_superstep): True while another is needed."""
+    cont = ctypes.c_int32(0)
+    _check(lib.mb_superstep(self.ctx.h, self.h, int(app), int(step), int(source), int(schedule),
+                            ctypes.byref(cont)), self.ctx.h)
+    return bool(cont.value)
+
+
+def _superstep_result(self, app, out=None):
+    """The stepped run's levels / distances / ranks and statistics; ends the run."""
+    if out is None:
+        out = np.empty(self.V, np.int32 if app == MB_APP_BFS else np.float32)
+    st = Stats()
+    _check(lib.mb_superstep_result(self.ctx.h, self.h, int(app), _ptr(out), ctypes.byref(st)),
+           self.ctx.h)
+    return out, st.as_dict()
+
+
+Graph.superstep = _superstep
+Graph.superstep_result = _superstep_result
 
 
 class Batch:

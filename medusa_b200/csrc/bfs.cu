@@ -543,7 +543,8 @@ __global__ void k_bfs_init(BfsArgs a) {
 // ---------------------------------------------------------------------------
 // host side
 
-void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats) {
+void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats, int phase, int force,
+             int *cont) {
     st.ensure(g);
     BfsArgs a;
     a.f = st.frontier_args(g, ctx.model(MB_MODEL_BFS));
@@ -554,7 +555,7 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
     a.rcol = g.rcol.as<int32_t>();
     a.level = st.level.as<int32_t>();
     a.vis = st.vis.as<uint32_t>();
-    upload_params(ctx, st.ctrl.p, source);
+    if (phase == LOOP_ALL || phase == LOOP_BEGIN) upload_params(ctx, st.ctrl.p, source);
 
     const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
@@ -621,7 +622,7 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
         MB_CHECK_LAUNCH();
     };
     sp.epilogue = nullptr;  // reached counts are kept by finish_superstep
-    run_loop(ctx, sp, stats);
+    run_loop(ctx, sp, stats, phase, force, cont);
 }
 
 }  // namespace mb

@@ -23,6 +23,9 @@ struct BfsState : FrontierState {
 };
 
 // One BFS from `source`; levels are left in st.level (device).
-void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats);
+// phase / force / cont: a run driven one superstep at a time (LoopPhase,
+// engine.cuh); the defaults run it whole.
+void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats, int phase = 0,
+             int force = -1, int *cont = nullptr);
 
 }  // namespace mb

@@ -21,6 +21,7 @@ struct AppStates {
     SsspState sssp;
     MsSsspState mssssp;
     PrState pr;
+    int stepped = -1;  // the app of the stepped run in progress (mb_superstep), or -1
 };
 int64_t generate_edges_host(const mb_gen_params &p, int32_t *src, int32_t *dst, float *w);
 void graph_generate(Context &ctx, Graph &g, const mb_gen_params &p, uint32_t flags);
@@ -648,6 +649,7 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
         if (nsrc < 1 || !sources || !levels_out) mb::fail(MB_ERR_INVALID, "bad sources/output");
         use_device(ctx);
         mb_graph *g = const_cast<mb_graph *>(gc);
+        apps(g).stepped = -1;  // a whole run ends any stepped one
         const int32_t V = g->g.V;
         std::vector<int32_t> src = fetch_i32(sources, nsrc);
         for (int32_t s : src)
@@ -705,6 +707,7 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
         if (nsrc < 1 || !sources || !dist_out) mb::fail(MB_ERR_INVALID, "bad sources/output");
         use_device(ctx);
         mb_graph *g = const_cast<mb_graph *>(gc);
+        apps(g).stepped = -1;  // a whole run ends any stepped one
         const int32_t V = g->g.V;
         std::vector<int32_t> src = fetch_i32(sources, nsrc);
         for (int32_t s : src)
@@ -763,12 +766,81 @@ int mb_pagerank(mb_ctx *ctx, const mb_graph *gc, int32_t iters, float init, floa
         if (iters < 0 || !rank_out) mb::fail(MB_ERR_INVALID, "bad iters/output");
         use_device(ctx);
         mb_graph *g = const_cast<mb_graph *>(gc);
+        apps(g).stepped = -1;  // a whole run ends any stepped one
         const int sched = ctx->c.schedule_policy == MB_POLICY_FORCED ? ctx->c.fixed_schedule
                                                                       : MB_SCHED_PUSH_EDGE_QUEUE;
         mb::run_pagerank(ctx->c, g->g, apps(g).pr, iters, init, sched, stats);
         MB_CUDA(cudaMemcpyAsync(rank_out, apps(g).pr.rank.p, sizeof(float) * (size_t)g->g.V,
                                 cudaMemcpyDefault, ctx->c.stream));
         MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int mb_superstep(mb_ctx *ctx, const mb_graph *gc, int32_t app, int32_t step, int32_t source,
+                 int32_t schedule, int32_t *continue_out) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (!continue_out || step < 0) mb::fail(MB_ERR_INVALID, "bad step/output");
+        if (schedule < -1 || schedule >= MB_NUM_SCHEDULES) mb::fail(MB_ERR_INVALID, "bad schedule");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        mb::AppStates &as = apps(g);
+        int cont = 0;
+        if (app == MB_APP_BFS || app == MB_APP_SSSP) {
+            if (step == 0 && (source < 0 || source >= g->g.V)) mb::fail(MB_ERR_INVALID, "source vertex out of range");
+            if (step > 0 && as.stepped != app) mb::fail(MB_ERR_INVALID, "no stepped run of this app in progress");
+            // step 0 starts the run and picks its first superstep, then runs it
+            if (step == 0) {
+                if (app == MB_APP_BFS) mb::run_bfs(ctx->c, g->g, as.bfs, source, nullptr, mb::LOOP_BEGIN, -1, &cont);
+                else mb::run_sssp(ctx->c, g->g, as.sssp, source, nullptr, mb::LOOP_BEGIN, -1, &cont);
+                as.stepped = app;
+            }
+            if (step == 0 && !cont) {
+                *continue_out = 0;
+                return;
+            }
+            if (app == MB_APP_BFS) mb::run_bfs(ctx->c, g->g, as.bfs, 0, nullptr, mb::LOOP_STEP, schedule, &cont);
+            else mb::run_sssp(ctx->c, g->g, as.sssp, 0, nullptr, mb::LOOP_STEP, schedule, &cont);
+        } else if (app == MB_APP_PAGERANK) {
+            if (schedule != -1 && schedule != MB_SCHED_PUSH_EDGE_QUEUE && schedule != MB_SCHED_PUSH_UNFUSED)
+                mb::fail(MB_ERR_INVALID, "PageRank schedules are 0 and 6");
+            if (step > 0 && as.stepped != app) mb::fail(MB_ERR_INVALID, "no stepped run of this app in progress");
+            const int sched = schedule == MB_SCHED_PUSH_UNFUSED ? MB_SCHED_PUSH_UNFUSED : MB_SCHED_PUSH_EDGE_QUEUE;
+            mb::PrState &pr = as.pr;
+            if (step == 0) mb::run_pagerank(ctx->c, g->g, pr, 1, 1.0f / (float)g->g.V, sched, nullptr);
+            else mb::run_pagerank(ctx->c, g->g, pr, 1, 0.f, sched, nullptr, pr.rank.as<float>());
+            as.stepped = app;
+            cont = 1;  // the host decides how many supersteps PageRank runs
+        } else {
+            mb::fail(MB_ERR_INVALID, "unknown app");
+        }
+        *continue_out = cont;
+    });
+}
+
+int mb_superstep_result(mb_ctx *ctx, const mb_graph *gc, int32_t app, void *out, mb_stats *stats) {
+    return guarded(ctx, [&] {
+        check_graph(ctx, gc);
+        if (!out) mb::fail(MB_ERR_INVALID, "null output");
+        use_device(ctx);
+        mb_graph *g = const_cast<mb_graph *>(gc);
+        mb::AppStates &as = apps(g);
+        if (as.stepped != app) mb::fail(MB_ERR_INVALID, "no stepped run of this app");
+        const size_t bytes = 4 * (size_t)g->g.V;
+        const void *src = nullptr;
+        if (app == MB_APP_BFS) {
+            mb::run_bfs(ctx->c, g->g, as.bfs, 0, stats, mb::LOOP_FINISH);
+            src = as.bfs.level.p;
+        } else if (app == MB_APP_SSSP) {
+            mb::run_sssp(ctx->c, g->g, as.sssp, 0, stats, mb::LOOP_FINISH);
+            src = as.sssp.dist.p;
+        } else {
+            src = as.pr.rank.p;
+            if (stats) *stats = mb_stats{};
+        }
+        MB_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDefault, ctx->c.stream));
+        MB_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        as.stepped = -1;
     });
 }
 
@@ -779,6 +851,7 @@ int mb_pagerank_from(mb_ctx *ctx, const mb_graph *gc, int32_t iters, const float
         if (iters < 0 || !rank_out || !init_ranks) mb::fail(MB_ERR_INVALID, "bad iters/input/output");
         use_device(ctx);
         mb_graph *g = const_cast<mb_graph *>(gc);
+        apps(g).stepped = -1;  // a whole run ends any stepped one
         const int sched = ctx->c.schedule_policy == MB_POLICY_FORCED ? ctx->c.fixed_schedule
                                                                       : MB_SCHED_PUSH_EDGE_QUEUE;
         // host ranks are staged into the PageRank state's own buffer, so a

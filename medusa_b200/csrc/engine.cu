@@ -42,7 +42,52 @@ int persistent_grid_size(const Context &ctx, const void *kernel, int threads) {
     return ctx.num_sms * std::min(per_sm, 4);
 }
 
-void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats) {
+// One superstep of a stepped run (see LoopPhase); the control block stays
+// on the device between calls.
+static void run_loop_phase(Context &ctx, LoopSpec &sp, mb_stats *stats, int phase, int force, int *cont) {
+    cudaStream_t s = ctx.stream;
+    const FrontierArgs &fa = sp.fa;
+    Ctrl *hc = (Ctrl *)ctx.ctrl_readback();
+    if (phase == LOOP_BEGIN) sp.prologue(s);
+    if (phase == LOOP_STEP) {
+        if (force >= 0) {
+            k_force_sched<<<1, 32, 0, s>>>(fa, force);
+            MB_CHECK_LAUNCH();
+        }
+        MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+        MB_CUDA(cudaStreamSynchronize(s));
+        if (hc->done) fail(MB_ERR_INVALID, std::string(sp.name) + ": no superstep left to run");
+        sp.branch(hc->branch, s);
+    }
+    if (phase == LOOP_BEGIN || phase == LOOP_STEP) {
+        k_select<<<1, 32, 0, s>>>(fa, sp.app, sp.cap, 0, 0, kNumBranches, 0);
+        MB_CHECK_LAUNCH();
+    }
+    if (phase == LOOP_FINISH && sp.epilogue) sp.epilogue(s);
+    MB_CUDA(cudaMemcpyAsync(hc, fa.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    if (cont) *cont = hc->done ? 0 : 1;
+    if (hc->err & ERR_STEP_CAP) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": superstep cap reached");
+    if (hc->err & ERR_BULK) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a bulk copy timed out");
+    if (hc->err & ERR_BARRIER)
+        fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a persistent-grid barrier timed out");
+    if (phase == LOOP_FINISH && stats) {
+        *stats = mb_stats{};
+        stats->supersteps = hc->supersteps;
+        stats->status_flags = hc->err;
+        stats->edges_traversed = (int64_t)hc->edges_reached;
+        stats->vertices_reached = (int64_t)hc->reached;
+        for (int i = 0; i < MB_NUM_SCHEDULES; i++) stats->schedule_count[i] = hc->sched_count[i];
+        stats->kernel_launches = hc->p.launches;
+        stats->edges_scanned = (int64_t)hc->work;
+    }
+}
+
+void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats, int phase, int force, int *cont) {
+    if (phase != LOOP_ALL) {
+        run_loop_phase(ctx, sp, stats, phase, force, cont);
+        return;
+    }
     cudaStream_t s = ctx.stream;
     const int nbranch = kNumBranches;
     FrontierState &st = *sp.st;

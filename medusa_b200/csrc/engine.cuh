@@ -87,8 +87,8 @@ struct Ctrl {
     uint32_t far_n[2];        // SSSP near-far: far-pile sizes
     int32_t fcur;             // far pile being filled
     int32_t splits;           // near-far split steps run
-    uint32_t bar_count;       // persistent-grid barrier: arrivals
-    uint32_t bar_gen;         // persistent-grid barrier: generation
+    uint32_t bar_count;       // persistent-grid barrier: arrivals over the run (top bit: gave up)
+    uint32_t bar_gen;         // unused
     int32_t persist_go;       // persistent grid: run another superstep
 };
 
@@ -426,6 +426,15 @@ __device__ inline void bookkeep_warp(const FrontierArgs &a, int app) {
     }
 }
 
+// A stepped run's next superstep with schedule s instead of the policy's.
+static __global__ void k_force_sched(FrontierArgs a, int s) {
+    Ctrl *c = a.ctrl;
+    if (threadIdx.x == 0 && !c->done) {
+        c->sched = s;
+        c->branch = route(c, s);
+    }
+}
+
 // Count one loop iteration; past the cap the run stops with an error, and
 // so does a run in which a bounded wait gave up.
 __device__ inline void count_iteration(Ctrl *c, int cap) {
@@ -477,36 +486,49 @@ static __global__ void k_select(FrontierArgs a, int app, int cap,
 }
 
 // Grid barrier of the persistent kernel (all blocks co-resident: cooperative
-// launch).  The wait is bounded: past kBarrierSpins polls (or the run's
-// wait_polls, when set) it records ERR_BARRIER and returns false, and the
+// launch).  bar_count counts arrivals over the whole run (zeroed by the
+// run's init kernel), so barrier k completes when it reaches k * gridDim.x:
+// one atomic per block, then polling of the same word with acquire loads
+// (which also drop this SM's stale L1 lines).  The wait is bounded: past
+// kBarrierSpins polls (or the run's wait_polls, when set) the block records
+// ERR_BARRIER, sets the counter's top bit -- every block still waiting, and
+// every later barrier, then fails at once -- and returns false, and the
 // caller leaves its loop.
 constexpr long kBarrierSpins = 1l << 22;
+constexpr unsigned kBarPoison = 1u << 31;
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ inline bool grid_sync(Ctrl *c) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned gen = ldg2(&c->bar_gen);
-        __threadfence();
+        __threadfence();  // this block's writes before its arrival
         const unsigned arrived = atomicAdd(&c->bar_count, 1u);
-        int ok = 1;
-        if (arrived == gridDim.x - 1) {
-            atomicExch(&c->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&c->bar_gen, 1u);
-        } else {
-            ok = 0;
+        int ok = 0;
+        if (arrived < kBarPoison) {
+            const unsigned target = (arrived / gridDim.x + 1) * gridDim.x;
             const long spins = c->p.wait_polls >= 0 ? (long)c->p.wait_polls : kBarrierSpins;
-            for (long it = 0; it < spins; it++) {
-                if (ldg2(&c->bar_gen) != gen) {
+            for (long it = 0;; it++) {
+                const unsigned v = ld_acquire_gpu(&c->bar_count);
+                if (v >= kBarPoison) break;  // another block gave up
+                if (v >= target) {
                     ok = 1;
                     break;
                 }
-                __nanosleep(32);
+                if (it >= spins) {
+                    atomicOr(&c->err, ERR_BARRIER);
+                    atomicOr(&c->bar_count, kBarPoison);
+                    break;
+                }
+                __nanosleep(16);
             }
-            if (!ok) atomicOr(&c->err, ERR_BARRIER);
         }
+        if (!ok) atomicOr(&c->err, ERR_BARRIER);
         __threadfence();
-        s_ok = ok && !(ldg2(&c->err) & ERR_BARRIER);
+        s_ok = ok;
     }
     __syncthreads();
     return s_ok;
@@ -680,7 +702,14 @@ struct LoopSpec {
     EmitFn epilogue;
     const char *name;
 };
-void run_loop(Context &ctx, LoopSpec &spec, mb_stats *stats);
+// The phases of a run driven one superstep at a time (mb_superstep): BEGIN
+// runs the prologue and picks the first superstep, STEP runs the picked one
+// (a schedule forced when force >= 0) and picks the next, FINISH runs the
+// epilogue and reads the statistics.  ALL is a whole run (one CUDA graph
+// launch, or the host-driven loop).  *cont: another superstep is needed.
+enum LoopPhase { LOOP_ALL = 0, LOOP_BEGIN = 1, LOOP_STEP = 2, LOOP_FINISH = 3 };
+void run_loop(Context &ctx, LoopSpec &spec, mb_stats *stats, int phase = LOOP_ALL, int force = -1,
+              int *cont = nullptr);
 
 // Blocks of the persistent kernel: every SM holds min(resident, 4) of them,
 // so a cooperative launch always fits.

@@ -318,7 +318,10 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
 //     per vertex (k_pr_hub_stage), then one CTA per vertex runs the parallel
 //     integer scan of pr_order.cuh over it (k_pr_hub_exact), on a side
 //     stream beside the others.
-constexpr int kSellU = 16;                      // rows of a group in flight
+#ifndef MB_SELL_U
+#define MB_SELL_U 16
+#endif
+constexpr int kSellU = MB_SELL_U;               // rows of a group in flight
 constexpr int kHubK = 16;                       // consecutive slots per thread
 constexpr int kHubBig = 16384;                  // in-degree above which a hub gets the big CTA
 constexpr int kHubMinDefault = 2048;
@@ -386,7 +389,10 @@ __global__ void __launch_bounds__(256) k_pr_sell(ExactArgs a) {
 // at most kStageItem slots, kStageU loads of each lane in flight.  The
 // scans below then read coalesced data instead of each hub's CTA gathering
 // at one SM's rate.
-constexpr int kStageItem = 4096;
+#ifndef MB_STAGE_ITEM
+#define MB_STAGE_ITEM 1024
+#endif
+constexpr int kStageItem = MB_STAGE_ITEM;
 constexpr int kStageU = 8;
 __global__ void __launch_bounds__(256) k_pr_hub_stage(ExactArgs a) {
     const int lane = threadIdx.x & 31;
@@ -1016,7 +1022,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
     const int grid_sell = resident((const void *)k_pr_sell, 256);
     const int hub_ctas = ctx.tunable[MB_TUNE_PR_HUB_CTAS] > 0 ? (int)ctx.tunable[MB_TUNE_PR_HUB_CTAS]
                                                                : std::max(ctx.num_sms / 4, 1);
-    const int grid_hub_warp = resident((const void *)k_pr_hub_warp, 256);
+    const int grid_hub_warp = std::max(resident((const void *)k_pr_hub_warp, 256) / 2, 1);
     const int grid_stage = resident((const void *)k_pr_hub_stage, 256);
     const int grid_hub_big = std::min(resident((const void *)k_pr_hub_exact<512, 512>, 512), hub_ctas);
     auto exact_args = [&](const PrArgs &a) {
@@ -1066,14 +1072,13 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                     MB_CHECK_LAUNCH();
                     MB_CUDA(cudaEventRecord(st.ev_fork, cs));
                     MB_CUDA(cudaStreamWaitEvent(st.side, st.ev_fork, 0));
-                    // the big hubs' CTA scans beside the rest, on few CTAs
+                    // the scans beside the rest: the big hubs one CTA each on
+                    // few CTAs, then the others one warp each
                     if (nbig)
                         k_pr_hub_exact<512, 512><<<std::min(nbig, grid_hub_big), 512, 0, st.side>>>(x, 0, nbig);
-                    MB_CHECK_LAUNCH();
-                }
-                if (nsmall) {  // one warp per hub
-                    k_pr_hub_warp<<<grid_for((int64_t)nsmall * 32, 256, grid_hub_warp), 256, 0, cs>>>(
-                        x, nbig, st.x_nhub);
+                    if (nsmall)
+                        k_pr_hub_warp<<<grid_for((int64_t)nsmall * 32, 256, grid_hub_warp), 256, 0, st.side>>>(
+                            x, nbig, st.x_nhub);
                     MB_CHECK_LAUNCH();
                 }
                 if (st.ngroups) k_pr_sell<<<grid_sell, 256, 0, cs>>>(x);

@@ -1072,7 +1072,8 @@ float sssp_default_delta(const Graph &g) {
     return (float)(mean_w * kDeltaWarps / std::max(1.0, mean_deg));
 }
 
-void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats) {
+void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase, int force,
+             int *cont) {
     st.ensure(g);
     SsspArgs a;
     a.f = st.frontier_args(g, ctx.model(MB_MODEL_SSSP));
@@ -1092,7 +1093,8 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.nbm = st.nbm.as<uint32_t>();
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
-    upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
+    if (phase == LOOP_ALL || phase == LOOP_BEGIN)
+        upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
 
     const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
     const bool bulk = ctx.tunable[MB_TUNE_BULK_STAGE] > 0;
@@ -1185,7 +1187,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         k_stats<<<ctx.num_sms * 4, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();
     };
-    run_loop(ctx, sp, stats);
+    run_loop(ctx, sp, stats, phase, force, cont);
 }
 
 }  // namespace mb

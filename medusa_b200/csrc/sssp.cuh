@@ -47,6 +47,9 @@ struct SsspState : FrontierState {
 uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g);
 
 // One SSSP from `source`; distances are left in st.dist (device).
-void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats);
+// phase / force / cont: a run driven one superstep at a time (LoopPhase,
+// engine.cuh); the defaults run it whole.
+void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase = 0,
+             int force = -1, int *cont = nullptr);
 
 }  // namespace mb

@@ -50,7 +50,7 @@ def test_tune_pagerank_keeps_results(gpu_ctx):
     from medusa_b200 import api, autotune
     g = gpu_ctx.generate(api.rmat_params(14, 1 << 18, 0.57, 0.19, 0.19, seed=3))
     try:
-        for order, keys in ((api.MB_PR_ORDER_REFERENCE, {"pr_light_vpl", "pr_hub_min"}),
+        for order, keys in ((api.MB_PR_ORDER_REFERENCE, {"pr_light_vpl", "pr_hub_min", "pr_hub_ctas"}),
                             (api.MB_PR_ORDER_FIXED, {"pr_light_vpl", "pr_short_pair"})):
             gpu_ctx.set_pagerank_order(order)
             r0, _ = g.pagerank(5, 1.0 / g.V)
@@ -63,5 +63,5 @@ def test_tune_pagerank_keeps_results(gpu_ctx):
     finally:
         gpu_ctx.set_pagerank_order(api.MB_PR_ORDER_REFERENCE)
         g.close()
-        for k in ("pr_light_vpl", "pr_short_pair", "pr_hub_min"):
+        for k in ("pr_light_vpl", "pr_short_pair", "pr_hub_min", "pr_hub_ctas"):
             gpu_ctx.set_tunable(k, -1)
