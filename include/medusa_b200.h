@@ -211,7 +211,9 @@ int mb_pagerank_from(mb_ctx *ctx, const mb_graph *g, int32_t iters, const float 
  * the traversal needs another superstep (PageRank: always 1; the host stops
  * it).  mb_superstep_result then copies the levels (int32), distances or
  * ranks (float) into out[V] (host or device) with the run's statistics and
- * ends the run.  A stepped run holds the graph's state of that app: any
+ * ends the run.  Each call runs exactly one superstep (the persistent
+ * tail and grid, which run several per launch, are off in a stepped run).
+ * A stepped run holds the graph's state of that app: any
  * whole-run call on the graph (mb_bfs, ...) ends it.  Results are those of
  * the whole-run calls bit for bit, whatever schedules are forced. */
 #define MB_APP_BFS 0

@@ -555,7 +555,14 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
     a.rcol = g.rcol.as<int32_t>();
     a.level = st.level.as<int32_t>();
     a.vis = st.vis.as<uint32_t>();
-    if (phase == LOOP_ALL || phase == LOOP_BEGIN) upload_params(ctx, st.ctrl.p, source);
+    if (phase == LOOP_ALL) upload_params(ctx, st.ctrl.p, source);
+    if (phase == LOOP_BEGIN) {  // a stepped run: one superstep per call (no persistent kernels)
+        const bool tail = ctx.tail, persist = ctx.persist;
+        ctx.tail = ctx.persist = false;
+        upload_params(ctx, st.ctrl.p, source);
+        ctx.tail = tail;
+        ctx.persist = persist;
+    }
 
     const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);

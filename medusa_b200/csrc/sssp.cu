@@ -1093,8 +1093,14 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.nbm = st.nbm.as<uint32_t>();
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
-    if (phase == LOOP_ALL || phase == LOOP_BEGIN)
+    if (phase == LOOP_ALL) upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
+    if (phase == LOOP_BEGIN) {  // a stepped run: one superstep per call (no persistent kernels)
+        const bool tail = ctx.tail, persist = ctx.persist;
+        ctx.tail = ctx.persist = false;
         upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
+        ctx.tail = tail;
+        ctx.persist = persist;
+    }
 
     const int grid_push = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_PUSH_BLOCKS_PER_SM, 8);
     const bool bulk = ctx.tunable[MB_TUNE_BULK_STAGE] > 0;

@@ -45,7 +45,8 @@ def test_stepped_bfs_sssp_pagerank_equal_the_reference(ctx, api, name):
     try:
         lv, st, n = stepped(g, api.MB_APP_BFS, s0)
         np.testing.assert_array_equal(lv, c["bfs_level"][0])
-        assert st["supersteps"] == n
+        # one superstep per call (a source with no out-edges needs none)
+        assert st["supersteps"] == n or (n == 1 and st["supersteps"] == 0)
         lv, _, _ = stepped(g, api.MB_APP_BFS, s0, rng.integers(0, 8, 64))
         np.testing.assert_array_equal(lv, c["bfs_level"][0])
         d, _, _ = stepped(g, api.MB_APP_SSSP, s0)
