@@ -88,7 +88,7 @@ struct Ctrl {
     int32_t fcur;             // far pile being filled
     int32_t splits;           // near-far split steps run
     uint32_t bar_count;       // persistent-grid barrier: arrivals over the run (top bit: gave up)
-    uint32_t bar_gen;         // unused
+    uint32_t pad_bar;
     int32_t persist_go;       // persistent grid: run another superstep
 };
 

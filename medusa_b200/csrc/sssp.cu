@@ -43,6 +43,7 @@ struct SsspArgs {
     int32_t *far[2];  // near-far piles (vertices whose distance is >= the threshold)
     uint32_t *farbm;  // membership bitmap of the pile being filled
     uint32_t *nbm;    // next-frontier bitmap of the bitmap-output push (all zero between uses)
+    float *dprev;     // distances before the superstep (the snapshot variant of that push)
 };
 
 __device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
@@ -104,6 +105,14 @@ struct PushSmem {
 // behind this switch, off.
 #ifndef MB_SSSP_MATCH
 #define MB_SSSP_MATCH 0
+#endif
+// The bitmap-output push without the per-edge distance read: every
+// relaxation is a fire-and-forget atomicMin, and the next frontier is the
+// set of vertices whose distance dropped below a snapshot taken before the
+// superstep (plain frontier Bellman-Ford only).  Measured against the
+// default; off unless set.
+#ifndef MB_SSSP_SNAPSHOT
+#define MB_SSSP_SNAPSHOT 0
 #endif
 // 128-bit col/wt loads in the edge-balanced push (needs 4 edges per thread:
 // MB_TILE_EDGES=1024).  Measured against the scalar loads; off.
@@ -246,6 +255,15 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
             }
         }
 #endif
+#if MB_SSSP_SNAPSHOT
+        if (kBmOut && thresh > 1e38f) {  // block-uniform
+#pragma unroll
+            for (int r = 0; r < kTileItems; r++)
+                if (ok[r]) atomicMin((unsigned *)&a.dist[v[r]], __float_as_uint(nd[r]));
+            __syncthreads();  // the tile's shared entries are reloaded next
+            continue;
+        }
+#endif
 #pragma unroll
         for (int r = 0; r < kTileItems; r++) dv[r] = ok[r] ? ld_dist(a, v[r]) : 0.f;
         if (kBmOut) {
@@ -336,6 +354,42 @@ __global__ void __launch_bounds__(kPushThreads) k_nbm2q(SsspArgs a) {
     }
     flush_counts(c, cn, 0);
 }
+
+#if MB_SSSP_SNAPSHOT
+__global__ void k_snap(SsspArgs a) {
+    count_launch(a.f.ctrl);
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
+         v += (int64_t)gridDim.x * blockDim.x)
+        a.dprev[v] = __ldcg(&a.dist[v]);
+}
+
+// After the snapshot push: the vertices whose distance dropped -> next queue.
+__global__ void __launch_bounds__(kPushThreads) k_snap2q(SsspArgs a) {
+    __shared__ BlockQueue bq;
+    count_launch(a.f.ctrl);
+    Ctrl *c = a.f.ctrl;
+    const int nxt = c->cur ^ 1;
+    const int32_t sv = c->step + 1;
+    if (threadIdx.x == 0) bq.n = 0;
+    __syncthreads();
+    uint32_t cn = 0;
+    const int64_t per = (int64_t)blockDim.x;
+    for (int64_t v0 = (int64_t)blockIdx.x * per; v0 < a.f.V; v0 += (int64_t)gridDim.x * per) {
+        const int64_t v = v0 + threadIdx.x;
+        bool in = false;
+        uint32_t deg = 0;
+        if (v < a.f.V && __ldcg(&a.dist[v]) < a.dprev[v]) {
+            in = true;
+            deg = (uint32_t)a.f.outdeg[v];
+            a.stamp[v] = sv;
+            cn++;
+        }
+        bq_push(bq, in && deg > 0, (int32_t)v, deg);
+        bq_flush(bq, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt), pick(a.f.tf, nxt));
+    }
+    flush_counts(c, cn, 0);
+}
+#endif
 
 // schedule 1: push, warp-per-vertex for lists >= 32, warp-wide gather below
 __global__ void __launch_bounds__(kPushThreads) k_push_warp_q(SsspArgs a) {
@@ -1091,6 +1145,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.far[1] = st.far[1].as<int32_t>();
     a.farbm = st.farbm.as<uint32_t>();
     a.nbm = st.nbm.as<uint32_t>();
+    a.dprev = st.dprev.as<float>();
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
     if (phase == LOOP_ALL) upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
@@ -1147,6 +1202,16 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
             MB_CHECK_LAUNCH();
             return;
         }
+#if MB_SSSP_SNAPSHOT
+        if (branch == kBranchPushBm && delta == 0.f) {
+            k_snap<<<grid_vtx, 256, 0, s>>>(a);
+            if (bulk) k_push_edge_bm<true><<<grid_push, kPushThreads, 0, s>>>(a);
+            else k_push_edge_bm<false><<<grid_push, kPushThreads, 0, s>>>(a);
+            k_snap2q<<<grid_vtx, kPushThreads, 0, s>>>(a);
+            MB_CHECK_LAUNCH();
+            return;
+        }
+#endif
         if (branch == kBranchPushBm) {
             if (bulk) k_push_edge_bm<true><<<grid_push, kPushThreads, 0, s>>>(a);
             else k_push_edge_bm<false><<<grid_push, kPushThreads, 0, s>>>(a);

@@ -9,7 +9,7 @@ namespace mb {
 float sssp_default_delta(const Graph &g);
 
 struct SsspState : FrontierState {
-    DevBuf dist, stamp, msg, far[2], farbm, nbm;
+    DevBuf dist, stamp, msg, far[2], farbm, nbm, dprev;
     float default_delta = 0.f;
     ~SsspState() { release(); }
     void release() {
@@ -21,6 +21,7 @@ struct SsspState : FrontierState {
         far[1].release();
         farbm.release();
         nbm.release();
+        dprev.release();
     }
     void ensure(const Graph &g) {
         if (ensure_frontier(g)) {
@@ -36,6 +37,7 @@ struct SsspState : FrontierState {
             far[1].reserve(sizeof(int32_t) * (size_t)g.V);
             farbm.reserve(sizeof(uint32_t) * (size_t)W);
             nbm.reserve(sizeof(uint32_t) * (size_t)W);
+            dprev.reserve(sizeof(float) * (size_t)g.V);
             default_delta = sssp_default_delta(g);
         }
     }
