@@ -836,7 +836,7 @@ void PrState::ensure(Context &ctx, const Graph &g) {
 
 void PrState::ensure_exact(Context &ctx, const Graph &g, int32_t hub_min) {
     if (exact_built && x_hub_min == hub_min) return;
-    build_meg_order(ctx, *const_cast<Graph *>(&g), *this);
+    build_meg_order(ctx, g, *this);
     release_exact();
     const int32_t V = g.V;
     cudaStream_t s = ctx.stream;
