@@ -366,7 +366,20 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
 #define MB_TUNE_PR_HUB_CTAS 16 /* PageRank in the reference's order: CTAs of the scans of
                                  the hubs above 16384 in-edges, which run beside the other
                                  kernels (default SMs / 4) */
-#define MB_NUM_TUNABLES 17
+#define MB_TUNE_SSSP_ASYNC 17 /* SSSP: 1 runs the traversal from a queue frontier as one
+                                asynchronous cooperative launch (no superstep barriers:
+                                warps relax the dirty vertices below a distance threshold
+                                that rises by MB_TUNE_ASYNC_DELTA whenever every warp is
+                                idle); 0 (the default) the BSP supersteps.  Under
+                                MB_POLICY_FIXED only (the other policies pick every
+                                superstep), and only on graphs without a negative or NaN
+                                weight.  Identical distances */
+#define MB_TUNE_ASYNC_DELTA 18 /* width by which the asynchronous SSSP's threshold rises
+                                 (default 8 x mean weight / mean out-degree, at least the
+                                 mean weight; 0: no threshold) */
+#define MB_TUNE_ASYNC_BLOCKS_PER_SM 19 /* CTAs of 256 threads per SM of the asynchronous
+                                         SSSP (default: as many as fit, at most 8) */
+#define MB_NUM_TUNABLES 20
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

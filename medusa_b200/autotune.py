@@ -14,6 +14,11 @@ first run after a change rebuilds the loop's CUDA graph); the median counts.
 import numpy as np
 
 
+# threshold steps of the asynchronous SSSP tried (-1: the per-graph default,
+# 8 x mean weight / mean out-degree; 0: no threshold)
+ASYNC_DELTAS = [-1, 0, 50, 200, 800, 3200]
+
+
 def _median_ms(fn, reps):
     fn()
     return float(np.median([fn()["device_ms"] for _ in range(reps)]))
@@ -55,9 +60,13 @@ def tune(ctx, run, space, reps=3, passes=1):
 
 
 def tune_sssp(ctx, g, source=0, reps=3):
-    """Bitmap-output push threshold and push grid for SSSP on graph g."""
+    """Asynchronous kernel on or off and its threshold step and grid, then
+    the bitmap-output push threshold and push grid for SSSP on graph g."""
     E = max(int(g.E), 1)
-    space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
+    space = {"sssp_async": [-1, 0],
+             "async_delta": ASYNC_DELTAS,
+             "async_blocks_per_sm": [-1, 2, 3],
+             "sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "bulk_stage": [-1, 1]}
     return tune(ctx, lambda: g.sssp([source])[1], space, reps)
@@ -84,7 +93,10 @@ def tune_traversals(ctx, g, source=0, reps=3):
         ss = g.sssp([source])[1]
         return {"device_ms": sb["device_ms"] + ss["device_ms"]}
 
-    space = {"sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
+    space = {"sssp_async": [-1, 0],
+             "async_delta": ASYNC_DELTAS,
+             "async_blocks_per_sm": [-1, 2, 3],
+             "sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "sssp_delta": [0.0, -1.0, 100.0, 1000.0, 10000.0],
              "tail_edges": [-1, 0, 2048, 4096],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],

@@ -581,8 +581,9 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
         MB_CHECK_LAUNCH();
     };
     sp.branch = [&](int branch, cudaStream_t s) {
-        // BFS never routes to the bitmap-output push (bm_push_min is 0)
-        if (branch == kBranchPushBm) branch = MB_SCHED_PUSH_EDGE_QUEUE;
+        // BFS never routes to the bitmap-output push (bm_push_min is 0) nor
+        // to the asynchronous kernel (sssp_async is 0)
+        if (branch == kBranchPushBm || branch == kBranchAsync) branch = MB_SCHED_PUSH_EDGE_QUEUE;
         if (branch == kBranchPushSmall) {
             k_push_edge_q<<<ctx.num_sms * kSmallPushPerSm, kPushThreads, 0, s>>>(a);
             MB_CHECK_LAUNCH();

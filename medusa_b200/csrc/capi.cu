@@ -302,6 +302,12 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "bulk staging is 0 or 1");
     if (which == MB_TUNE_PR_HUB_MIN && value != -1 && (value < 64 || value > 0x7fffffff))
         return set_error(ctx, MB_ERR_INVALID, "PageRank hub threshold must be >= 64");
+    if (which == MB_TUNE_SSSP_ASYNC && value > 1)
+        return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP is 0 or 1");
+    if (which == MB_TUNE_ASYNC_DELTA && value > (1 << 30))
+        return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP delta must be <= 2^30");
+    if (which == MB_TUNE_ASYNC_BLOCKS_PER_SM && (value == 0 || value > 8))
+        return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP blocks per SM must be 1..8");
     ctx->c.tunable[which] = value;
     ctx->c.tune_gen++;  // captured loop graphs embed launch shapes: rebuild them
     return MB_OK;

@@ -4,7 +4,8 @@
 
 namespace mb {
 
-void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, uint32_t bm_push_min) {
+void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, uint32_t bm_push_min,
+                   int32_t sssp_async, float async_delta) {
     static_assert(sizeof(RunParams) <= Context::kCtrlOff, "params staging too small");
     static_assert(sizeof(Ctrl) <= Context::kSmallBytes - Context::kCtrlOff, "ctrl readback too small");
     RunParams *p = (RunParams *)(ctx.pinned_small + Context::kParamsOff);
@@ -19,6 +20,8 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->replay_then_fixed = ctx.replay_then_fixed ? 1 : 0;
     p->max_step = ctx.max_step;
     p->bm_push_min = bm_push_min;
+    p->sssp_async = sssp_async;
+    p->async_delta = async_delta;
     p->bfs_alpha = ctx.tunable[MB_TUNE_BFS_ALPHA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_ALPHA] : 15;
     p->bfs_beta = ctx.tunable[MB_TUNE_BFS_BETA] > 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_BETA] : 20;
     p->bfs_gamma = ctx.tunable[MB_TUNE_BFS_GAMMA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_GAMMA] : kBfsGammaDefault;
@@ -71,6 +74,8 @@ static void run_loop_phase(Context &ctx, LoopSpec &sp, mb_stats *stats, int phas
     if (hc->err & ERR_BULK) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a bulk copy timed out");
     if (hc->err & ERR_BARRIER)
         fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a persistent-grid barrier timed out");
+    if (hc->err & ERR_ASYNC)
+        fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a wait of the asynchronous kernel timed out");
     if (phase == LOOP_FINISH && stats) {
         *stats = mb_stats{};
         stats->supersteps = hc->supersteps;
@@ -165,6 +170,8 @@ void run_loop(Context &ctx, LoopSpec &sp, mb_stats *stats, int phase, int force,
         if (hc->err & ERR_BULK) fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a bulk copy timed out");
         if (hc->err & ERR_BARRIER)
             fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a persistent-grid barrier timed out");
+        if (hc->err & ERR_ASYNC)
+            fail(MB_ERR_TIMEOUT, std::string(sp.name) + ": a wait of the asynchronous kernel timed out");
         if (stats) {
             stats->supersteps = hc->supersteps;
             stats->status_flags = hc->err;

@@ -22,6 +22,7 @@ constexpr int FMT_QUEUE = 0, FMT_BITMAP = 1, FMT_NONE = 2;
 constexpr int ERR_STEP_CAP = 1;
 constexpr int ERR_BARRIER = 2;     // a grid barrier of the persistent kernel gave up
 constexpr int ERR_BULK = 4;        // a bulk copy into shared memory did not complete in time
+constexpr int ERR_ASYNC = 8;       // a wait of the asynchronous SSSP kernel gave up
 // Internal step of near-far SSSP (not a user schedule): raise the distance
 // threshold and move far-pile vertices below it into the near queue.
 constexpr int kSchedSplit = MB_NUM_SCHEDULES;
@@ -42,7 +43,11 @@ constexpr int kBranchPushBm = kBranchPersist + 1;
 // p.small_push_max out-edges): the same push on a grid of two CTAs per SM,
 // which dispatches and retires faster than the full grid.
 constexpr int kBranchPushSmall = kBranchPushBm + 1;
-constexpr int kNumBranches = kBranchPushSmall + 1;
+// SSSP schedule 0 on a queue frontier with asynchronous relaxation on: one
+// cooperative launch relaxes until no distance can drop (the rest of the
+// traversal, without superstep barriers).
+constexpr int kBranchAsync = kBranchPushSmall + 1;
+constexpr int kNumBranches = kBranchAsync + 1;
 constexpr int kSmallPushPerSm = 2;  // CTAs per SM of the small-grid push
 constexpr int kTailThreads = 1024;
 constexpr uint32_t kTailEntries = 2048, kTailEdges = 8192;
@@ -153,6 +158,7 @@ __host__ __device__ inline bool persist_supported(int s) {
 
 __device__ inline int route(const Ctrl *c, int s) {
     if (c->p.persist && persist_supported(s)) return kBranchPersist;
+    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.sssp_async) return kBranchAsync;
     if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.tail &&
         c->front_n <= kTailEntries && c->front_m <= c->p.tail_edges)
         return kBranchTail;
@@ -443,7 +449,7 @@ __device__ inline void count_iteration(Ctrl *c, int cap) {
         c->err |= ERR_STEP_CAP;
         c->done = 1;
     }
-    if (c->err & (ERR_BARRIER | ERR_BULK)) c->done = 1;
+    if (c->err & (ERR_BARRIER | ERR_BULK | ERR_ASYNC)) c->done = 1;
 }
 
 // Top of every loop iteration (one warp): bookkeeping of the superstep that

@@ -34,6 +34,8 @@ struct RunParams {
     int32_t bfs_gamma;          // BFS fixed rule: bottom-up only from E / gamma frontier out-edges (0: any)
     int64_t wait_polls;         // polls before a bounded device wait gives up (-1: each wait's default)
     uint32_t small_push_max;    // schedule 0 frontiers up to this many out-edges use the small grid
+    int32_t sssp_async;         // SSSP: schedule 0 on a queue frontier runs the asynchronous kernel
+    float async_delta;          // its threshold step (0: no threshold)
     uint32_t pad_;
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
@@ -41,6 +43,6 @@ struct RunParams {
 // Write this run's RunParams (policy, forced schedule, replay list, source,
 // SSSP bucket width) to a control block whose first member is RunParams.
 void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f,
-                   uint32_t bm_push_min = 0);
+                   uint32_t bm_push_min = 0, int32_t sssp_async = 0, float async_delta = 0.f);
 
 }  // namespace mb

@@ -44,6 +44,14 @@ struct SsspArgs {
     uint32_t *farbm;  // membership bitmap of the pile being filled
     uint32_t *nbm;    // next-frontier bitmap of the bitmap-output push (all zero between uses)
     float *dprev;     // distances before the superstep (the snapshot variant of that push)
+    AsyncState *as;   // the asynchronous kernel's counters
+    // the asynchronous kernel's dirty bitmap over vertex ids [0, V) and hub
+    // chunk ids [V, V + nchunks) (a.nbm when the graph has no hub)
+    uint32_t *adirty;
+    int64_t WA;                   // its words
+    const int32_t *hub_cbase;     // first chunk (id - V) of each hub
+    const int32_t *chunk_src;     // hub of each chunk
+    const int32_t *chunk_rs;      // first out-edge of each chunk
 };
 
 __device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
@@ -1020,6 +1028,400 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
     }
 }
 
+// ---- asynchronous SSSP (kBranchAsync) ---------------------------------------
+// The rest of the traversal, from the current queue frontier to the
+// fixpoint, in ONE cooperative launch with no superstep barriers: a chaotic
+// relaxation ordered by a distance threshold, in the manner of Meyer &
+// Sanders' delta-stepping (J. Algorithms 49, 2003) run asynchronously.
+//  - a.adirty is the dirty bitmap: v's bit is set when dist[v] dropped and
+//    v's out-edges have not yet been relaxed from the new distance;
+//  - hubs: a vertex with more than kAsyncChunk out-edges owns one extra id
+//    per kAsyncChunk of them (ids V + hub_cbase[v] + j).  Claiming the hub
+//    sets its chunks' bits instead of relaxing; each chunk is then claimed
+//    (when the hub's distance is below T) and relaxed by its own owner warp
+//    from the hub's distance read at that claim, so one hub's edges spread
+//    over many warps;
+//  - warp g owns the bitmap words g, g + G, g + 2G, ... (G = warps of the
+//    grid; interleaved, so the low-numbered hubs of R-MAT graphs spread out).
+//    Only the owner clears bits: it claims the bits of vertices whose
+//    distance is below the threshold T with one atomicAnd per word, re-reads
+//    their distances and relaxes their out-edges warp-wide, 32 edges per
+//    strip; a lower distance is atomicMin'ed and the neighbour's bit set;
+//  - termination: AsyncState::p counts the bits a warp may set (added, and
+//    its return awaited, before the warp sets any) and AsyncState::d the
+//    part it did not set plus every finished claim.  Both only grow, and
+//    sum(p) - sum(d) is never below the bits set plus the claims in flight.
+//    A warp reads every d, then every p: equal sums mean that at a moment
+//    between the two reads no bit was set and no claim in flight, and from
+//    then on nothing can set one, so every warp leaves;
+//  - a warp that finds nothing below T reports itself idle once per phase
+//    (the CTA's warps in shared memory, then one global count per CTA); the
+//    last CTA raises T by delta (or to the least distance seen above T plus
+//    delta) and opens the next phase.  T only orders the claims: every order
+//    reaches the same fixpoint, the exact distances;
+//  - every wait is bounded: the start barrier and a warp's run of idle
+//    passes give up after wait_polls (default kAsyncSpins), set ERR_ASYNC
+//    and make every warp leave; a warp with more claiming passes than the
+//    run's superstep cap sets ERR_STEP_CAP and does the same;
+//  - polling: only warp 0 of each CTA reads the termination counters and
+//    the abort flag (after an idle pass), and tells its CTA through shared
+//    memory; idle warps sleep 128 ns to 2 us between passes.
+// Ordering: a value returned by an atomic is used in the operand of the next
+// atomic that must come after it (an always-zero shift), so the hardware
+// issues the second only once the first has been performed at L2.
+constexpr int kAsyncThreads = 256;
+constexpr int kAsyncWarps = kAsyncThreads / 32;
+constexpr int kAsyncU = 2;  // strips of 32 edges in flight per warp
+constexpr long kAsyncSpins = 1l << 22;
+constexpr uint32_t kInfBits = 0x7f800000u;
+static_assert(kAsyncSlots == 32, "one work counter slot per lane");
+
+__device__ __forceinline__ unsigned long long ld_rlx64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_rlx32(const void *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t atom_and_acquire(uint32_t *p, uint32_t m) {
+    uint32_t old;
+    asm volatile("atom.acquire.gpu.global.and.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(m) : "memory");
+    return old;
+}
+__device__ __forceinline__ float warp_min_f(float x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x = fminf(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+__device__ __forceinline__ void async_abort(Ctrl *c, AsyncState *S, int err) {
+    atomicOr(&c->err, err);
+    atomicExch((unsigned *)&S->abort_.v, 1u);
+}
+
+// True (in every lane) when no dirty bit is set and no claim is in flight.
+__device__ __forceinline__ bool async_finished(AsyncState *S) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long d = warp_sum(ld_rlx64(&S->d[lane].v));
+    // the p loads wait for every d load (d < 2^63: the offset is zero)
+    const unsigned long long p = warp_sum(ld_rlx64(&S->p[lane].v + (d >> 63)));
+    return p == d;
+}
+
+constexpr int32_t kAsyncChunk = 1024;
+// MB_TUNE_SSSP_ASYNC = -1: the asynchronous kernel unless near-far buckets
+// or the persistent grid were asked for
+constexpr bool kAsyncDefault = false;
+
+// Relax what this warp claimed: lane l holds one dirty id (or v < 0) -- a
+// vertex (its out-edges), a hub (the bits of its chunks) or a chunk (its
+// out-edges).  Every item (an edge, or a chunk bit) may set one dirty bit.
+// Returns the edges relaxed (every lane).
+__device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S, int slot, int32_t v) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    uint32_t *dirty = a.adirty;
+    const int32_t V = a.f.V;
+    const bool mine = v >= 0;
+    const uint32_t claimed = __ballot_sync(FULL, mine);
+    int32_t base = 0;   // edge (or chunk id) of the lane's first item
+    uint32_t deg = 0;   // its items
+    bool hub = false;
+    float du = 0.f;
+    if (mine) {
+        // after the claim (acquire): the latest distances
+        if (v < V) {
+            const int32_t rs = __ldg(&a.row[v]);
+            deg = (uint32_t)(__ldg(&a.row[v + 1]) - rs);
+            du = ld_dist(a, v);
+            base = rs;
+            if (deg > (uint32_t)kAsyncChunk) {
+                hub = true;
+                base = V + __ldg(&a.hub_cbase[v]);
+                deg = (deg + kAsyncChunk - 1) / kAsyncChunk;
+            }
+        } else {
+            const int32_t h = __ldg(&a.chunk_src[v - V]);
+            base = __ldg(&a.chunk_rs[v - V]);
+            deg = (uint32_t)min(kAsyncChunk, __ldg(&a.row[h + 1]) - base);
+            du = ld_dist(a, h);
+        }
+    }
+    const uint32_t incl = warp_incl_scan_u32(deg);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    const int32_t base_e = base - (int32_t)(incl - deg);  // item k of the owner: base_e(owner) + k
+    const uint32_t hubs = __ballot_sync(FULL, hub);
+    unsigned long long pre = 0;
+    if (lane == 0 && total) pre = atomicAdd(&S->p[slot].v, (unsigned long long)total);
+    const int32_t order = (int32_t)(__shfl_sync(FULL, pre, 0) >> 63);  // zero
+    uint32_t newly = 0;
+    for (uint32_t b0 = 0; b0 < total; b0 += 32 * kAsyncU) {
+        int32_t x[kAsyncU];
+        float nd[kAsyncU], dx[kAsyncU];
+        bool ok[kAsyncU];
+#pragma unroll
+        for (int u = 0; u < kAsyncU; u++) {
+            const uint32_t k = b0 + (uint32_t)(u * 32 + lane);
+            int lo = 0;  // lanes whose inclusive prefix is <= k: the owner of item k
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const uint32_t pm = __shfl_sync(FULL, incl, lo + step - 1);
+                if (pm <= k) lo += step;
+            }
+            const int32_t be = __shfl_sync(FULL, base_e, lo & 31);
+            const float ds = __shfl_sync(FULL, du, lo & 31);
+            const bool own_hub = (hubs >> (lo & 31)) & 1u;
+            ok[u] = k < total;
+            const int32_t e = be + (int32_t)k;
+            if (ok[u] && own_hub) {  // a chunk of a claimed hub becomes dirty
+                const uint32_t bit = 1u << ((e + order) & 31);
+                if (!(atomicOr(&dirty[e >> 5], bit) & bit)) newly++;
+                ok[u] = false;
+            }
+            x[u] = ok[u] ? __ldg(&a.col[e]) : 0;
+            nd[u] = ok[u] ? ds + __ldg(&a.wt[e]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kAsyncU; u++) dx[u] = ok[u] ? ld_dist(a, x[u]) : 0.f;
+#pragma unroll
+        for (int u = 0; u < kAsyncU; u++) {
+            if (ok[u] && nd[u] < dx[u]) {
+                const unsigned old = atomicMin((unsigned *)&a.dist[x[u]], __float_as_uint(nd[u]));
+                if (nd[u] < __uint_as_float(old)) {
+                    const uint32_t bit = 1u << ((x[u] + order) & 31);
+                    if (!(atomicOr(&dirty[x[u] >> 5], bit) & bit)) newly++;
+                }
+            }
+        }
+    }
+    newly = warp_sum(newly);
+    // performed after every bit set above (its operand depends on them)
+    if (lane == 0 && (total | claimed))
+        atomicAdd(&S->d[slot].v, (unsigned long long)(total - newly) + (unsigned long long)__popc(claimed));
+    return total - warp_sum(hub ? deg : 0u);
+}
+
+// Lane 0 of a warp whose pass found nothing below the threshold, once per
+// phase: count the warp idle; the CTA's last warp counts the CTA, and the
+// grid's last CTA opens the next phase.
+__device__ __forceinline__ void async_idle(Ctrl *c, AsyncState *S, uint32_t *s_idle, uint32_t ph,
+                                           float T, float delta, float above, int cap) {
+    uint32_t dep = 0;
+    if (above < __uint_as_float(kInfBits))
+        dep = atomicMin((unsigned *)&S->mn[ph & 1].v, __float_as_uint(above));
+    // distances are non-negative: dep >> 31 is zero
+    const uint32_t k = atomicAdd(&s_idle[ph & 1], 1u + (dep >> 31)) + 1u;
+    if (k != (uint32_t)kAsyncWarps) return;
+    // this CTA's warps all reported phase ph; none reports ph + 1 before the
+    // phase opens, which needs this CTA's count below
+    const uint32_t r = atomicExch(&s_idle[(ph + 1) & 1], 0u);
+    __threadfence();
+    const uint32_t g = atomicAdd((unsigned *)&S->idle[ph & 1].v, 1u + (r >> 31)) + 1u;
+    if (g != gridDim.x) return;
+    // every CTA idle in phase ph: raise the threshold
+    const uint32_t mb = atomicExch((unsigned *)&S->mn[ph & 1].v, kInfBits);
+    const float m = __uint_as_float(mb);
+    float tn = T + delta;
+    if (m < __uint_as_float(kInfBits) && m + delta > tn) tn = m + delta;
+    const uint32_t r2 = atomicExch((unsigned *)&S->idle[(ph + 1) & 1].v, 0u);
+    const uint32_t nph = ph + 1u + (r2 >> 31) + (mb >> 31);  // both shifts zero
+    atomicExch(&S->pt.v, ((unsigned long long)nph << 32) | __float_as_uint(tn));
+    atomicAdd(&c->splits, 1);
+    atomicAdd(&c->supersteps, 1);
+    if ((int64_t)nph > (int64_t)cap) async_abort(c, S, ERR_STEP_CAP);
+}
+
+__global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int cap) {
+    const unsigned FULL = 0xffffffffu;
+    Ctrl *c = a.f.ctrl;
+    count_launch(c);
+    AsyncState *S = a.as;
+    uint32_t *dirty = a.adirty;
+    __shared__ uint32_t s_idle[2];
+    __shared__ int s_ok;
+    __shared__ volatile int s_done;  // set by the CTA's checker warp: every warp leaves
+    // claimed vertices waiting for a full batch of 32 (per warp)
+    __shared__ int32_t s_bv[kAsyncWarps][64];
+    int32_t *bv = s_bv[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = gridDim.x * kAsyncWarps;
+    const uint32_t gw = blockIdx.x * kAsyncWarps + (threadIdx.x >> 5);
+    const int slot = (int)(gw & (kAsyncSlots - 1));
+    const long budget = c->p.wait_polls >= 0 ? (long)c->p.wait_polls : kAsyncSpins;
+    const float delta = c->p.async_delta;
+    const float inf = __uint_as_float(kInfBits);
+    const int64_t W = a.WA;
+    const int32_t V = a.f.V;
+    if (threadIdx.x < 2) s_idle[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) s_done = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0)  // finish_superstep credits the frontier's edges
+        atomicAdd((unsigned long long *)&c->work, 0ull - (unsigned long long)c->front_m);
+    // 1. the queue frontier's vertices become dirty
+    {
+        const int cur = c->cur;
+        const uint32_t n = (uint32_t)(c->q[cur] >> 32);
+        const int32_t *qv = pick(a.f.qv, cur);
+        uint32_t again = 0;
+        float dmin = inf;
+        for (uint32_t b0 = gw * 32u; b0 < n; b0 += nwarps * 32u) {
+            const uint32_t i = b0 + (uint32_t)lane;
+            const bool ok = i < n;
+            const int32_t v = ok ? qv[i] : 0;
+            const unsigned m = __ballot_sync(FULL, ok);
+            unsigned long long pre = 0;
+            if (lane == 0) pre = atomicAdd(&S->p[slot].v, (unsigned long long)__popc(m));
+            const int32_t order = (int32_t)(__shfl_sync(FULL, pre, 0) >> 63);
+            if (ok) {
+                dmin = fminf(dmin, ld_dist(a, v));
+                const uint32_t bit = 1u << ((v + order) & 31);
+                if (atomicOr(&dirty[v >> 5], bit) & bit) again++;
+            }
+        }
+        again = warp_sum(again);
+        dmin = warp_min_f(dmin);
+        if (lane == 0) {
+            if (again) atomicAdd(&S->d[slot].v, (unsigned long long)again);
+            if (dmin < inf) atomicMin((unsigned *)&S->t0.v, __float_as_uint(dmin));
+            __threadfence();
+        }
+    }
+    // 2. start barrier (bounded)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd((unsigned *)&S->bar.v, 1u);
+        int ok = 0;
+        for (long it = 0;; it++) {
+            if (ld_acquire_gpu((const unsigned *)&S->bar.v) >= gridDim.x) {
+                ok = 1;
+                break;
+            }
+            if (it >= budget) break;
+            __nanosleep(32);
+        }
+        if (!ok) async_abort(c, S, ERR_ASYNC);
+        s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const float t0 = __uint_as_float(ld_rlx32(&S->t0.v));
+    const float T0 = delta > 0.f ? t0 + delta : inf;
+    // 3. claim and relax until no work is left
+    uint32_t reported = 0xffffffffu;
+    long idle = 0, busy = 0;
+    unsigned long long relaxed = 0;
+    const bool checker = (threadIdx.x >> 5) == 0;
+    for (;;) {
+        if (s_done) break;
+        // warp 0 of each CTA, after an idle pass, looks for the end of the
+        // run (every fourth idle pass: the test reads 64 counter lines) or
+        // an abort, and tells the CTA's other warps through shared memory
+        if (checker && idle > 0) {
+            bool fin = ld_rlx32(&S->abort_.v) != 0u;
+            if (!fin && (idle & 3) == 1) fin = async_finished(S);
+            if (fin) {
+                if (lane == 0) s_done = 1;
+                break;
+            }
+        }
+        const unsigned long long pt = ld_rlx64(&S->pt.v);
+        const uint32_t ph = (uint32_t)(pt >> 32);
+        const float T = ph ? __uint_as_float((uint32_t)pt) : T0;
+        bool found = false;
+        float above = inf;
+        uint32_t nb = 0;  // vertices in bv (warp-uniform)
+        for (int64_t b0 = gw; b0 < W; b0 += (int64_t)nwarps * 32) {
+            const int64_t wl = b0 + (int64_t)lane * nwarps;
+            const uint32_t xl = wl < W ? __ldcg(&dirty[wl]) : 0u;
+            uint32_t nz = __ballot_sync(FULL, xl != 0u);
+            while (nz) {
+                const int j = __ffs(nz) - 1;
+                nz &= nz - 1;
+                const int64_t w = b0 + (int64_t)j * nwarps;
+                const uint32_t x = __shfl_sync(FULL, xl, j);
+                const bool has = (x >> lane) & 1u;
+                const int32_t id = (int32_t)(w * 32 + lane);
+                const float d = !has ? inf : ld_dist(a, id < V ? id : __ldg(&a.chunk_src[id - V]));
+                const bool below = has && d < T;
+                if (has && !below) above = fminf(above, d);
+                const uint32_t mask = __ballot_sync(FULL, below);
+                if (!mask) continue;
+                uint32_t old = 0;
+                if (lane == 0) old = atom_and_acquire(&dirty[w], ~mask);
+                const uint32_t claimed = __shfl_sync(FULL, old, 0) & mask;
+                if (!claimed) continue;
+                found = true;
+                if ((claimed >> lane) & 1u) bv[nb + __popc(claimed & lanemask_lt())] = id;
+                nb += __popc(claimed);
+                __syncwarp();
+                if (nb >= 32) {
+                    relaxed += async_relax(a, S, slot, bv[lane]);
+                    const uint32_t rest = nb - 32;
+                    const int32_t t = lane < (int)rest ? bv[32 + lane] : -1;
+                    __syncwarp();
+                    if (lane < (int)rest) bv[lane] = t;
+                    nb = rest;
+                    __syncwarp();
+                }
+            }
+        }
+        if (nb) {
+            relaxed += async_relax(a, S, slot, lane < (int)nb ? bv[lane] : -1);
+            __syncwarp();
+        }
+        if (found) {
+            idle = 0;
+            if (++busy > (long)cap) {  // more claiming passes than supersteps allowed
+                if (lane == 0) {
+                    async_abort(c, S, ERR_STEP_CAP);
+                    s_done = 1;
+                }
+                break;
+            }
+            continue;
+        }
+        if (reported != ph) {
+            reported = ph;
+            above = warp_min_f(above);
+            if (lane == 0) async_idle(c, S, s_idle, ph, T, delta, above, cap);
+            __syncwarp();
+        }
+        if (++idle > budget) {
+            if (lane == 0) {
+                async_abort(c, S, ERR_ASYNC);
+                s_done = 1;
+            }
+            break;
+        }
+        __nanosleep(128u << (idle < 4 ? idle : 4));
+    }
+    if (lane == 0 && relaxed) atomicAdd((unsigned long long *)&c->work, relaxed);
+}
+
+// Hub chunk tables of the asynchronous kernel (once per graph).
+__global__ void k_chunk_count(const int32_t *row, int32_t V, uint32_t *cnt) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t deg = row[v + 1] - row[v];
+        cnt[v] = deg > kAsyncChunk ? (uint32_t)((deg + kAsyncChunk - 1) / kAsyncChunk) : 0u;
+    }
+}
+__global__ void k_chunk_fill(const int32_t *row, int32_t V, const int32_t *cbase, int32_t *csrc,
+                             int32_t *crs) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t rs = row[v], deg = row[v + 1] - rs;
+        if (deg <= kAsyncChunk) continue;
+        const int32_t n = (deg + kAsyncChunk - 1) / kAsyncChunk, c0 = cbase[v];
+        for (int32_t j = 0; j < n; j++) {
+            csrc[c0 + j] = (int32_t)v;
+            crs[c0 + j] = rs + j * kAsyncChunk;
+        }
+    }
+}
+
 __global__ void k_sssp_init(SsspArgs a) {
     count_launch(a.f.ctrl);
     Ctrl *c = a.f.ctrl;
@@ -1052,6 +1454,10 @@ __global__ void k_sssp_init(SsspArgs a) {
         c->splits = 0;
         c->bar_count = 0;
         c->q[1] = 0ull;
+        a.as->pt.v = 0ull;
+        a.as->mn[0].v = kInfBits;
+        a.as->mn[1].v = kInfBits;
+        a.as->t0.v = kInfBits;
         c->m_unvisited = a.f.E - deg;
         c->n_unvisited = a.f.V - 1;
         if (deg > 0) {
@@ -1063,6 +1469,15 @@ __global__ void k_sssp_init(SsspArgs a) {
         }
     }
     for (int32_t t = threadIdx.x; deg > 0 && t * kTile < deg; t += blockDim.x) pick(a.f.tf, 0)[t] = 0;
+    // the asynchronous kernel's counters (thread 0 set the threshold lines above)
+    {
+        unsigned long long *w = &a.as->p[0].v;
+        constexpr int kWords = (int)(offsetof(AsyncState, pt) / 8);
+        for (int i = threadIdx.x; i < kWords; i += blockDim.x) w[i] = 0ull;
+        if (threadIdx.x < 2) a.as->idle[threadIdx.x].v = 0ull;
+        if (threadIdx.x == 2) a.as->bar.v = 0ull;
+        if (threadIdx.x == 3) a.as->abort_.v = 0ull;
+    }
     __syncthreads();
     if (threadIdx.x == 0) choose_next(c, APP_SSSP, a.f.V, a.f.E);
 }
@@ -1095,13 +1510,21 @@ __global__ void k_stats(SsspArgs a) {
     }
 }
 
-__global__ void k_weight_sum(const float *w, int64_t E, double *out) {
+__global__ void k_weight_sum(const float *w, int64_t E, double *out, unsigned *bad) {
     double t = 0.0;
+    unsigned nb = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < E;
-         i += (int64_t)gridDim.x * blockDim.x)
-        t += w[i];
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = w[i];
+        t += x;
+        nb += !(x >= 0.f);  // negative or NaN
+    }
     t = warp_sum(t);
-    if ((threadIdx.x & 31) == 0) atomicAdd(out, t);
+    nb = warp_sum(nb);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, t);
+        if (nb) atomicAdd(bad, nb);
+    }
 }
 
 }  // namespace
@@ -1112,19 +1535,72 @@ uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g) {
     return (uint32_t)std::min<int64_t>(std::max<int64_t>(1 << 20, g.E / 8), 0xffffffffll);
 }
 
-float sssp_default_delta(const Graph &g) {
-    if (g.E == 0) return 0.f;
+void sssp_weight_stats(const Graph &g, double *mean_w, bool *bad) {
+    *mean_w = 0.0;
+    *bad = false;
+    if (g.E == 0) return;
     DevBuf acc;
-    acc.reserve(sizeof(double));
-    MB_CUDA(cudaMemset(acc.p, 0, sizeof(double)));
-    k_weight_sum<<<grid_for(g.E, 256, 1184), 256>>>(g.wt.as<float>(), g.E, acc.as<double>());
+    acc.reserve(sizeof(double) + sizeof(unsigned));
+    MB_CUDA(cudaMemset(acc.p, 0, sizeof(double) + sizeof(unsigned)));
+    unsigned *d_bad = (unsigned *)(acc.as<char>() + sizeof(double));
+    k_weight_sum<<<grid_for(g.E, 256, 1184), 256>>>(g.wt.as<float>(), g.E, acc.as<double>(), d_bad);
     MB_CHECK_LAUNCH();
-    double sum = 0;
-    MB_CUDA(cudaMemcpy(&sum, acc.p, sizeof(double), cudaMemcpyDeviceToHost));
+    struct {
+        double sum;
+        unsigned nbad;
+    } h;
+    MB_CUDA(cudaMemcpy(&h.sum, acc.p, sizeof(double), cudaMemcpyDeviceToHost));
+    MB_CUDA(cudaMemcpy(&h.nbad, d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost));
     acc.release();
-    const double mean_w = sum / (double)g.E, mean_deg = (double)g.E / (double)g.V;
+    *mean_w = h.sum / (double)g.E;
+    *bad = h.nbad != 0;
+}
+
+float sssp_default_delta(const Graph &g, double mean_w) {
+    if (g.E == 0) return 0.f;
+    const double mean_deg = (double)g.E / (double)g.V;
     constexpr double kDeltaWarps = 32.0;
     return (float)(mean_w * kDeltaWarps / std::max(1.0, mean_deg));
+}
+
+float sssp_async_delta(const Graph &g, double mean_w) {
+    if (g.E == 0) return 0.f;
+    const double mean_deg = (double)g.E / (double)g.V;
+    return (float)std::max(mean_w, mean_w * 8.0 / std::max(1.0, mean_deg));
+}
+
+// Hub chunk tables of the asynchronous kernel for graph g (once).
+static void async_chunks(Context &ctx, Graph &g, SsspState &st) {
+    if (st.nchunks >= 0) return;
+    cudaStream_t s = ctx.stream;
+    const int32_t V = g.V;
+    if (V == 0) {
+        st.nchunks = 0;
+        return;
+    }
+    const int gridV = grid_for(V, 256, ctx.num_sms * 8);
+    st.hub_cbase.reserve(sizeof(int32_t) * (size_t)V);
+    DevBuf tot;
+    tot.reserve(sizeof(uint32_t));
+    k_chunk_count<<<gridV, 256, 0, s>>>(g.row.as<int32_t>(), V, st.hub_cbase.as<uint32_t>());
+    MB_CHECK_LAUNCH();
+    scan_exclusive_u32(ctx, st.hub_cbase.as<uint32_t>(), st.hub_cbase.as<uint32_t>(), V, tot.as<uint32_t>(), s);
+    uint32_t nc = 0;
+    MB_CUDA(cudaMemcpyAsync(&nc, tot.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+    tot.release();
+    if (nc) {
+        st.chunk_src.reserve(sizeof(int32_t) * (size_t)nc);
+        st.chunk_rs.reserve(sizeof(int32_t) * (size_t)nc);
+        k_chunk_fill<<<gridV, 256, 0, s>>>(g.row.as<int32_t>(), V, st.hub_cbase.as<int32_t>(),
+                                           st.chunk_src.as<int32_t>(), st.chunk_rs.as<int32_t>());
+        MB_CHECK_LAUNCH();
+        st.adirty.reserve(sizeof(uint32_t) * (((size_t)V + nc + 31) / 32));
+        MB_CUDA(cudaStreamSynchronize(s));
+    } else {
+        st.hub_cbase.release();
+    }
+    st.nchunks = nc;
 }
 
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase, int force,
@@ -1147,9 +1623,32 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.farbm = st.farbm.as<uint32_t>();
     a.nbm = st.nbm.as<uint32_t>();
     a.dprev = st.dprev.as<float>();
+    a.as = st.as.as<AsyncState>();
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
-    if (phase == LOOP_ALL) upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g));
+    // asynchronous relaxation: the tunable, else on unless the near-far
+    // buckets or the persistent grid were asked for
+    // (fixed policy only: the other policies choose every superstep's schedule)
+    const int64_t t_async = ctx.tunable[MB_TUNE_SSSP_ASYNC];
+    // (fixed policy only: the other policies choose every superstep's
+    // schedule; non-negative weights only: with a negative or NaN weight the
+    // BSP loop's superstep cap is what ends a run)
+    const int32_t async =
+        ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
+            ? 0
+            : (t_async >= 0 ? (int32_t)t_async
+                            : (kAsyncDefault && delta == 0.f && !ctx.persist ? 1 : 0));
+    const float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
+                                                                     : st.async_delta;
+    if (async) async_chunks(ctx, g, st);
+    const int64_t nchunks = st.nchunks > 0 ? st.nchunks : 0;
+    a.adirty = nchunks ? st.adirty.as<uint32_t>() : a.nbm;
+    a.WA = ((int64_t)g.V + nchunks + 31) / 32;
+    a.hub_cbase = st.hub_cbase.as<int32_t>();
+    a.chunk_src = st.chunk_src.as<int32_t>();
+    a.chunk_rs = st.chunk_rs.as<int32_t>();
+    if (phase == LOOP_ALL)
+        upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g), async, async_delta);
     if (phase == LOOP_BEGIN) {  // a stepped run: one superstep per call (no persistent kernels)
         const bool tail = ctx.tail, persist = ctx.persist;
         ctx.tail = ctx.persist = false;
@@ -1163,6 +1662,17 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
     const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
+    int async_grid = 0;
+    {
+        int per_sm = 0;
+        MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_sssp_async,
+                                                              kAsyncThreads, 0));
+        if (per_sm < 1) fail(MB_ERR_UNSUPPORTED, "asynchronous SSSP kernel does not fit on an SM");
+        per_sm = std::min(per_sm, 8);
+        if (ctx.tunable[MB_TUNE_ASYNC_BLOCKS_PER_SM] > 0)
+            per_sm = std::min(per_sm, (int)ctx.tunable[MB_TUNE_ASYNC_BLOCKS_PER_SM]);
+        async_grid = ctx.num_sms * per_sm;
+    }
     MB_CUDA(cudaFuncSetAttribute((const void *)k_tail, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kTailSmemBytes));
     LoopSpec sp;
@@ -1178,6 +1688,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
         MB_CUDA(cudaMemsetAsync(a.farbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
         MB_CUDA(cudaMemsetAsync(a.nbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
+        if (a.adirty != a.nbm) MB_CUDA(cudaMemsetAsync(a.adirty, 0, sizeof(uint32_t) * (size_t)a.WA, s));
         k_sssp_init<<<1, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();
     };
@@ -1194,6 +1705,10 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         }
         if (branch == kBranchPersist) {
             launch_cooperative((const void *)k_persist, persist_grid, kPushThreads, s, a, sp.cap);
+            return;
+        }
+        if (branch == kBranchAsync) {
+            launch_cooperative((const void *)k_sssp_async, async_grid, kAsyncThreads, s, a, sp.cap);
             return;
         }
         if (branch == kBranchPushSmall) {

@@ -4,13 +4,45 @@
 
 namespace mb {
 
+// Mean edge weight of a graph, and whether any weight is negative or NaN.
+void sssp_weight_stats(const Graph &g, double *mean_w, bool *bad);
 // Default near-far bucket width of a graph: kDeltaWarps warps' worth of
 // edges per bucket at the mean degree, times the mean weight.
-float sssp_default_delta(const Graph &g);
+float sssp_default_delta(const Graph &g, double mean_w);
+// Default threshold step of the asynchronous SSSP: 8 x mean weight / mean
+// out-degree, at least the mean weight.
+float sssp_async_delta(const Graph &g, double mean_w);
+
+// Shared state of the asynchronous SSSP kernel (sssp.cu), one per run,
+// zeroed by the run's init kernel.  Every counter sits on its own 128-byte
+// line: the work counters are spread over kAsyncSlots lines so that the
+// warps' atomics do not queue on one address.
+constexpr int kAsyncSlots = 32;
+struct alignas(128) AsyncLine {
+    unsigned long long v;
+    unsigned long long pad_[15];
+};
+struct AsyncState {
+    AsyncLine p[kAsyncSlots];  // monotone: dirty bits a warp may set, added before it sets any
+    AsyncLine d[kAsyncSlots];  // monotone: the part of that it did not set, plus finished claims
+    AsyncLine pt;              // (phase << 32) | float bits of the threshold (phase 0: the start's)
+    AsyncLine idle[2];         // CTAs whose warps all went idle in the phase of that parity
+    AsyncLine mn[2];           // least distance seen above the threshold in that phase (float bits)
+    AsyncLine t0;              // least distance of the starting frontier (float bits)
+    AsyncLine bar;             // start barrier: CTAs arrived
+    AsyncLine abort_;          // nonzero: a wait gave up and every warp leaves
+};
 
 struct SsspState : FrontierState {
-    DevBuf dist, stamp, msg, far[2], farbm, nbm, dprev;
+    DevBuf dist, stamp, msg, far[2], farbm, nbm, dprev, as;
+    // hub chunks of the asynchronous kernel, made on its first run on the
+    // graph (nchunks < 0: not yet): dirty bitmap over V + nchunks ids, the
+    // first chunk of each hub, each chunk's hub and first out-edge
+    DevBuf adirty, hub_cbase, chunk_src, chunk_rs;
+    int64_t nchunks = -1;
     float default_delta = 0.f;
+    float async_delta = 0.f;
+    bool weights_ok = true;  // no negative or NaN weight (the asynchronous kernel needs it)
     ~SsspState() { release(); }
     void release() {
         release_frontier();
@@ -22,6 +54,15 @@ struct SsspState : FrontierState {
         farbm.release();
         nbm.release();
         dprev.release();
+        as.release();
+        release_chunks();
+    }
+    void release_chunks() {
+        adirty.release();
+        hub_cbase.release();
+        chunk_src.release();
+        chunk_rs.release();
+        nchunks = -1;
     }
     void ensure(const Graph &g) {
         if (ensure_frontier(g)) {
@@ -38,7 +79,14 @@ struct SsspState : FrontierState {
             farbm.reserve(sizeof(uint32_t) * (size_t)W);
             nbm.reserve(sizeof(uint32_t) * (size_t)W);
             dprev.reserve(sizeof(float) * (size_t)g.V);
-            default_delta = sssp_default_delta(g);
+            as.reserve(sizeof(AsyncState));
+            release_chunks();
+            double mean_w = 0.0;
+            bool bad = false;
+            sssp_weight_stats(g, &mean_w, &bad);
+            default_delta = sssp_default_delta(g, mean_w);
+            async_delta = sssp_async_delta(g, mean_w);
+            weights_ok = !bad;
         }
     }
 };

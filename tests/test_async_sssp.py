@@ -1,0 +1,131 @@
+"""The asynchronous SSSP kernel (MB_TUNE_SSSP_ASYNC): the rest of a traversal
+in one cooperative launch, with no superstep barriers.
+
+Shortest-path distances over integer weights stored as float are exact and
+unique, so any order of relaxations reaches the reference's distances bit for
+bit: every golden graph (fixtures made by the reference's own CPU superstep),
+every threshold step, both loop modes, graphs whose hubs are split into
+chunks, and the full-size configurations against the BSP supersteps."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api():
+    from medusa_b200 import api as a
+    return a
+
+
+@pytest.fixture(params=[False, True], ids=["hostloop", "graph"])
+def actx(request, gpu_ctx, api):
+    gpu_ctx.set_graph_capture(request.param)
+    gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+    gpu_ctx.set_tunable("sssp_async", 1)
+    yield gpu_ctx
+    for k in ("sssp_async", "async_delta", "async_blocks_per_sm"):
+        gpu_ctx.set_tunable(k, -1)
+    gpu_ctx.set_graph_capture(True)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_async_sssp_matches_reference(actx, name):
+    c = load_golden(name)
+    g = actx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        # -1: the per-graph step; 0: no threshold; 1: one weight unit; huge
+        for delta in (-1, 0, 1, 1 << 30):
+            actx.set_tunable("async_delta", delta)
+            for i, s in enumerate(c["sources"]):
+                d, st = g.sssp([int(s)])
+                np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32),
+                                              err_msg="delta %d source %d" % (delta, s))
+    finally:
+        g.close()
+
+
+@pytest.mark.parametrize("seed", [9, 10])
+def test_async_sssp_hub_chunks(actx, api, seed):
+    """Skewed R-MAT (0.57, 0.19, 0.19) with hubs of several thousand
+    out-edges: a hub's edges are relaxed as 1024-edge chunks by many warps."""
+    p = api.rmat_params(14, 1 << 20, 0.57, 0.19, 0.19, seed=seed, wmin=1, wmax=1000)
+    V, s, d, w = api.generate_edges_host(p)
+    assert np.bincount(s, minlength=V).max() > 4 * 1024
+    want, _ = O.sssp(V, s, d, w, 0)
+    g = actx.generate(p)
+    try:
+        for delta in (-1, 0, 50):
+            actx.set_tunable("async_delta", delta)
+            for bps in (-1, 1):
+                actx.set_tunable("async_blocks_per_sm", bps)
+                got, st = g.sssp([0])
+                np.testing.assert_array_equal(got[0].view(np.uint32), want.view(np.uint32),
+                                              err_msg="delta %d blocks %d" % (delta, bps))
+                # every reached vertex's out-edges relaxed at least once
+                assert st["edges_scanned"] >= st["edges_traversed"]
+    finally:
+        g.close()
+
+
+def test_async_sssp_star_hub_and_isolated_source(actx, api):
+    """One vertex with 5000 out-edges (five chunks), a chain behind it, and
+    a source with no out-edges (nothing to relax)."""
+    rng = np.random.default_rng(3)
+    V = 7000
+    src = np.concatenate([np.zeros(5000, np.int32), np.arange(5000, 6998, dtype=np.int32)])
+    dst = np.concatenate([np.arange(1, 5001, dtype=np.int32), np.arange(5001, 6999, dtype=np.int32)])
+    w = rng.integers(1, 100, len(src)).astype(np.float32)
+    g = actx.graph_from_edges(V, src, dst, w)
+    try:
+        for s0 in (0, 6999):
+            want, _ = O.sssp(V, src, dst, w, s0)
+            got, _ = g.sssp([s0])
+            np.testing.assert_array_equal(got[0].view(np.uint32), want.view(np.uint32))
+    finally:
+        g.close()
+
+
+def test_async_sssp_negative_weight_takes_the_bsp_loop(gpu_ctx, api):
+    """A graph with a negative weight runs the BSP loop even when the
+    asynchronous kernel is asked for (the loop's superstep cap is what bounds
+    such a run); without a negative cycle it gets the oracle's distances."""
+    V = 4
+    src = np.array([0, 1, 0, 2], np.int32)
+    dst = np.array([1, 2, 2, 3], np.int32)
+    w = np.array([5, -2, 4, 1], np.float32)
+    g = gpu_ctx.graph_from_edges(V, src, dst, w)
+    try:
+        gpu_ctx.set_tunable("sssp_async", 1)
+        got, st = g.sssp([0])
+        want, _ = O.sssp(V, src, dst, w, 0)
+        np.testing.assert_array_equal(got[0], want)
+    finally:
+        gpu_ctx.set_tunable("sssp_async", -1)
+        g.close()
+
+
+@pytest.mark.parametrize("which", ["c2_rmat", "c3_grid"])
+def test_async_sssp_full_size_equals_bsp(gpu_ctx, api, which):
+    """C2 (R-MAT 2^20 / 2^24) and C3 (1448^2 grid): the asynchronous kernel
+    and the BSP supersteps give the same distances bit for bit, and the
+    asynchronous one relaxes fewer edges."""
+    if which == "c2_rmat":
+        p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
+    else:
+        p = api.grid_params(1448, 1448, 0.1, 0.005, seed=1, wmin=1, wmax=100)
+    g = gpu_ctx.generate(p)
+    try:
+        gpu_ctx.set_tunable("sssp_async", 0)
+        ref, st0 = g.sssp([0])
+        gpu_ctx.set_tunable("sssp_async", 1)
+        got, st1 = g.sssp([0])
+        np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
+        assert st1["edges_traversed"] == st0["edges_traversed"]
+        assert st1["edges_scanned"] < st0["edges_scanned"]
+    finally:
+        gpu_ctx.set_tunable("sssp_async", -1)
+        g.close()

@@ -1,8 +1,9 @@
 """The error paths of the bounded device waits and of the superstep cap.
 
 Every wait on the device is bounded: the grid barrier of the persistent BSP
-kernels, the team barrier of the many-graph kernel and the wait for a bulk
-copy into shared memory give up after a number of polls, record an error
+kernels, the team barrier of the many-graph kernel, the wait for a bulk copy
+into shared memory and the start barrier and idle polls of the asynchronous
+SSSP kernel give up after a number of polls, record an error
 flag and return, and the run fails with MB_ERR_TIMEOUT; a loop that passes
 its superstep cap does the same.  MB_TUNE_WAIT_POLLS = 0 makes every such
 wait give up at once and MB_TUNE_STEP_CAP = 1 stops a loop after one
@@ -91,12 +92,31 @@ def test_bulk_copy_wait_gives_up(api, graph):
     ctx, g, want_l, want_d = graph
     try:
         ctx.set_persistent_tail(False)
+        ctx.set_tunable("sssp_async", 0)  # the staged push is a BSP superstep
         ctx.set_tunable("bulk_stage", 1)
         ctx.set_tunable("wait_polls", 0)
         with pytest.raises(api.MedusaError) as e:
             g.sssp([0])
         assert e.value.code == api.MB_ERR_TIMEOUT
         assert "bulk copy" in str(e.value)
+    finally:
+        _still_works(ctx, api, g, want_l, want_d)
+
+
+@pytest.mark.parametrize("capture", [True, False], ids=["graph", "hostloop"])
+def test_async_sssp_wait_gives_up(api, graph, capture):
+    """The asynchronous SSSP kernel with a zero poll budget: every CTA but the
+    last to arrive gives up at the start barrier, every warp leaves, and the
+    run reports the wait."""
+    ctx, g, want_l, want_d = graph
+    try:
+        ctx.set_graph_capture(capture)
+        ctx.set_tunable("sssp_async", 1)
+        ctx.set_tunable("wait_polls", 0)
+        with pytest.raises(api.MedusaError) as e:
+            g.sssp([0])
+        assert e.value.code == api.MB_ERR_TIMEOUT
+        assert "asynchronous" in str(e.value)
     finally:
         _still_works(ctx, api, g, want_l, want_d)
 

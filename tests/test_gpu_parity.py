@@ -75,6 +75,7 @@ def test_sssp_bulk_staged_push_matches_reference(ctx, api, name):
     c = load_golden(name)
     g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
     ctx.set_tunable("bulk_stage", 1)
+    ctx.set_tunable("sssp_async", 0)  # the BSP supersteps
     try:
         for bm_min in (-1, 1):
             ctx.set_tunable("sssp_bm_push_min", bm_min)
@@ -84,7 +85,7 @@ def test_sssp_bulk_staged_push_matches_reference(ctx, api, name):
                 np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32),
                                               err_msg="bm_push_min %d" % bm_min)
     finally:
-        for k in ("bulk_stage", "sssp_bm_push_min", "tail_edges"):
+        for k in ("bulk_stage", "sssp_bm_push_min", "tail_edges", "sssp_async"):
             ctx.set_tunable(k, -1)
         g.close()
 
@@ -371,6 +372,7 @@ def test_sssp_bitmap_output_push(ctx, api, name):
     g = ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
     ctx.set_tunable("sssp_bm_push_min", 1)
     ctx.set_tunable("tail_edges", 0)
+    ctx.set_tunable("sssp_async", 0)  # the BSP supersteps
     try:
         for i, s in enumerate(c["sources"]):
             d, st = g.sssp([int(s)])
@@ -388,6 +390,7 @@ def test_sssp_bitmap_output_push(ctx, api, name):
         ctx.set_policy(api.MB_POLICY_FIXED)
         ctx.set_tunable("sssp_bm_push_min", -1)
         ctx.set_tunable("tail_edges", -1)
+        ctx.set_tunable("sssp_async", -1)
         g.close()
 
 
