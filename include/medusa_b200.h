@@ -379,7 +379,14 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                  mean weight; 0: no threshold) */
 #define MB_TUNE_ASYNC_BLOCKS_PER_SM 19 /* CTAs of 256 threads per SM of the asynchronous
                                          SSSP (default: as many as fit, at most 8) */
-#define MB_NUM_TUNABLES 20
+#define MB_TUNE_BFS_ASYNC 20 /* BFS: 1 runs a single-source BFS under MB_POLICY_FIXED as
+                               the asynchronous kernel with every weight 1 (levels are
+                               hop distances; one cooperative launch); 0 (the default)
+                               the direction-optimising BSP supersteps.  Identical
+                               levels */
+#define MB_TUNE_BFS_ASYNC_DELTA 21 /* threshold step of the asynchronous BFS, in hops
+                                     (default 1: every vertex relaxed once) */
+#define MB_NUM_TUNABLES 22
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

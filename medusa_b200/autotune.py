@@ -63,7 +63,7 @@ def tune_sssp(ctx, g, source=0, reps=3):
     """Asynchronous kernel on or off and its threshold step and grid, then
     the bitmap-output push threshold and push grid for SSSP on graph g."""
     E = max(int(g.E), 1)
-    space = {"sssp_async": [-1, 0],
+    space = {"sssp_async": [-1, 0, 1],
              "async_delta": ASYNC_DELTAS,
              "async_blocks_per_sm": [-1, 2, 3],
              "sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
@@ -93,7 +93,7 @@ def tune_traversals(ctx, g, source=0, reps=3):
         ss = g.sssp([source])[1]
         return {"device_ms": sb["device_ms"] + ss["device_ms"]}
 
-    space = {"sssp_async": [-1, 0],
+    space = {"sssp_async": [-1, 0, 1],
              "async_delta": ASYNC_DELTAS,
              "async_blocks_per_sm": [-1, 2, 3],
              "sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),

@@ -17,6 +17,7 @@
 namespace mb {
 struct AppStates {
     BfsState bfs;
+    SsspState bfs_async;  // the asynchronous BFS's unit-weight runs (MB_TUNE_BFS_ASYNC)
     MsBfsState msbfs;
     SsspState sssp;
     MsSsspState mssssp;
@@ -306,6 +307,10 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP is 0 or 1");
     if (which == MB_TUNE_ASYNC_DELTA && value > (1 << 30))
         return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP delta must be <= 2^30");
+    if (which == MB_TUNE_BFS_ASYNC && value > 1)
+        return set_error(ctx, MB_ERR_INVALID, "asynchronous BFS is 0 or 1");
+    if (which == MB_TUNE_BFS_ASYNC_DELTA && value > (1 << 30))
+        return set_error(ctx, MB_ERR_INVALID, "asynchronous BFS delta must be <= 2^30");
     if (which == MB_TUNE_ASYNC_BLOCKS_PER_SM && (value == 0 || value > 8))
         return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP blocks per SM must be 1..8");
     ctx->c.tunable[which] = value;
@@ -687,9 +692,16 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
             if (stats) *stats = total;
             return;
         }
+        const bool bfs_async = ctx->c.tunable[MB_TUNE_BFS_ASYNC] > 0 &&
+                               ctx->c.schedule_policy == MB_POLICY_FIXED && !ctx->c.persist;
+        if (bfs_async) apps(g).bfs.ensure(g->g);
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};
-            mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st);
+            if (bfs_async)
+                mb::run_sssp(ctx->c, g->g, apps(g).bfs_async, src[i], &st, mb::LOOP_ALL, -1, nullptr,
+                             apps(g).bfs.level.as<int32_t>());
+            else
+                mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st);
             MB_CUDA(cudaMemcpyAsync(levels_out + (size_t)i * V, apps(g).bfs.level.p,
                                     sizeof(int32_t) * (size_t)V, cudaMemcpyDefault, ctx->c.stream));
             total.supersteps = std::max(total.supersteps, st.supersteps);

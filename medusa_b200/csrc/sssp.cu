@@ -49,9 +49,10 @@ struct SsspArgs {
     // chunk ids [V, V + nchunks) (a.nbm when the graph has no hub)
     uint32_t *adirty;
     int64_t WA;                   // its words
-    const int32_t *hub_cbase;     // first chunk (id - V) of each hub
-    const int32_t *chunk_src;     // hub of each chunk
-    const int32_t *chunk_rs;      // first out-edge of each chunk
+    const int32_t *hub_cbase;     // first chunk of each hub
+    const int32_t *chunk_src;     // hub of the chunk at each position (id - V)
+    const int32_t *chunk_rs;      // first out-edge of the chunk at each position
+    int32_t nc32;                 // chunk c sits at id V + (c % 32) * nc32 + c / 32
 };
 
 __device__ __forceinline__ float ld_dist(const SsspArgs &a, int32_t v) {
@@ -1036,11 +1037,13 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
 //  - a.adirty is the dirty bitmap: v's bit is set when dist[v] dropped and
 //    v's out-edges have not yet been relaxed from the new distance;
 //  - hubs: a vertex with more than kAsyncChunk out-edges owns one extra id
-//    per kAsyncChunk of them (ids V + hub_cbase[v] + j).  Claiming the hub
-//    sets its chunks' bits instead of relaxing; each chunk is then claimed
-//    (when the hub's distance is below T) and relaxed by its own owner warp
-//    from the hub's distance read at that claim, so one hub's edges spread
-//    over many warps;
+//    per kAsyncChunk of them.  Chunk c (hub_cbase[v] + j for the j-th of v)
+//    sits at id V + (c % 32) * nc32 + c / 32, so the consecutive chunks of a
+//    hub fall in different bitmap words and thus to different owner warps.
+//    Claiming the hub sets its chunks' bits instead of relaxing; each chunk
+//    is then claimed (when the hub's distance is below T) and relaxed by its
+//    owner from the hub's distance read at that claim, so one hub's edges
+//    spread over many warps and no warp gets a long serial batch;
 //  - warp g owns the bitmap words g, g + G, g + 2G, ... (G = warps of the
 //    grid; interleaved, so the low-numbered hubs of R-MAT graphs spread out).
 //    Only the owner clears bits: it claims the bits of vertices whose
@@ -1071,7 +1074,13 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
 // issues the second only once the first has been performed at L2.
 constexpr int kAsyncThreads = 256;
 constexpr int kAsyncWarps = kAsyncThreads / 32;
-constexpr int kAsyncU = 2;  // strips of 32 edges in flight per warp
+#ifndef MB_ASYNC_U
+#define MB_ASYNC_U 2
+#endif
+#ifndef MB_ASYNC_SLEEP_MAX
+#define MB_ASYNC_SLEEP_MAX 4  // idle sleep 128 ns << min(idle passes, this)
+#endif
+constexpr int kAsyncU = MB_ASYNC_U;  // strips of 32 edges in flight per warp
 constexpr long kAsyncSpins = 1l << 22;
 constexpr uint32_t kInfBits = 0x7f800000u;
 static_assert(kAsyncSlots == 32, "one work counter slot per lane");
@@ -1110,7 +1119,10 @@ __device__ __forceinline__ bool async_finished(AsyncState *S) {
     return p == d;
 }
 
-constexpr int32_t kAsyncChunk = 1024;
+#ifndef MB_ASYNC_CHUNK
+#define MB_ASYNC_CHUNK 128
+#endif
+constexpr int32_t kAsyncChunk = MB_ASYNC_CHUNK;
 // MB_TUNE_SSSP_ASYNC = -1: the asynchronous kernel unless near-far buckets
 // or the persistent grid were asked for
 constexpr bool kAsyncDefault = false;
@@ -1119,7 +1131,18 @@ constexpr bool kAsyncDefault = false;
 // vertex (its out-edges), a hub (the bits of its chunks) or a chunk (its
 // out-edges).  Every item (an edge, or a chunk bit) may set one dirty bit.
 // Returns the edges relaxed (every lane).
-__device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S, int slot, int32_t v) {
+// Local continuation (MB_ASYNC_LOCAL): a vertex this warp newly makes dirty
+// with a distance below the threshold T is also recorded in `nxt` (up to
+// kAsyncNext, *nn of them, warp-uniform), and the warp claims and relaxes it
+// next itself instead of leaving it to its owner's next pass.
+#ifndef MB_ASYNC_LOCAL
+#define MB_ASYNC_LOCAL 0
+#endif
+constexpr uint32_t kAsyncNext = 64;
+
+template <bool kUnit>
+__device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S, int slot, int32_t v,
+                                                float T, int32_t *nxt, uint32_t *nn) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     uint32_t *dirty = a.adirty;
@@ -1176,23 +1199,39 @@ __device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S
             ok[u] = k < total;
             const int32_t e = be + (int32_t)k;
             if (ok[u] && own_hub) {  // a chunk of a claimed hub becomes dirty
-                const uint32_t bit = 1u << ((e + order) & 31);
-                if (!(atomicOr(&dirty[e >> 5], bit) & bit)) newly++;
+                const int32_t c = e - V;
+                const int32_t id = V + (c & 31) * a.nc32 + (c >> 5);
+                const uint32_t bit = 1u << ((id + order) & 31);
+                if (!(atomicOr(&dirty[id >> 5], bit) & bit)) newly++;
                 ok[u] = false;
             }
             x[u] = ok[u] ? __ldg(&a.col[e]) : 0;
-            nd[u] = ok[u] ? ds + __ldg(&a.wt[e]) : 0.f;
+            nd[u] = ok[u] ? ds + (kUnit ? 1.f : __ldg(&a.wt[e])) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < kAsyncU; u++) dx[u] = ok[u] ? ld_dist(a, x[u]) : 0.f;
+        bool keep[kAsyncU];
 #pragma unroll
         for (int u = 0; u < kAsyncU; u++) {
+            keep[u] = false;
             if (ok[u] && nd[u] < dx[u]) {
                 const unsigned old = atomicMin((unsigned *)&a.dist[x[u]], __float_as_uint(nd[u]));
                 if (nd[u] < __uint_as_float(old)) {
                     const uint32_t bit = 1u << ((x[u] + order) & 31);
-                    if (!(atomicOr(&dirty[x[u] >> 5], bit) & bit)) newly++;
+                    if (!(atomicOr(&dirty[x[u] >> 5], bit) & bit)) {
+                        newly++;
+                        keep[u] = MB_ASYNC_LOCAL && nd[u] < T;
+                    }
                 }
+            }
+        }
+        if (MB_ASYNC_LOCAL) {
+#pragma unroll
+            for (int u = 0; u < kAsyncU; u++) {
+                const uint32_t km = __ballot_sync(FULL, keep[u]);
+                const uint32_t pos = *nn + __popc(km & lanemask_lt());
+                if (keep[u] && pos < kAsyncNext) nxt[pos] = x[u];
+                *nn = min(kAsyncNext, *nn + (uint32_t)__popc(km));
             }
         }
     }
@@ -1233,6 +1272,8 @@ __device__ __forceinline__ void async_idle(Ctrl *c, AsyncState *S, uint32_t *s_i
     if ((int64_t)nph > (int64_t)cap) async_abort(c, S, ERR_STEP_CAP);
 }
 
+// kUnit: every weight 1 (BFS levels as hop distances; a.wt is not read).
+template <bool kUnit>
 __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int cap) {
     const unsigned FULL = 0xffffffffu;
     Ctrl *c = a.f.ctrl;
@@ -1242,9 +1283,12 @@ __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int ca
     __shared__ uint32_t s_idle[2];
     __shared__ int s_ok;
     __shared__ volatile int s_done;  // set by the CTA's checker warp: every warp leaves
-    // claimed vertices waiting for a full batch of 32 (per warp)
+    // claimed vertices waiting for a full batch of 32, and the vertices the
+    // warp keeps for itself (local continuation), per warp
     __shared__ int32_t s_bv[kAsyncWarps][64];
+    __shared__ int32_t s_nxt[kAsyncWarps][kAsyncNext];
     int32_t *bv = s_bv[threadIdx.x >> 5];
+    int32_t *nxt = s_nxt[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const uint32_t nwarps = gridDim.x * kAsyncWarps;
     const uint32_t gw = blockIdx.x * kAsyncWarps + (threadIdx.x >> 5);
@@ -1332,6 +1376,43 @@ __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int ca
         bool found = false;
         float above = inf;
         uint32_t nb = 0;  // vertices in bv (warp-uniform)
+        uint32_t nn = 0;  // vertices in nxt (warp-uniform)
+        // relax full batches of bv (all of it when `all`), taking the kept
+        // vertices of nxt into bv (claimed back from the bitmap) as they come
+        auto drain = [&](bool all) {
+            for (;;) {
+                if (nn > 0 && nb < 32) {
+                    const uint32_t take = min(nn, 32u);
+                    const int32_t x = lane < (int)take ? nxt[lane] : -1;
+                    const int32_t rest = lane + (int)take < (int)nn ? nxt[lane + take] : -1;
+                    __syncwarp();
+                    if (lane + take < nn) nxt[lane] = rest;
+                    nn -= take;
+                    bool got = false;
+                    if (x >= 0) {
+                        const uint32_t bit = 1u << (x & 31);
+                        got = (atom_and_acquire(&dirty[x >> 5], ~bit) & bit) != 0u;
+                    }
+                    const uint32_t gm = __ballot_sync(FULL, got);
+                    if (got) bv[nb + __popc(gm & lanemask_lt())] = x;
+                    nb += __popc(gm);
+                    __syncwarp();
+                    continue;
+                }
+                if (nb >= 32 || (all && nb > 0)) {
+                    relaxed += async_relax<kUnit>(a, S, slot, lane < (int)nb ? bv[lane] : -1, T, nxt, &nn);
+                    const uint32_t done = min(nb, 32u);
+                    const uint32_t rest = nb - done;
+                    const int32_t t = lane < (int)rest ? bv[32 + lane] : -1;
+                    __syncwarp();
+                    if (lane < (int)rest) bv[lane] = t;
+                    nb = rest;
+                    __syncwarp();
+                    continue;
+                }
+                break;
+            }
+        };
         for (int64_t b0 = gw; b0 < W; b0 += (int64_t)nwarps * 32) {
             const int64_t wl = b0 + (int64_t)lane * nwarps;
             const uint32_t xl = wl < W ? __ldcg(&dirty[wl]) : 0u;
@@ -1356,21 +1437,10 @@ __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int ca
                 if ((claimed >> lane) & 1u) bv[nb + __popc(claimed & lanemask_lt())] = id;
                 nb += __popc(claimed);
                 __syncwarp();
-                if (nb >= 32) {
-                    relaxed += async_relax(a, S, slot, bv[lane]);
-                    const uint32_t rest = nb - 32;
-                    const int32_t t = lane < (int)rest ? bv[32 + lane] : -1;
-                    __syncwarp();
-                    if (lane < (int)rest) bv[lane] = t;
-                    nb = rest;
-                    __syncwarp();
-                }
+                drain(false);
             }
         }
-        if (nb) {
-            relaxed += async_relax(a, S, slot, lane < (int)nb ? bv[lane] : -1);
-            __syncwarp();
-        }
+        drain(true);
         if (found) {
             idle = 0;
             if (++busy > (long)cap) {  // more claiming passes than supersteps allowed
@@ -1395,7 +1465,7 @@ __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int ca
             }
             break;
         }
-        __nanosleep(128u << (idle < 4 ? idle : 4));
+        __nanosleep(128u << (idle < MB_ASYNC_SLEEP_MAX ? idle : MB_ASYNC_SLEEP_MAX));
     }
     if (lane == 0 && relaxed) atomicAdd((unsigned long long *)&c->work, relaxed);
 }
@@ -1408,16 +1478,17 @@ __global__ void k_chunk_count(const int32_t *row, int32_t V, uint32_t *cnt) {
         cnt[v] = deg > kAsyncChunk ? (uint32_t)((deg + kAsyncChunk - 1) / kAsyncChunk) : 0u;
     }
 }
-__global__ void k_chunk_fill(const int32_t *row, int32_t V, const int32_t *cbase, int32_t *csrc,
-                             int32_t *crs) {
+__global__ void k_chunk_fill(const int32_t *row, int32_t V, const int32_t *cbase, int32_t nc32,
+                             int32_t *csrc, int32_t *crs) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t rs = row[v], deg = row[v + 1] - rs;
         if (deg <= kAsyncChunk) continue;
         const int32_t n = (deg + kAsyncChunk - 1) / kAsyncChunk, c0 = cbase[v];
         for (int32_t j = 0; j < n; j++) {
-            csrc[c0 + j] = (int32_t)v;
-            crs[c0 + j] = rs + j * kAsyncChunk;
+            const int32_t c = c0 + j, q = (c & 31) * nc32 + (c >> 5);
+            csrc[q] = (int32_t)v;
+            crs[q] = rs + j * kAsyncChunk;
         }
     }
 }
@@ -1510,6 +1581,16 @@ __global__ void k_stats(SsspArgs a) {
     }
 }
 
+// Hop distances of a unit-weight run -> BFS levels (-1 unreached).
+__global__ void k_dist_to_level(SsspArgs a, int32_t *level) {
+    count_launch(a.f.ctrl);
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < a.f.V;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const float d = a.dist[v];
+        level[v] = d < kMedusaMax ? (int32_t)d : -1;
+    }
+}
+
 __global__ void k_weight_sum(const float *w, int64_t E, double *out, unsigned *bad) {
     double t = 0.0;
     unsigned nb = 0;
@@ -1589,13 +1670,15 @@ static void async_chunks(Context &ctx, Graph &g, SsspState &st) {
     MB_CUDA(cudaMemcpyAsync(&nc, tot.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
     tot.release();
+    st.nc32 = (int32_t)((nc + 31) / 32);
     if (nc) {
-        st.chunk_src.reserve(sizeof(int32_t) * (size_t)nc);
-        st.chunk_rs.reserve(sizeof(int32_t) * (size_t)nc);
-        k_chunk_fill<<<gridV, 256, 0, s>>>(g.row.as<int32_t>(), V, st.hub_cbase.as<int32_t>(),
+        const size_t slots = 32 * (size_t)st.nc32;  // chunk positions, holes included
+        st.chunk_src.reserve(sizeof(int32_t) * slots);
+        st.chunk_rs.reserve(sizeof(int32_t) * slots);
+        k_chunk_fill<<<gridV, 256, 0, s>>>(g.row.as<int32_t>(), V, st.hub_cbase.as<int32_t>(), st.nc32,
                                            st.chunk_src.as<int32_t>(), st.chunk_rs.as<int32_t>());
         MB_CHECK_LAUNCH();
-        st.adirty.reserve(sizeof(uint32_t) * (((size_t)V + nc + 31) / 32));
+        st.adirty.reserve(sizeof(uint32_t) * (((size_t)V + slots + 31) / 32));
         MB_CUDA(cudaStreamSynchronize(s));
     } else {
         st.hub_cbase.release();
@@ -1604,7 +1687,9 @@ static void async_chunks(Context &ctx, Graph &g, SsspState &st) {
 }
 
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase, int force,
-             int *cont) {
+             int *cont, int32_t *bfs_levels) {
+    if (bfs_levels && (phase != LOOP_ALL || ctx.persist))
+        fail(MB_ERR_INVALID, "asynchronous BFS: whole runs without the persistent grid only");
     st.ensure(g);
     SsspArgs a;
     a.f = st.frontier_args(g, ctx.model(MB_MODEL_SSSP));
@@ -1627,28 +1712,33 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
     // asynchronous relaxation: the tunable, else on unless the near-far
-    // buckets or the persistent grid were asked for
-    // (fixed policy only: the other policies choose every superstep's schedule)
+    // buckets or the persistent grid were asked for (fixed policy only: the
+    // other policies choose every superstep's schedule; non-negative weights
+    // only: with a negative or NaN weight the BSP loop's superstep cap is
+    // what ends a run).  A BFS run (bfs_levels) is always asynchronous, with
+    // every weight 1 and a threshold step in hops.
+    const bool unit = bfs_levels != nullptr;
     const int64_t t_async = ctx.tunable[MB_TUNE_SSSP_ASYNC];
-    // (fixed policy only: the other policies choose every superstep's
-    // schedule; non-negative weights only: with a negative or NaN weight the
-    // BSP loop's superstep cap is what ends a run)
     const int32_t async =
-        ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
-            ? 0
-            : (t_async >= 0 ? (int32_t)t_async
-                            : (kAsyncDefault && delta == 0.f && !ctx.persist ? 1 : 0));
-    const float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
-                                                                     : st.async_delta;
+        unit ? 1
+             : (ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
+                    ? 0
+                    : (t_async >= 0 ? (int32_t)t_async
+                                    : (kAsyncDefault && delta == 0.f && !ctx.persist ? 1 : 0)));
+    float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
+                                                               : st.async_delta;
+    if (unit)
+        async_delta = ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] : 1.f;
     if (async) async_chunks(ctx, g, st);
     const int64_t nchunks = st.nchunks > 0 ? st.nchunks : 0;
+    a.nc32 = nchunks ? st.nc32 : 0;
     a.adirty = nchunks ? st.adirty.as<uint32_t>() : a.nbm;
-    a.WA = ((int64_t)g.V + nchunks + 31) / 32;
+    a.WA = ((int64_t)g.V + 32 * (int64_t)a.nc32 + 31) / 32;
     a.hub_cbase = st.hub_cbase.as<int32_t>();
     a.chunk_src = st.chunk_src.as<int32_t>();
     a.chunk_rs = st.chunk_rs.as<int32_t>();
     if (phase == LOOP_ALL)
-        upload_params(ctx, st.ctrl.p, source, delta, sssp_bm_push_min(ctx, g), async, async_delta);
+        upload_params(ctx, st.ctrl.p, source, unit ? 0.f : delta, sssp_bm_push_min(ctx, g), async, async_delta);
     if (phase == LOOP_BEGIN) {  // a stepped run: one superstep per call (no persistent kernels)
         const bool tail = ctx.tail, persist = ctx.persist;
         ctx.tail = ctx.persist = false;
@@ -1662,11 +1752,11 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     const int grid_vtx = ctx.num_sms * ctx.blocks_per_sm(MB_TUNE_VERTEX_BLOCKS_PER_SM, 8);
     const int grid_edge = grid_vtx;
     const int persist_grid = persistent_grid_size(ctx, (const void *)k_persist, kPushThreads);
+    const void *async_kernel = unit ? (const void *)k_sssp_async<true> : (const void *)k_sssp_async<false>;
     int async_grid = 0;
     {
         int per_sm = 0;
-        MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_sssp_async,
-                                                              kAsyncThreads, 0));
+        MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, async_kernel, kAsyncThreads, 0));
         if (per_sm < 1) fail(MB_ERR_UNSUPPORTED, "asynchronous SSSP kernel does not fit on an SM");
         per_sm = std::min(per_sm, 8);
         if (ctx.tunable[MB_TUNE_ASYNC_BLOCKS_PER_SM] > 0)
@@ -1708,7 +1798,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
             return;
         }
         if (branch == kBranchAsync) {
-            launch_cooperative((const void *)k_sssp_async, async_grid, kAsyncThreads, s, a, sp.cap);
+            launch_cooperative(async_kernel, async_grid, kAsyncThreads, s, a, sp.cap);
             return;
         }
         if (branch == kBranchPushSmall) {
@@ -1772,6 +1862,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     };
     sp.epilogue = [&](cudaStream_t s) {
         k_stats<<<ctx.num_sms * 4, 256, 0, s>>>(a);
+        if (unit) k_dist_to_level<<<grid_vtx, 256, 0, s>>>(a, bfs_levels);
         MB_CHECK_LAUNCH();
     };
     run_loop(ctx, sp, stats, phase, force, cont);

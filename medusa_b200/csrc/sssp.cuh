@@ -36,10 +36,11 @@ struct AsyncState {
 struct SsspState : FrontierState {
     DevBuf dist, stamp, msg, far[2], farbm, nbm, dprev, as;
     // hub chunks of the asynchronous kernel, made on its first run on the
-    // graph (nchunks < 0: not yet): dirty bitmap over V + nchunks ids, the
-    // first chunk of each hub, each chunk's hub and first out-edge
+    // graph (nchunks < 0: not yet): dirty bitmap over V + 32 * nc32 ids, the
+    // first chunk of each hub, each chunk position's hub and first out-edge
     DevBuf adirty, hub_cbase, chunk_src, chunk_rs;
     int64_t nchunks = -1;
+    int32_t nc32 = 0;  // chunk c sits at id V + (c % 32) * nc32 + c / 32
     float default_delta = 0.f;
     float async_delta = 0.f;
     bool weights_ok = true;  // no negative or NaN weight (the asynchronous kernel needs it)
@@ -63,6 +64,7 @@ struct SsspState : FrontierState {
         chunk_src.release();
         chunk_rs.release();
         nchunks = -1;
+        nc32 = 0;
     }
     void ensure(const Graph &g) {
         if (ensure_frontier(g)) {
@@ -99,7 +101,10 @@ uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g);
 // One SSSP from `source`; distances are left in st.dist (device).
 // phase / force / cont: a run driven one superstep at a time (LoopPhase,
 // engine.cuh); the defaults run it whole.
+// bfs_levels (device, V entries): instead a BFS from `source` by the
+// asynchronous kernel with every weight 1 (whole runs only; the state should
+// then serve BFS runs only, so that its loop graph stays the unit-weight one).
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase = 0,
-             int force = -1, int *cont = nullptr);
+             int force = -1, int *cont = nullptr, int32_t *bfs_levels = nullptr);
 
 }  // namespace mb

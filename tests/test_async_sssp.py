@@ -51,7 +51,7 @@ def test_async_sssp_matches_reference(actx, name):
 @pytest.mark.parametrize("seed", [9, 10])
 def test_async_sssp_hub_chunks(actx, api, seed):
     """Skewed R-MAT (0.57, 0.19, 0.19) with hubs of several thousand
-    out-edges: a hub's edges are relaxed as 1024-edge chunks by many warps."""
+    out-edges: a hub's edges are relaxed as 128-edge chunks by many warps."""
     p = api.rmat_params(14, 1 << 20, 0.57, 0.19, 0.19, seed=seed, wmin=1, wmax=1000)
     V, s, d, w = api.generate_edges_host(p)
     assert np.bincount(s, minlength=V).max() > 4 * 1024
@@ -72,8 +72,8 @@ def test_async_sssp_hub_chunks(actx, api, seed):
 
 
 def test_async_sssp_star_hub_and_isolated_source(actx, api):
-    """One vertex with 5000 out-edges (five chunks), a chain behind it, and
-    a source with no out-edges (nothing to relax)."""
+    """One vertex with 5000 out-edges (40 chunks), a chain behind it, and a
+    source with no out-edges (nothing to relax)."""
     rng = np.random.default_rng(3)
     V = 7000
     src = np.concatenate([np.zeros(5000, np.int32), np.arange(5000, 6998, dtype=np.int32)])
@@ -111,8 +111,8 @@ def test_async_sssp_negative_weight_takes_the_bsp_loop(gpu_ctx, api):
 @pytest.mark.parametrize("which", ["c2_rmat", "c3_grid"])
 def test_async_sssp_full_size_equals_bsp(gpu_ctx, api, which):
     """C2 (R-MAT 2^20 / 2^24) and C3 (1448^2 grid): the asynchronous kernel
-    and the BSP supersteps give the same distances bit for bit, and the
-    asynchronous one relaxes fewer edges."""
+    and the BSP supersteps give the same distances bit for bit; with a
+    threshold step of 100 the asynchronous one relaxes fewer edges."""
     if which == "c2_rmat":
         p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
     else:
@@ -122,10 +122,56 @@ def test_async_sssp_full_size_equals_bsp(gpu_ctx, api, which):
         gpu_ctx.set_tunable("sssp_async", 0)
         ref, st0 = g.sssp([0])
         gpu_ctx.set_tunable("sssp_async", 1)
-        got, st1 = g.sssp([0])
-        np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
-        assert st1["edges_traversed"] == st0["edges_traversed"]
+        for delta in (-1, 100):
+            gpu_ctx.set_tunable("async_delta", delta)
+            got, st1 = g.sssp([0])
+            np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
+            assert st1["edges_traversed"] == st0["edges_traversed"]
         assert st1["edges_scanned"] < st0["edges_scanned"]
     finally:
         gpu_ctx.set_tunable("sssp_async", -1)
+        gpu_ctx.set_tunable("async_delta", -1)
+        g.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_async_bfs_matches_reference(gpu_ctx, api, name):
+    """MB_TUNE_BFS_ASYNC: BFS as the asynchronous kernel with every weight 1
+    (levels are hop distances, exact in float): the reference's levels for
+    every threshold step, both loop modes."""
+    c = load_golden(name)
+    g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        gpu_ctx.set_tunable("bfs_async", 1)
+        for capture in (True, False):
+            gpu_ctx.set_graph_capture(capture)
+            for delta in (-1, 2, 1 << 20):
+                gpu_ctx.set_tunable("bfs_async_delta", delta)
+                for i, s in enumerate(c["sources"]):
+                    lv, st = g.bfs([int(s)])
+                    np.testing.assert_array_equal(lv[0], c["bfs_level"][i],
+                                                  err_msg="delta %d source %d" % (delta, s))
+    finally:
+        for k in ("bfs_async", "bfs_async_delta"):
+            gpu_ctx.set_tunable(k, -1)
+        gpu_ctx.set_graph_capture(True)
+        g.close()
+
+
+@pytest.mark.parametrize("which", ["c2_rmat", "c3_grid"])
+def test_async_bfs_full_size_equals_bsp(gpu_ctx, api, which):
+    if which == "c2_rmat":
+        p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
+    else:
+        p = api.grid_params(1448, 1448, 0.1, 0.005, seed=1, wmin=1, wmax=100)
+    g = gpu_ctx.generate(p)
+    try:
+        ref, st0 = g.bfs([0])
+        gpu_ctx.set_tunable("bfs_async", 1)
+        got, st1 = g.bfs([0])
+        np.testing.assert_array_equal(got, ref)
+        assert st1["edges_traversed"] == st0["edges_traversed"]
+        assert st1["vertices_reached"] == st0["vertices_reached"]
+    finally:
+        gpu_ctx.set_tunable("bfs_async", -1)
         g.close()
