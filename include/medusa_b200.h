@@ -386,7 +386,12 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                levels */
 #define MB_TUNE_BFS_ASYNC_DELTA 21 /* threshold step of the asynchronous BFS, in hops
                                      (default 1: every vertex relaxed once) */
-#define MB_NUM_TUNABLES 22
+#define MB_TUNE_ASYNC_BELOW 22 /* > 0: the asynchronous SSSP (when on) takes over only
+                                 once the frontier, after reaching this many out-edges,
+                                 has fewer -- the large supersteps run as BSP pushes and
+                                 the long tail of small ones as one asynchronous launch;
+                                 0 or -1 (the default): from the first superstep */
+#define MB_NUM_TUNABLES 23
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

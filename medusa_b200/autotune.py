@@ -59,28 +59,62 @@ def tune(ctx, run, space, reps=3, passes=1):
     return best, table
 
 
+def tune_joint(ctx, run, names, candidates, reps=3):
+    """Try each tuple of `candidates` for the tunables `names` together (for
+    settings that only matter jointly, such as a kernel switch and its
+    parameter); leaves the fastest set.  Returns (best {name: value}, table)."""
+    best = tuple(_get(ctx, n) for n in names)
+    best_ms = _median_ms(run, reps)
+    table = [(dict(zip(names, best)), best_ms)]
+    for cand in candidates:
+        if tuple(cand) == best:
+            continue
+        for n, v in zip(names, cand):
+            _set(ctx, n, v)
+        ms = _median_ms(run, reps)
+        table.append((dict(zip(names, cand)), ms))
+        if ms < best_ms:
+            best_ms, best = ms, tuple(cand)
+    for n, v in zip(names, best):
+        _set(ctx, n, v)
+    return dict(zip(names, best)), table
+
+
+# (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA) and (MB_TUNE_BFS_ASYNC,
+# MB_TUNE_BFS_ASYNC_DELTA) pairs tried together
+SSSP_ASYNC_PAIRS = [(-1, -1), (0, -1)] + [(1, d) for d in ASYNC_DELTAS]
+BFS_ASYNC_PAIRS = [(-1, -1), (1, -1), (1, 2), (1, 4), (1, 8)]
+
+
 def tune_sssp(ctx, g, source=0, reps=3):
     """Asynchronous kernel on or off and its threshold step and grid, then
     the bitmap-output push threshold and push grid for SSSP on graph g."""
     E = max(int(g.E), 1)
-    space = {"sssp_async": [-1, 0, 1],
-             "async_delta": ASYNC_DELTAS,
-             "async_blocks_per_sm": [-1, 2, 3],
+    run = lambda: g.sssp([source])[1]
+    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta"), SSSP_ASYNC_PAIRS, reps)
+    space = {"async_blocks_per_sm": [-1, 2, 3],
              "sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "bulk_stage": [-1, 1]}
-    return tune(ctx, lambda: g.sssp([source])[1], space, reps)
+    b2, t2 = tune(ctx, run, space, reps)
+    best.update(b2)
+    return best, table + t2
 
 
 def tune_bfs(ctx, g, source=0, reps=3):
-    """Persistent-tail size and the push / per-vertex grids for BFS on g."""
+    """Asynchronous BFS on or off and its threshold step, the persistent-tail
+    size and the push / per-vertex grids for BFS on g."""
+    run = lambda: g.bfs([source])[1]
+    best, table = tune_joint(ctx, run, ("bfs_async", "bfs_async_delta"), BFS_ASYNC_PAIRS, reps)
     space = {"tail_edges": [-1, 0, 2048, 4096, 6144],
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
              "vertex_blocks_per_sm": [-1, 4, 12, 16],
              "bfs_alpha": [-1, 0, 4, 60],
              "bfs_beta": [-1, 5, 80],
              "bfs_gamma": [-1, 0, 64]}
-    return tune(ctx, lambda: g.bfs([source])[1], space, reps)
+    b2, t2 = tune(ctx, run, space, reps)
+    best.update(b2)
+    return best, table + t2
 
 
 def tune_traversals(ctx, g, source=0, reps=3):
@@ -93,9 +127,11 @@ def tune_traversals(ctx, g, source=0, reps=3):
         ss = g.sssp([source])[1]
         return {"device_ms": sb["device_ms"] + ss["device_ms"]}
 
-    space = {"sssp_async": [-1, 0, 1],
-             "async_delta": ASYNC_DELTAS,
-             "async_blocks_per_sm": [-1, 2, 3],
+    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta"), SSSP_ASYNC_PAIRS, reps)
+    b2, t2 = tune_joint(ctx, run, ("bfs_async", "bfs_async_delta"), BFS_ASYNC_PAIRS, reps)
+    best.update(b2)
+    table += t2
+    space = {"async_blocks_per_sm": [-1, 2, 3],
              "sssp_bm_push_min": sorted({-1, 0, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "sssp_delta": [0.0, -1.0, 100.0, 1000.0, 10000.0],
              "tail_edges": [-1, 0, 2048, 4096],
@@ -105,7 +141,9 @@ def tune_traversals(ctx, g, source=0, reps=3):
              "bfs_beta": [-1, 5, 80],
              "bfs_gamma": [-1, 0, 64],
              "bulk_stage": [-1, 1]}
-    return tune(ctx, run, space, reps)
+    b3, t3 = tune(ctx, run, space, reps)
+    best.update(b3)
+    return best, table + t3
 
 
 def tune_pagerank(ctx, g, iters=10, reps=3, out=None):

@@ -5,7 +5,7 @@
 namespace mb {
 
 void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, uint32_t bm_push_min,
-                   int32_t sssp_async, float async_delta) {
+                   int32_t sssp_async, float async_delta, uint32_t async_below) {
     static_assert(sizeof(RunParams) <= Context::kCtrlOff, "params staging too small");
     static_assert(sizeof(Ctrl) <= Context::kSmallBytes - Context::kCtrlOff, "ctrl readback too small");
     RunParams *p = (RunParams *)(ctx.pinned_small + Context::kParamsOff);
@@ -22,6 +22,7 @@ void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta, ui
     p->bm_push_min = bm_push_min;
     p->sssp_async = sssp_async;
     p->async_delta = async_delta;
+    p->async_below = async_below;
     p->bfs_alpha = ctx.tunable[MB_TUNE_BFS_ALPHA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_ALPHA] : 15;
     p->bfs_beta = ctx.tunable[MB_TUNE_BFS_BETA] > 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_BETA] : 20;
     p->bfs_gamma = ctx.tunable[MB_TUNE_BFS_GAMMA] >= 0 ? (int32_t)ctx.tunable[MB_TUNE_BFS_GAMMA] : kBfsGammaDefault;

@@ -95,6 +95,8 @@ struct Ctrl {
     uint32_t bar_count;       // persistent-grid barrier: arrivals over the run (top bit: gave up)
     uint32_t pad_bar;
     int32_t persist_go;       // persistent grid: run another superstep
+    int32_t peaked;           // SSSP: a frontier reached p.async_below out-edges
+    int32_t pad_peaked;
 };
 
 // Frontier buffers and graph shape every engine kernel sees.
@@ -158,7 +160,9 @@ __host__ __device__ inline bool persist_supported(int s) {
 
 __device__ inline int route(const Ctrl *c, int s) {
     if (c->p.persist && persist_supported(s)) return kBranchPersist;
-    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.sssp_async) return kBranchAsync;
+    if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.sssp_async &&
+        (c->p.async_below == 0 || (c->peaked && c->front_m < c->p.async_below)))
+        return kBranchAsync;
     if (s == MB_SCHED_PUSH_EDGE_QUEUE && c->mode == FMT_QUEUE && c->p.tail &&
         c->front_n <= kTailEntries && c->front_m <= c->p.tail_edges)
         return kBranchTail;
@@ -195,6 +199,7 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     }
     c->front_n = n;
     c->front_m = m;
+    if (c->p.async_below && m >= c->p.async_below) c->peaked = 1;
     if (c->p.max_step >= 0 && c->step > c->p.max_step) {  // trace collection: stop here
         c->done = 1;
         return;

@@ -281,7 +281,12 @@ int32_t collect_traces(Context &ctx, Graph &g, BfsState &bst, SsspState &sst, Ms
     const bool graphs = ctx.use_graphs, tail = ctx.tail, persist = ctx.persist,
                tracing = ctx.tracing, rtf = ctx.replay_then_fixed;
     const std::vector<int8_t> replay = ctx.replay;
+    // the traces are of BSP supersteps: the asynchronous SSSP kernel (which
+    // runs a whole traversal as one superstep) stays off while collecting
+    const int64_t async = ctx.tunable[MB_TUNE_SSSP_ASYNC];
+    ctx.tunable[MB_TUNE_SSSP_ASYNC] = 0;
     auto restore = [&] {
+        ctx.tunable[MB_TUNE_SSSP_ASYNC] = async;
         ctx.schedule_policy = policy;
         ctx.fixed_schedule = fixed;
         ctx.max_step = max_step;

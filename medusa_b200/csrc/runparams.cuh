@@ -36,13 +36,15 @@ struct RunParams {
     uint32_t small_push_max;    // schedule 0 frontiers up to this many out-edges use the small grid
     int32_t sssp_async;         // SSSP: schedule 0 on a queue frontier runs the asynchronous kernel
     float async_delta;          // its threshold step (0: no threshold)
-    uint32_t pad_;
+    uint32_t async_below;       // > 0: ... only once the frontier, after reaching this many
+                                // out-edges, has fewer (the big supersteps stay BSP)
     int8_t replay[kMaxReplay];  // MB_POLICY_ORACLE_BEST: schedule per superstep
 };
 
 // Write this run's RunParams (policy, forced schedule, replay list, source,
 // SSSP bucket width) to a control block whose first member is RunParams.
 void upload_params(Context &ctx, void *ctrl_dev, int32_t source, float delta = 0.f,
-                   uint32_t bm_push_min = 0, int32_t sssp_async = 0, float async_delta = 0.f);
+                   uint32_t bm_push_min = 0, int32_t sssp_async = 0, float async_delta = 0.f,
+                   uint32_t async_below = 0);
 
 }  // namespace mb

@@ -1120,13 +1120,13 @@ __device__ __forceinline__ bool async_finished(AsyncState *S) {
 }
 
 #ifndef MB_ASYNC_CHUNK
-#define MB_ASYNC_CHUNK 128
+#define MB_ASYNC_CHUNK 64
 #endif
 constexpr int32_t kAsyncChunk = MB_ASYNC_CHUNK;
-// MB_TUNE_SSSP_ASYNC = -1: the asynchronous kernel unless near-far buckets
-// or the persistent grid were asked for
-constexpr bool kAsyncDefault = false;
-
+// Default threshold step of the asynchronous BFS, in hops: 4 measured best
+// on the 1448^2 grid (1 -> 94 phases, 1.53 ms; 4 -> 25 phases, 0.85 ms; every
+// vertex still relaxed once).
+constexpr float kBfsAsyncDelta = 4.f;
 // Relax what this warp claimed: lane l holds one dirty id (or v < 0) -- a
 // vertex (its out-edges), a hub (the bits of its chunks) or a chunk (its
 // out-edges).  Every item (an edge, or a chunk bit) may set one dirty bit.
@@ -1136,7 +1136,7 @@ constexpr bool kAsyncDefault = false;
 // kAsyncNext, *nn of them, warp-uniform), and the warp claims and relaxes it
 // next itself instead of leaving it to its owner's next pass.
 #ifndef MB_ASYNC_LOCAL
-#define MB_ASYNC_LOCAL 0
+#define MB_ASYNC_LOCAL 1
 #endif
 constexpr uint32_t kAsyncNext = 64;
 
@@ -1524,6 +1524,7 @@ __global__ void k_sssp_init(SsspArgs a) {
         c->fcur = 0;
         c->splits = 0;
         c->bar_count = 0;
+        c->peaked = 0;
         c->q[1] = 0ull;
         a.as->pt.v = 0ull;
         a.as->mn[0].v = kInfBits;
@@ -1647,7 +1648,7 @@ float sssp_default_delta(const Graph &g, double mean_w) {
 float sssp_async_delta(const Graph &g, double mean_w) {
     if (g.E == 0) return 0.f;
     const double mean_deg = (double)g.E / (double)g.V;
-    return (float)std::max(mean_w, mean_w * 8.0 / std::max(1.0, mean_deg));
+    return (float)std::max(mean_w, mean_w * 24.0 / std::max(1.0, mean_deg));
 }
 
 // Hub chunk tables of the asynchronous kernel for graph g (once).
@@ -1724,12 +1725,16 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
              : (ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
                     ? 0
                     : (t_async >= 0 ? (int32_t)t_async
-                                    : (kAsyncDefault && delta == 0.f && !ctx.persist ? 1 : 0)));
+                                    : (async_by_default(g) && delta == 0.f && !ctx.persist ? 1 : 0)));
     float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
                                                                : st.async_delta;
     if (unit)
-        async_delta = ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] : 1.f;
-    if (async) async_chunks(ctx, g, st);
+        async_delta = ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA]
+                                                                : kBfsAsyncDelta;
+    // made on the first run whether or not it is asynchronous: the pointers
+    // below are captured in the run's loop graph, which must not change
+    // when a later run switches the kernel on
+    async_chunks(ctx, g, st);
     const int64_t nchunks = st.nchunks > 0 ? st.nchunks : 0;
     a.nc32 = nchunks ? st.nc32 : 0;
     a.adirty = nchunks ? st.adirty.as<uint32_t>() : a.nbm;
@@ -1737,8 +1742,11 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.hub_cbase = st.hub_cbase.as<int32_t>();
     a.chunk_src = st.chunk_src.as<int32_t>();
     a.chunk_rs = st.chunk_rs.as<int32_t>();
+    const uint32_t async_below =
+        unit ? 0u : (uint32_t)std::min<int64_t>(std::max<int64_t>(ctx.tunable[MB_TUNE_ASYNC_BELOW], 0), 0xffffffffll);
     if (phase == LOOP_ALL)
-        upload_params(ctx, st.ctrl.p, source, unit ? 0.f : delta, sssp_bm_push_min(ctx, g), async, async_delta);
+        upload_params(ctx, st.ctrl.p, source, unit ? 0.f : delta, sssp_bm_push_min(ctx, g), async, async_delta,
+                      async_below);
     if (phase == LOOP_BEGIN) {  // a stepped run: one superstep per call (no persistent kernels)
         const bool tail = ctx.tail, persist = ctx.persist;
         ctx.tail = ctx.persist = false;

@@ -41,3 +41,21 @@ def test_a_worse_candidate_is_never_kept():
     ctx.t["a"] = 4
     best, _ = autotune.tune(ctx, lambda: cost(ctx), {"a": [-1, 0, 100]}, reps=3)
     assert best["a"] == 4 and ctx.t["a"] == 4
+
+
+def test_joint_search_tries_a_switch_with_each_of_its_parameters():
+    """A kernel switch that only pays with the right parameter: coordinate
+    descent one tunable at a time would keep the switch off (off beats on at
+    the default parameter); the joint search finds (on, 200)."""
+    ctx = FakeCtx()
+
+    def run():
+        on, d = ctx.t["a"], ctx.t["b"]
+        if on != 1:
+            return {"device_ms": 5.0}
+        return {"device_ms": 7.0 if d == -1 else 1.0 + abs(d - 200) / 100}
+
+    best, table = autotune.tune_joint(ctx, run, ("a", "b"), [(-1, -1), (1, -1), (1, 50), (1, 200), (1, 800)],
+                                      reps=1)
+    assert best == {"a": 1, "b": 200} and ctx.t == {"a": 1, "b": 200}
+    assert len(table) == 5  # the current setting, then the four others
