@@ -83,6 +83,10 @@ def tune_joint(ctx, run, names, candidates, reps=3):
 # (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA) and (MB_TUNE_BFS_ASYNC,
 # MB_TUNE_BFS_ASYNC_DELTA) pairs tried together
 SSSP_ASYNC_PAIRS = [(-1, -1), (0, -1)] + [(1, d) for d in ASYNC_DELTAS]
+# (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA, MB_TUNE_ASYNC_BELOW): the BSP
+# supersteps while the frontier is large, then the asynchronous kernel
+SSSP_ASYNC_TRIPLES = [(-1, -1, -1), (0, -1, -1)] + [(1, d, -1) for d in ASYNC_DELTAS] + \
+    [(1, 0, 1 << b) for b in (18, 20, 22)]
 BFS_ASYNC_PAIRS = [(-1, -1), (1, -1), (1, 2), (1, 4), (1, 8)]
 
 
@@ -91,7 +95,7 @@ def tune_sssp(ctx, g, source=0, reps=3):
     the bitmap-output push threshold and push grid for SSSP on graph g."""
     E = max(int(g.E), 1)
     run = lambda: g.sssp([source])[1]
-    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta"), SSSP_ASYNC_PAIRS, reps)
+    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta", "async_below"), SSSP_ASYNC_TRIPLES, reps)
     space = {"async_blocks_per_sm": [-1, 2, 3],
              "sssp_bm_push_min": sorted({-1, 0, 1 << 16, 1 << 18, 1 << 20, 1 << 22, E // 8, E // 32}),
              "push_blocks_per_sm": [-1, 4, 6, 12, 16],
@@ -127,7 +131,7 @@ def tune_traversals(ctx, g, source=0, reps=3):
         ss = g.sssp([source])[1]
         return {"device_ms": sb["device_ms"] + ss["device_ms"]}
 
-    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta"), SSSP_ASYNC_PAIRS, reps)
+    best, table = tune_joint(ctx, run, ("sssp_async", "async_delta", "async_below"), SSSP_ASYNC_TRIPLES, reps)
     b2, t2 = tune_joint(ctx, run, ("bfs_async", "bfs_async_delta"), BFS_ASYNC_PAIRS, reps)
     best.update(b2)
     table += t2

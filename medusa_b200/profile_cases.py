@@ -17,7 +17,8 @@ library's, the reference's).  Prints one line per repetition with
 the library's device time.  --hostloop runs the host-driven loop (kernels in
 conditional-node graphs are invisible to ncu); --trace prints each superstep
 of the last repetition (BFS 8 B per frontier out-edge + 20 B per frontier
-vertex, SSSP 12 + 20, as algorithmic bytes)."""
+vertex, SSSP 12 + 20, as algorithmic bytes).  --set NAME=VALUE sets a
+tunable (medusa_b200.api.TUNABLES) before the runs; repeatable."""
 import argparse
 import sys
 
@@ -52,10 +53,15 @@ def main(argv=None):
     ap.add_argument("--trace", action="store_true",
                     help="print every superstep (branch, frontier, CUDA-event ms) of the last rep")
     ap.add_argument("--pr-order", choices=["fixed", "reference"], default=None)
+    ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                    help="a tunable for the runs (e.g. sssp_async=1)")
     args = ap.parse_args(argv)
     ctx = api.Context(0)
     if args.hostloop:
         ctx.set_graph_capture(False)
+    for kv in args.set:
+        name, value = kv.split("=", 1)
+        ctx.set_tunable(name, int(value))
     if args.pr_order:
         ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED if args.pr_order == "fixed"
                                else api.MB_PR_ORDER_REFERENCE)
