@@ -124,6 +124,13 @@ struct PushSmem {
 #ifndef MB_SSSP_SNAPSHOT
 #define MB_SSSP_SNAPSHOT 0
 #endif
+// The bitmap-output push's neighbour-distance check through L1 (a cached
+// copy can only be higher than the current distance -- distances only drop
+// -- so a stale hit costs a spurious atomicMin and frontier bit, never a
+// missed relaxation).  Measurement switch.
+#ifndef MB_SSSP_DIST_L1
+#define MB_SSSP_DIST_L1 0
+#endif
 // 128-bit col/wt loads in the edge-balanced push (needs 4 edges per thread:
 // MB_TILE_EDGES=1024).  Measured against the scalar loads; off.
 #ifndef MB_PUSH_VEC4
@@ -275,7 +282,8 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
         }
 #endif
 #pragma unroll
-        for (int r = 0; r < kTileItems; r++) dv[r] = ok[r] ? ld_dist(a, v[r]) : 0.f;
+        for (int r = 0; r < kTileItems; r++)
+            dv[r] = ok[r] ? ((MB_SSSP_DIST_L1 && kBmOut) ? __ldca(&a.dist[v[r]]) : ld_dist(a, v[r])) : 0.f;
         if (kBmOut) {
 #pragma unroll
             for (int r = 0; r < kTileItems; r++) {
