@@ -370,7 +370,9 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 asynchronous cooperative launch (no superstep barriers:
                                 warps relax the dirty vertices below a distance threshold
                                 that rises by MB_TUNE_ASYNC_DELTA whenever every warp is
-                                idle); 0 (the default) the BSP supersteps.  Under
+                                idle); 0 the BSP supersteps; default: 1 on graphs whose
+                                largest out-degree is at most 64 (no hubs), unless a
+                                near-far width or the persistent grid is set.  Under
                                 MB_POLICY_FIXED only (the other policies pick every
                                 superstep), and only on graphs without a negative or NaN
                                 weight.  Identical distances */
@@ -381,11 +383,12 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                          SSSP (default: as many as fit, at most 8) */
 #define MB_TUNE_BFS_ASYNC 20 /* BFS: 1 runs a single-source BFS under MB_POLICY_FIXED as
                                the asynchronous kernel with every weight 1 (levels are
-                               hop distances; one cooperative launch); 0 (the default)
-                               the direction-optimising BSP supersteps.  Identical
-                               levels */
+                               hop distances; one cooperative launch); 0 the
+                               direction-optimising BSP supersteps; default: 1 on graphs
+                               without hubs (largest out-degree <= 64) of at most 6
+                               edges per vertex.  Identical levels */
 #define MB_TUNE_BFS_ASYNC_DELTA 21 /* threshold step of the asynchronous BFS, in hops
-                                     (default 1: every vertex relaxed once) */
+                                     (default 4) */
 #define MB_TUNE_ASYNC_BELOW 22 /* > 0: the asynchronous SSSP (when on) takes over only
                                  once the frontier, after reaching this many out-edges,
                                  has fewer -- the large supersteps run as BSP pushes and

@@ -1733,7 +1733,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
              : (ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
                     ? 0
                     : (t_async >= 0 ? (int32_t)t_async
-                                    : (async_by_default(g) && delta == 0.f && !ctx.persist ? 1 : 0)));
+                                    : (async_by_default(g, false) && delta == 0.f && !ctx.persist ? 1 : 0)));
     float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
                                                                : st.async_delta;
     if (unit)

@@ -93,14 +93,18 @@ struct SsspState : FrontierState {
     }
 };
 
-// MB_TUNE_SSSP_ASYNC / MB_TUNE_BFS_ASYNC = -1: the asynchronous kernel on
-// graphs of low degree without hubs (mean out-degree <= 8, largest <= 64:
-// road- and grid-like graphs, whose hundreds of small supersteps it folds
-// into one launch), unless near-far buckets or the persistent grid were
-// asked for.  Measured on B200: the 1448^2 grid's SSSP 2.5 -> 1.2 ms and BFS
-// 1.34 -> 0.85 ms; on R-MAT graphs the BSP supersteps are as fast or faster.
-inline bool async_by_default(const Graph &g) {
-    return g.V > 0 && g.max_outdeg <= 64 && (double)g.E <= 8.0 * (double)g.V;
+// MB_TUNE_SSSP_ASYNC = -1: the asynchronous kernel on graphs without hubs
+// (largest out-degree <= 64), unless near-far buckets or the persistent grid
+// were asked for.  MB_TUNE_BFS_ASYNC = -1: the same on graphs that are also
+// sparse (mean out-degree <= 6).  Measured on B200 (ms, BSP -> asynchronous):
+// SSSP on the 1448^2 grid 2.5 -> 1.2, uniform 2^20 / 2^24 1.19 -> 0.74,
+// uniform 2^18 / 2^22 0.64 -> 0.43; BFS on the grid 1.34 -> 0.72, uniform
+// 2^20 with 4 edges per vertex 0.31 -> 0.27, but uniform 2^20 / 2^24 0.21 ->
+// 0.29 (the direction-optimising pulls skip most edges).  On R-MAT graphs
+// (hubs) the BSP supersteps are as fast or faster for both.
+inline bool async_by_default(const Graph &g, bool bfs) {
+    if (g.V <= 0 || g.max_outdeg > 64) return false;
+    return !bfs || (double)g.E <= 6.0 * (double)g.V;
 }
 
 // Frontier out-edges from which schedule 0 writes a next-frontier bitmap
