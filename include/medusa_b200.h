@@ -373,15 +373,18 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 idle); 0 the BSP supersteps; default: 1 on graphs whose
                                 largest out-degree is at most 64 (no hubs), unless a
                                 near-far width or the persistent grid is set.  Under
-                                MB_POLICY_FIXED only (the other policies pick every
-                                superstep), and only on graphs without a negative or NaN
-                                weight.  Identical distances */
+                                MB_POLICY_FIXED and MB_POLICY_LEARNED (it is how schedule
+                                0 runs the rest of a traversal; the forced and replay
+                                policies name every superstep's schedule), and only on
+                                graphs without a negative or NaN weight.  Identical
+                                distances */
 #define MB_TUNE_ASYNC_DELTA 18 /* width by which the asynchronous SSSP's threshold rises
                                  (default 8 x mean weight / mean out-degree, at least the
                                  mean weight; 0: no threshold) */
 #define MB_TUNE_ASYNC_BLOCKS_PER_SM 19 /* CTAs of 256 threads per SM of the asynchronous
                                          SSSP (default: as many as fit, at most 8) */
-#define MB_TUNE_BFS_ASYNC 20 /* BFS: 1 runs a single-source BFS under MB_POLICY_FIXED as
+#define MB_TUNE_BFS_ASYNC 20 /* BFS: 1 runs a single-source BFS (MB_POLICY_FIXED or
+                               MB_POLICY_LEARNED) as
                                the asynchronous kernel with every weight 1 (levels are
                                hop distances; one cooperative launch); 0 the
                                direction-optimising BSP supersteps; default: 1 on graphs

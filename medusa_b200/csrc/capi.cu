@@ -694,7 +694,9 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
         }
         const int64_t t_async = ctx->c.tunable[MB_TUNE_BFS_ASYNC];
         const bool bfs_async = (t_async > 0 || (t_async < 0 && mb::async_by_default(g->g, true))) &&
-                               ctx->c.schedule_policy == MB_POLICY_FIXED && !ctx->c.persist;
+                               (ctx->c.schedule_policy == MB_POLICY_FIXED ||
+                                ctx->c.schedule_policy == MB_POLICY_LEARNED) &&
+                               !ctx->c.persist;
         if (bfs_async) apps(g).bfs.ensure(g->g);
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};

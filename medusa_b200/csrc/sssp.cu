@@ -1721,16 +1721,18 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     // near-far bucket width: the context's, or a per-graph default
     const float delta = ctx.sssp_delta >= 0.f ? ctx.sssp_delta : st.default_delta;
     // asynchronous relaxation: the tunable, else on unless the near-far
-    // buckets or the persistent grid were asked for (fixed policy only: the
-    // other policies choose every superstep's schedule; non-negative weights
-    // only: with a negative or NaN weight the BSP loop's superstep cap is
-    // what ends a run).  A BFS run (bfs_levels) is always asynchronous, with
-    // every weight 1 and a threshold step in hops.
+    // buckets or the persistent grid were asked for (fixed and learned
+    // policies only -- it is how schedule 0 runs the rest of a traversal; the
+    // forced and replay policies name every superstep's schedule;
+    // non-negative weights only: with a negative or NaN weight the BSP
+    // loop's superstep cap is what ends a run).  A BFS run (bfs_levels) is
+    // always asynchronous, with every weight 1 and a threshold step in hops.
     const bool unit = bfs_levels != nullptr;
     const int64_t t_async = ctx.tunable[MB_TUNE_SSSP_ASYNC];
+    const bool policy_ok = ctx.schedule_policy == MB_POLICY_FIXED || ctx.schedule_policy == MB_POLICY_LEARNED;
     const int32_t async =
         unit ? 1
-             : (ctx.schedule_policy != MB_POLICY_FIXED || !st.weights_ok
+             : (!policy_ok || !st.weights_ok
                     ? 0
                     : (t_async >= 0 ? (int32_t)t_async
                                     : (async_by_default(g, false) && delta == 0.f && !ctx.persist ? 1 : 0)));
