@@ -175,3 +175,73 @@ def test_async_bfs_full_size_equals_bsp(gpu_ctx, api, which):
     finally:
         gpu_ctx.set_tunable("bfs_async", -1)
         g.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_hybrid_route_matches_reference(actx, name):
+    """MB_TUNE_ASYNC_BELOW: BSP supersteps while the frontier is large, then
+    the asynchronous kernel for the rest (a threshold of 1 edge: the kernel
+    takes over right after the first frontier with out-edges)."""
+    c = load_golden(name)
+    g = actx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        for below, delta in ((1, 0), (64, -1), (1 << 30, 0)):
+            actx.set_tunable("async_below", below)
+            actx.set_tunable("async_delta", delta)
+            for i, s in enumerate(c["sources"]):
+                d, _ = g.sssp([int(s)])
+                np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32),
+                                              err_msg="below %d source %d" % (below, s))
+    finally:
+        actx.set_tunable("async_below", -1)
+        g.close()
+
+
+def test_hybrid_route_full_size_c2(gpu_ctx, api):
+    """C2 at full size: BSP supersteps until the frontier drops below 2^18 /
+    2^20 out-edges after its peak, then the asynchronous kernel: the BSP
+    loop's distances bit for bit."""
+    p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
+    g = gpu_ctx.generate(p)
+    try:
+        gpu_ctx.set_tunable("sssp_async", 0)
+        ref, st0 = g.sssp([0])
+        gpu_ctx.set_tunable("sssp_async", 1)
+        gpu_ctx.set_tunable("async_delta", 0)
+        for below in (1 << 18, 1 << 20):
+            gpu_ctx.set_tunable("async_below", below)
+            got, st = g.sssp([0])
+            np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
+            assert st["edges_traversed"] == st0["edges_traversed"]
+            assert 1 < st["supersteps"] < st0["supersteps"] + 8
+    finally:
+        for k in ("sssp_async", "async_delta", "async_below"):
+            gpu_ctx.set_tunable(k, -1)
+        g.close()
+
+
+def test_learned_policy_takes_the_asynchronous_route(gpu_ctx, api):
+    """Under the learned policy schedule 0 may run as the asynchronous kernel
+    too (on a hub-free graph, its default), with the fixed rule's distances;
+    under the replay policy it never does (every superstep is named)."""
+    p = api.uniform_params(1 << 14, 1 << 17, seed=5, wmin=1, wmax=1000)
+    V, s, d, w = api.generate_edges_host(p)
+    want, _ = O.sssp(V, s, d, w, 0)
+    g = gpu_ctx.generate(p)
+    try:
+        w0 = np.zeros(api.lib.mb_scheduler_num_params(), np.float32)
+        gpu_ctx.scheduler_set_weights(w0, api.MB_MODEL_SSSP)  # ties: the fixed rule's choice
+        for policy in (api.MB_POLICY_LEARNED, api.MB_POLICY_ORACLE_BEST):
+            if policy == api.MB_POLICY_ORACLE_BEST:
+                gpu_ctx.set_replay([0] * 8)
+            else:
+                gpu_ctx.set_policy(policy)
+            got, st = g.sssp([0])
+            np.testing.assert_array_equal(got[0].view(np.uint32), want.view(np.uint32))
+            if policy == api.MB_POLICY_ORACLE_BEST:
+                assert st["schedule_count"][0] > 3  # one superstep per BSP step
+            else:
+                assert st["schedule_count"][0] == 1  # the whole traversal in one launch
+    finally:
+        gpu_ctx.set_policy(api.MB_POLICY_FIXED)
+        g.close()
