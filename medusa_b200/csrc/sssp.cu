@@ -1219,6 +1219,37 @@ __device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S
 #pragma unroll
         for (int u = 0; u < kAsyncU; u++) dx[u] = ok[u] ? ld_dist(a, x[u]) : 0.f;
         bool keep[kAsyncU];
+#if MB_ASYNC_LOCAL == 2
+        // a vertex that dropped below T is kept by this warp WITHOUT setting
+        // its dirty bit (no publish, no claim back: two L2 round trips less
+        // per hop of a light-edge chain); it counts as set in the work
+        // counters until this warp relaxes it.  The rest are published.
+        bool imp[kAsyncU];
+#pragma unroll
+        for (int u = 0; u < kAsyncU; u++) {
+            imp[u] = false;
+            if (ok[u] && nd[u] < dx[u]) {
+                const unsigned old = atomicMin((unsigned *)&a.dist[x[u]], __float_as_uint(nd[u]));
+                imp[u] = nd[u] < __uint_as_float(old);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kAsyncU; u++) {
+            const bool cand = imp[u] && nd[u] < T;
+            const uint32_t km = __ballot_sync(FULL, cand);
+            const uint32_t pos = *nn + __popc(km & lanemask_lt());
+            keep[u] = cand && pos < kAsyncNext;
+            if (keep[u]) {
+                nxt[pos] = x[u];
+                newly++;
+            }
+            *nn = min(kAsyncNext, *nn + (uint32_t)__popc(km));
+            if (imp[u] && !keep[u]) {
+                const uint32_t bit = 1u << ((x[u] + order) & 31);
+                if (!(atomicOr(&dirty[x[u] >> 5], bit) & bit)) newly++;
+            }
+        }
+#else
 #pragma unroll
         for (int u = 0; u < kAsyncU; u++) {
             keep[u] = false;
@@ -1233,7 +1264,8 @@ __device__ __forceinline__ uint32_t async_relax(const SsspArgs &a, AsyncState *S
                 }
             }
         }
-        if (MB_ASYNC_LOCAL) {
+#endif
+        if (MB_ASYNC_LOCAL == 1) {
 #pragma unroll
             for (int u = 0; u < kAsyncU; u++) {
                 const uint32_t km = __ballot_sync(FULL, keep[u]);
@@ -1398,8 +1430,12 @@ __global__ void __launch_bounds__(kAsyncThreads) k_sssp_async(SsspArgs a, int ca
                     nn -= take;
                     bool got = false;
                     if (x >= 0) {
+#if MB_ASYNC_LOCAL == 2
+                        got = true;  // never published: no claim needed
+#else
                         const uint32_t bit = 1u << (x & 31);
                         got = (atom_and_acquire(&dirty[x >> 5], ~bit) & bit) != 0u;
+#endif
                     }
                     const uint32_t gm = __ballot_sync(FULL, got);
                     if (got) bv[nb + __popc(gm & lanemask_lt())] = x;
