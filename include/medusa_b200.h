@@ -391,7 +391,7 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                without hubs (largest out-degree <= 64) of at most 6
                                edges per vertex.  Identical levels */
 #define MB_TUNE_BFS_ASYNC_DELTA 21 /* threshold step of the asynchronous BFS, in hops
-                                     (default 4) */
+                                     (default 8) */
 #define MB_TUNE_ASYNC_BELOW 22 /* > 0: the asynchronous SSSP (when on) takes over only
                                  once the frontier, after reaching this many out-edges,
                                  has fewer -- the large supersteps run as BSP pushes and
