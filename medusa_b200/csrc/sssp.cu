@@ -43,7 +43,6 @@ struct SsspArgs {
     int32_t *far[2];  // near-far piles (vertices whose distance is >= the threshold)
     uint32_t *farbm;  // membership bitmap of the pile being filled
     uint32_t *nbm;    // next-frontier bitmap of the bitmap-output push (all zero between uses)
-    uint8_t *nbyte;   // the same as one byte per vertex (MB_SSSP_BYTEMAP)
     float *dprev;     // distances before the superstep (the snapshot variant of that push)
     AsyncState *as;   // the asynchronous kernel's counters
     // the asynchronous kernel's dirty bitmap over vertex ids [0, V) and hub
@@ -131,12 +130,6 @@ struct PushSmem {
 // missed relaxation).  Measurement switch.
 #ifndef MB_SSSP_DIST_L1
 #define MB_SSSP_DIST_L1 0
-#endif
-// The bitmap-output push marking the next frontier with a plain byte store
-// per vertex (one byte per vertex, idempotent) instead of an atomicOr on a
-// bitmap word; the compaction then reads bytes.  Measurement switch.
-#ifndef MB_SSSP_BYTEMAP
-#define MB_SSSP_BYTEMAP 0
 #endif
 // 128-bit col/wt loads in the edge-balanced push (needs 4 edges per thread:
 // MB_TILE_EDGES=1024).  Measured against the scalar loads; off.
@@ -298,7 +291,6 @@ __device__ __forceinline__ void work_push_edge_q(const SsspArgs &a, PushSmem &sm
                 if (ok[r] && nd[r] < dv[r]) {
                     atomicMin((unsigned *)&a.dist[v[r]], __float_as_uint(nd[r]));
                     if (nd[r] >= thresh) to_far = true;
-                    else if (MB_SSSP_BYTEMAP) a.nbyte[v[r]] = 1;
                     else atomicOr(&a.nbm[v[r] >> 5], 1u << (v[r] & 31));
                 }
                 far_push(a, c, to_far, v[r]);
@@ -366,14 +358,9 @@ __global__ void __launch_bounds__(kPushThreads) k_nbm2q(SsspArgs a) {
     for (int64_t w0 = (int64_t)blockIdx.x * wpb; w0 < a.f.W; w0 += (int64_t)gridDim.x * wpb) {
         const int64_t w = w0 + (threadIdx.x >> 5);
         const int32_t v = (int32_t)(w * 32 + lane);
-#if MB_SSSP_BYTEMAP
-        const bool in = v < a.f.V && a.nbyte[v];
-        if (in) a.nbyte[v] = 0;
-#else
         const uint32_t word = w < a.f.W ? a.nbm[w] : 0u;
         if (word && lane == 0) a.nbm[w] = 0u;
         const bool in = (word >> lane) & 1u;
-#endif
         uint32_t deg = 0;
         if (in) {
             deg = (uint32_t)a.f.outdeg[v];
@@ -1765,7 +1752,6 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.far[1] = st.far[1].as<int32_t>();
     a.farbm = st.farbm.as<uint32_t>();
     a.nbm = st.nbm.as<uint32_t>();
-    a.nbyte = st.nbyte.as<uint8_t>();
     a.dprev = st.dprev.as<float>();
     a.as = st.as.as<AsyncState>();
     // near-far bucket width: the context's, or a per-graph default
@@ -1846,7 +1832,6 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         MB_CUDA(cudaMemsetAsync(a.stamp, 0xff, sizeof(int32_t) * (size_t)a.f.V, s));
         MB_CUDA(cudaMemsetAsync(a.farbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
         MB_CUDA(cudaMemsetAsync(a.nbm, 0, sizeof(uint32_t) * (size_t)a.f.W, s));
-        if (MB_SSSP_BYTEMAP) MB_CUDA(cudaMemsetAsync(a.nbyte, 0, (size_t)a.f.V, s));
         if (a.adirty != a.nbm) MB_CUDA(cudaMemsetAsync(a.adirty, 0, sizeof(uint32_t) * (size_t)a.WA, s));
         k_sssp_init<<<1, 256, 0, s>>>(a);
         MB_CHECK_LAUNCH();

@@ -34,7 +34,7 @@ struct AsyncState {
 };
 
 struct SsspState : FrontierState {
-    DevBuf dist, stamp, msg, far[2], farbm, nbm, nbyte, dprev, as;
+    DevBuf dist, stamp, msg, far[2], farbm, nbm, dprev, as;
     // hub chunks of the asynchronous kernel, made on its first run on the
     // graph (nchunks < 0: not yet): dirty bitmap over V + 32 * nc32 ids, the
     // first chunk of each hub, each chunk position's hub and first out-edge
@@ -54,7 +54,6 @@ struct SsspState : FrontierState {
         far[1].release();
         farbm.release();
         nbm.release();
-        nbyte.release();
         dprev.release();
         as.release();
         release_chunks();
@@ -81,7 +80,6 @@ struct SsspState : FrontierState {
             far[1].reserve(sizeof(int32_t) * (size_t)g.V);
             farbm.reserve(sizeof(uint32_t) * (size_t)W);
             nbm.reserve(sizeof(uint32_t) * (size_t)W);
-            nbyte.reserve(32 * (size_t)W);  // one byte per vertex (rounded up to whole words)
             dprev.reserve(sizeof(float) * (size_t)g.V);
             as.reserve(sizeof(AsyncState));
             release_chunks();
