@@ -544,7 +544,7 @@ __global__ void k_bfs_init(BfsArgs a) {
 // host side
 
 void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats, int phase, int force,
-             int *cont) {
+             int *cont, const EmitFn *after) {
     st.ensure(g);
     BfsArgs a;
     a.f = st.frontier_args(g, ctx.model(MB_MODEL_BFS));
@@ -630,6 +630,7 @@ void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *sta
         MB_CHECK_LAUNCH();
     };
     sp.epilogue = nullptr;  // reached counts are kept by finish_superstep
+    if (after) sp.after = *after;
     run_loop(ctx, sp, stats, phase, force, cont);
 }
 

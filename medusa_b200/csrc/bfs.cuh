@@ -25,7 +25,8 @@ struct BfsState : FrontierState {
 // One BFS from `source`; levels are left in st.level (device).
 // phase / force / cont: a run driven one superstep at a time (LoopPhase,
 // engine.cuh); the defaults run it whole.
+// after: queued behind a whole run, before its host synchronisation.
 void run_bfs(Context &ctx, Graph &g, BfsState &st, int32_t source, mb_stats *stats, int phase = 0,
-             int force = -1, int *cont = nullptr);
+             int force = -1, int *cont = nullptr, const EmitFn *after = nullptr);
 
 }  // namespace mb

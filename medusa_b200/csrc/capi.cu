@@ -700,13 +700,16 @@ int mb_bfs(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsrc
         if (bfs_async) apps(g).bfs.ensure(g->g);
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};
+            // the levels' copy out rides on the run's own synchronisation
+            const mb::EmitFn copy_out = [&](cudaStream_t s) {
+                MB_CUDA(cudaMemcpyAsync(levels_out + (size_t)i * V, apps(g).bfs.level.p,
+                                        sizeof(int32_t) * (size_t)V, cudaMemcpyDefault, s));
+            };
             if (bfs_async)
                 mb::run_sssp(ctx->c, g->g, apps(g).bfs_async, src[i], &st, mb::LOOP_ALL, -1, nullptr,
-                             apps(g).bfs.level.as<int32_t>());
+                             apps(g).bfs.level.as<int32_t>(), &copy_out);
             else
-                mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st);
-            MB_CUDA(cudaMemcpyAsync(levels_out + (size_t)i * V, apps(g).bfs.level.p,
-                                    sizeof(int32_t) * (size_t)V, cudaMemcpyDefault, ctx->c.stream));
+                mb::run_bfs(ctx->c, g->g, apps(g).bfs, src[i], &st, mb::LOOP_ALL, -1, nullptr, &copy_out);
             total.supersteps = std::max(total.supersteps, st.supersteps);
             total.status_flags |= st.status_flags;
             total.edges_traversed += st.edges_traversed;
@@ -763,9 +766,12 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
         }
         for (int32_t i = 0; i < nsrc; i++) {
             mb_stats st{};
-            mb::run_sssp(ctx->c, g->g, apps(g).sssp, src[i], &st);
-            MB_CUDA(cudaMemcpyAsync(dist_out + (size_t)i * V, apps(g).sssp.dist.p,
-                                    sizeof(float) * (size_t)V, cudaMemcpyDefault, ctx->c.stream));
+            // the distances' copy out rides on the run's own synchronisation
+            const mb::EmitFn copy_out = [&](cudaStream_t s) {
+                MB_CUDA(cudaMemcpyAsync(dist_out + (size_t)i * V, apps(g).sssp.dist.p,
+                                        sizeof(float) * (size_t)V, cudaMemcpyDefault, s));
+            };
+            mb::run_sssp(ctx->c, g->g, apps(g).sssp, src[i], &st, mb::LOOP_ALL, -1, nullptr, nullptr, &copy_out);
             total.supersteps = std::max(total.supersteps, st.supersteps);
             total.status_flags |= st.status_flags;
             total.edges_traversed += st.edges_traversed;

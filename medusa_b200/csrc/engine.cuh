@@ -712,6 +712,10 @@ struct LoopSpec {
     EmitBranch branch;
     EmitFn epilogue;
     const char *name;
+    // whole runs (LOOP_ALL): queued after the run's end event and before
+    // its one host synchronisation (e.g. the copy of the run's output to the
+    // caller), so that it costs no synchronisation of its own
+    EmitFn after;
 };
 // The phases of a run driven one superstep at a time (mb_superstep): BEGIN
 // runs the prologue and picks the first superstep, STEP runs the picked one

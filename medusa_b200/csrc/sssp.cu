@@ -1732,7 +1732,7 @@ static void async_chunks(Context &ctx, Graph &g, SsspState &st) {
 }
 
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase, int force,
-             int *cont, int32_t *bfs_levels) {
+             int *cont, int32_t *bfs_levels, const EmitFn *after) {
     if (bfs_levels && (phase != LOOP_ALL || ctx.persist))
         fail(MB_ERR_INVALID, "asynchronous BFS: whole runs without the persistent grid only");
     st.ensure(g);
@@ -1919,6 +1919,7 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
         if (unit) k_dist_to_level<<<grid_vtx, 256, 0, s>>>(a, bfs_levels);
         MB_CHECK_LAUNCH();
     };
+    if (after) sp.after = *after;
     run_loop(ctx, sp, stats, phase, force, cont);
 }
 

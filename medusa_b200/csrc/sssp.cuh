@@ -118,7 +118,9 @@ uint32_t sssp_bm_push_min(const Context &ctx, const Graph &g);
 // bfs_levels (device, V entries): instead a BFS from `source` by the
 // asynchronous kernel with every weight 1 (whole runs only; the state should
 // then serve BFS runs only, so that its loop graph stays the unit-weight one).
+// after: queued behind a whole run, before its host synchronisation.
 void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *stats, int phase = 0,
-             int force = -1, int *cont = nullptr, int32_t *bfs_levels = nullptr);
+             int force = -1, int *cont = nullptr, int32_t *bfs_levels = nullptr,
+             const EmitFn *after = nullptr);
 
 }  // namespace mb

@@ -245,3 +245,53 @@ def test_learned_policy_takes_the_asynchronous_route(gpu_ctx, api):
     finally:
         gpu_ctx.set_policy(api.MB_POLICY_FIXED)
         g.close()
+
+
+def test_async_sssp_zero_weights_and_a_zero_cycle(actx, api):
+    """Zero weights, including a zero-weight cycle: a relaxation only counts
+    when it lowers a distance, so the kernel ends; the distances are the
+    oracle's."""
+    rng = np.random.default_rng(21)
+    V = 3000
+    src = rng.integers(0, V, 20000).astype(np.int32)
+    dst = rng.integers(0, V, 20000).astype(np.int32)
+    w = rng.integers(0, 5, 20000).astype(np.float32)  # a fifth of the weights are 0
+    cyc = np.arange(10, dtype=np.int32)
+    src = np.concatenate([src, cyc])
+    dst = np.concatenate([dst, (cyc + 1) % 10])
+    w = np.concatenate([w, np.zeros(10, np.float32)])
+    g = actx.graph_from_edges(V, src, dst, w)
+    try:
+        for s0 in (0, 5):
+            want, _ = O.sssp(V, src, dst, w, s0)
+            for delta in (-1, 0, 1):
+                actx.set_tunable("async_delta", delta)
+                got, _ = g.sssp([s0])
+                np.testing.assert_array_equal(got[0].view(np.uint32), want.view(np.uint32))
+    finally:
+        g.close()
+
+
+def test_async_sssp_fractional_weights_equal_the_bsp_loop(gpu_ctx, api):
+    """Non-integer weights: the distances are the least fixpoint of
+    d[v] = min over in-edges of fl(d[u] + w), which every order of
+    relaxations reaches (fl(a + w) is monotone in a), so the asynchronous
+    kernel gives the BSP loop's floats bit for bit."""
+    rng = np.random.default_rng(22)
+    V = 20000
+    src = rng.integers(0, V, 160000).astype(np.int32)
+    dst = rng.integers(0, V, 160000).astype(np.int32)
+    w = rng.uniform(0.001, 3.0, 160000).astype(np.float32)
+    g = gpu_ctx.graph_from_edges(V, src, dst, w)
+    try:
+        gpu_ctx.set_tunable("sssp_async", 0)
+        ref, _ = g.sssp([0])
+        gpu_ctx.set_tunable("sssp_async", 1)
+        for delta in (-1, 0, 1):
+            gpu_ctx.set_tunable("async_delta", delta)
+            got, _ = g.sssp([0])
+            np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
+    finally:
+        gpu_ctx.set_tunable("sssp_async", -1)
+        gpu_ctx.set_tunable("async_delta", -1)
+        g.close()
