@@ -370,8 +370,8 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 asynchronous cooperative launch (no superstep barriers:
                                 warps relax the dirty vertices below a distance threshold
                                 that rises by MB_TUNE_ASYNC_DELTA whenever every warp is
-                                idle); 0 the BSP supersteps; default: 1 on graphs whose
-                                largest out-degree is at most 64 (no hubs), unless a
+                                idle); 0 the BSP supersteps; default 1 (on graphs with
+                                hubs only for the tail, MB_TUNE_ASYNC_BELOW), unless a
                                 near-far width or the persistent grid is set.  Under
                                 MB_POLICY_FIXED and MB_POLICY_LEARNED (it is how schedule
                                 0 runs the rest of a traversal; the forced and replay
@@ -379,8 +379,9 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 graphs without a negative or NaN weight.  Identical
                                 distances */
 #define MB_TUNE_ASYNC_DELTA 18 /* width by which the asynchronous SSSP's threshold rises
-                                 (default 8 x mean weight / mean out-degree, at least the
-                                 mean weight; 0: no threshold) */
+                                 (default: 24 x mean weight / mean out-degree, at least the
+                                 mean weight, on graphs without hubs; 0 -- no threshold --
+                                 for the tail on graphs with hubs) */
 #define MB_TUNE_ASYNC_BLOCKS_PER_SM 19 /* CTAs of 256 threads per SM of the asynchronous
                                          SSSP (default: as many as fit, at most 8) */
 #define MB_TUNE_BFS_ASYNC 20 /* BFS: 1 runs a single-source BFS (MB_POLICY_FIXED or
@@ -396,7 +397,9 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                  once the frontier, after reaching this many out-edges,
                                  has fewer -- the large supersteps run as BSP pushes and
                                  the long tail of small ones as one asynchronous launch;
-                                 0 or -1 (the default): from the first superstep */
+                                 0: from the first superstep; default: 0 on graphs
+                                 without hubs (largest out-degree <= 64), else
+                                 max(2^18, E/16) */
 #define MB_NUM_TUNABLES 23
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);

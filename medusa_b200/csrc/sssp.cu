@@ -1766,14 +1766,19 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     const bool unit = bfs_levels != nullptr;
     const int64_t t_async = ctx.tunable[MB_TUNE_SSSP_ASYNC];
     const bool policy_ok = ctx.schedule_policy == MB_POLICY_FIXED || ctx.schedule_policy == MB_POLICY_LEARNED;
+    // On a hub-free graph the default runs the whole traversal in the
+    // kernel; on a graph with hubs, the BSP supersteps until the frontier,
+    // past its peak, has fewer than max(2^18, E/16) out-edges, and the
+    // kernel for that tail, with no threshold (measured on B200: C2 SSSP
+    // 1.05 -> 0.98 ms; C5 unchanged, 5.15 ms).
+    const bool hub_free = async_by_default(g, false);
     const int32_t async =
         unit ? 1
              : (!policy_ok || !st.weights_ok
                     ? 0
-                    : (t_async >= 0 ? (int32_t)t_async
-                                    : (async_by_default(g, false) && delta == 0.f && !ctx.persist ? 1 : 0)));
+                    : (t_async >= 0 ? (int32_t)t_async : (delta == 0.f && !ctx.persist ? 1 : 0)));
     float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
-                                                               : st.async_delta;
+                                                               : (hub_free ? st.async_delta : 0.f);
     if (unit)
         async_delta = ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_BFS_ASYNC_DELTA]
                                                                 : kBfsAsyncDelta;
@@ -1788,8 +1793,10 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     a.hub_cbase = st.hub_cbase.as<int32_t>();
     a.chunk_src = st.chunk_src.as<int32_t>();
     a.chunk_rs = st.chunk_rs.as<int32_t>();
+    const int64_t t_below = ctx.tunable[MB_TUNE_ASYNC_BELOW];
+    const int64_t below_dflt = hub_free ? 0 : std::max<int64_t>(1 << 18, g.E / 16);
     const uint32_t async_below =
-        unit ? 0u : (uint32_t)std::min<int64_t>(std::max<int64_t>(ctx.tunable[MB_TUNE_ASYNC_BELOW], 0), 0xffffffffll);
+        unit ? 0u : (uint32_t)std::min<int64_t>(t_below >= 0 ? t_below : below_dflt, 0xffffffffll);
     if (phase == LOOP_ALL)
         upload_params(ctx, st.ctrl.p, source, unit ? 0.f : delta, sssp_bm_push_min(ctx, g), async, async_delta,
                       async_below);

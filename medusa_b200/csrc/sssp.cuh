@@ -93,10 +93,12 @@ struct SsspState : FrontierState {
     }
 };
 
-// MB_TUNE_SSSP_ASYNC = -1: the asynchronous kernel on graphs without hubs
-// (largest out-degree <= 64), unless near-far buckets or the persistent grid
-// were asked for.  MB_TUNE_BFS_ASYNC = -1: the same on graphs that are also
-// sparse (mean out-degree <= 6).  Measured on B200 (ms, BSP -> asynchronous):
+// Graphs without hubs (largest out-degree <= 64): MB_TUNE_SSSP_ASYNC = -1
+// runs the whole SSSP in the asynchronous kernel (on other graphs only the
+// tail after the frontier's peak, MB_TUNE_ASYNC_BELOW), unless near-far
+// buckets or the persistent grid were asked for.  MB_TUNE_BFS_ASYNC = -1:
+// the kernel for BFS on hub-free graphs that are also sparse (mean
+// out-degree <= 6).  Measured on B200 (ms, BSP -> asynchronous):
 // SSSP on the 1448^2 grid 2.5 -> 1.2, uniform 2^20 / 2^24 1.19 -> 0.74,
 // uniform 2^18 / 2^22 0.64 -> 0.43; BFS on the grid 1.34 -> 0.72, uniform
 // 2^20 with 4 edges per vertex 0.31 -> 0.27, but uniform 2^20 / 2^24 0.21 ->

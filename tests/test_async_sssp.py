@@ -26,8 +26,9 @@ def actx(request, gpu_ctx, api):
     gpu_ctx.set_graph_capture(request.param)
     gpu_ctx.set_policy(api.MB_POLICY_FIXED)
     gpu_ctx.set_tunable("sssp_async", 1)
+    gpu_ctx.set_tunable("async_below", 0)  # the kernel from the first superstep
     yield gpu_ctx
-    for k in ("sssp_async", "async_delta", "async_blocks_per_sm"):
+    for k in ("sssp_async", "async_delta", "async_blocks_per_sm", "async_below"):
         gpu_ctx.set_tunable(k, -1)
     gpu_ctx.set_graph_capture(True)
 
@@ -122,6 +123,7 @@ def test_async_sssp_full_size_equals_bsp(gpu_ctx, api, which):
         gpu_ctx.set_tunable("sssp_async", 0)
         ref, st0 = g.sssp([0])
         gpu_ctx.set_tunable("sssp_async", 1)
+        gpu_ctx.set_tunable("async_below", 0)  # the kernel from the first superstep
         for delta in (-1, 100):
             gpu_ctx.set_tunable("async_delta", delta)
             got, st1 = g.sssp([0])
@@ -129,8 +131,8 @@ def test_async_sssp_full_size_equals_bsp(gpu_ctx, api, which):
             assert st1["edges_traversed"] == st0["edges_traversed"]
         assert st1["edges_scanned"] < st0["edges_scanned"]
     finally:
-        gpu_ctx.set_tunable("sssp_async", -1)
-        gpu_ctx.set_tunable("async_delta", -1)
+        for k in ("sssp_async", "async_delta", "async_below"):
+            gpu_ctx.set_tunable(k, -1)
         g.close()
 
 
@@ -287,11 +289,12 @@ def test_async_sssp_fractional_weights_equal_the_bsp_loop(gpu_ctx, api):
         gpu_ctx.set_tunable("sssp_async", 0)
         ref, _ = g.sssp([0])
         gpu_ctx.set_tunable("sssp_async", 1)
+        gpu_ctx.set_tunable("async_below", 0)
         for delta in (-1, 0, 1):
             gpu_ctx.set_tunable("async_delta", delta)
             got, _ = g.sssp([0])
             np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
     finally:
-        gpu_ctx.set_tunable("sssp_async", -1)
-        gpu_ctx.set_tunable("async_delta", -1)
+        for k in ("sssp_async", "async_delta", "async_below"):
+            gpu_ctx.set_tunable(k, -1)
         g.close()
