@@ -83,9 +83,10 @@ def tune_joint(ctx, run, names, candidates, reps=3):
 # (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA) and (MB_TUNE_BFS_ASYNC,
 # MB_TUNE_BFS_ASYNC_DELTA) pairs tried together
 SSSP_ASYNC_PAIRS = [(-1, -1), (0, -1)] + [(1, d) for d in ASYNC_DELTAS]
-# (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA, MB_TUNE_ASYNC_BELOW): the BSP
-# supersteps while the frontier is large, then the asynchronous kernel
-SSSP_ASYNC_TRIPLES = [(-1, -1, -1), (0, -1, -1)] + [(1, d, -1) for d in ASYNC_DELTAS] + \
+# (MB_TUNE_SSSP_ASYNC, MB_TUNE_ASYNC_DELTA, MB_TUNE_ASYNC_BELOW): the
+# defaults, the BSP loop alone, the kernel from the first superstep with each
+# step, and the BSP supersteps while the frontier is large, then the kernel
+SSSP_ASYNC_TRIPLES = [(-1, -1, -1), (0, -1, -1)] + [(1, d, 0) for d in ASYNC_DELTAS] + \
     [(1, 0, 1 << b) for b in (18, 20, 22)]
 BFS_ASYNC_PAIRS = [(-1, -1), (1, -1), (1, 2), (1, 4), (1, 8)]
 

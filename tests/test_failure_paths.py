@@ -112,6 +112,7 @@ def test_async_sssp_wait_gives_up(api, graph, capture):
     try:
         ctx.set_graph_capture(capture)
         ctx.set_tunable("sssp_async", 1)
+        ctx.set_tunable("async_below", 0)  # the kernel from the first superstep
         ctx.set_tunable("wait_polls", 0)
         with pytest.raises(api.MedusaError) as e:
             g.sssp([0])
