@@ -86,12 +86,17 @@ __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
     const int32_t *qv = cur ? a.qv[1] : a.qv[0];
     const uint32_t *qo = cur ? a.qo[1] : a.qo[0];
     const uint32_t *front = cur ? a.front[1] : a.front[0];
+    const int32_t *tf = cur ? a.tf[1] : a.tf[0];
+    const uint32_t tiles = (m + kTile - 1) / kTile;
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t c0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * kWarpEdges; c0 < m;
          c0 += warps * kWarpEdges) {
-        // owner entry of the chunk's first edge (binary search over qo)
-        int lo = 0, hi = (int)n;
+        // owner entry of the chunk's first edge: a binary search over qo
+        // within the entries of its merge-path tile (tf[t] holds edge t*kTile,
+        // tf[t+1] edge (t+1)*kTile > c0), not over the whole queue
+        const uint32_t t = (uint32_t)c0 / kTile;
+        int lo = tf[t], hi = t + 1 < tiles ? tf[t + 1] + 1 : (int)n;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (qo[mid] <= (uint32_t)c0) lo = mid; else hi = mid;
