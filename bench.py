@@ -229,6 +229,30 @@ def reset_tunables(ctx, api):
     ctx.set_sssp_delta(0.0)
 
 
+def verify_against_bsp(ctx, api, g, lv_out, d_out):
+    """The timed runs' outputs (device tensors, source 0) against one run of
+    the BSP loop with every tunable at its default and the asynchronous
+    kernels off; the tuned settings are restored afterwards.  Returns
+    {"bfs_levels": bool, "sssp_distances": bool} (bit for bit)."""
+    import torch
+    saved = {k: ctx.get_tunable(k) for k in api.TUNABLES}
+    saved_delta = ctx.sssp_delta
+    try:
+        reset_tunables(ctx, api)
+        ctx.set_tunable("sssp_async", 0)
+        ctx.set_tunable("bfs_async", 0)
+        lv = torch.empty_like(lv_out)
+        dd = torch.empty_like(d_out)
+        g.bfs([0], out=lv)
+        g.sssp([0], out=dd)
+        return {"bfs_levels": bool(torch.equal(lv, lv_out)),
+                "sssp_distances": bool(torch.equal(dd.view(torch.int32), d_out.view(torch.int32)))}
+    finally:
+        for k, v in saved.items():
+            ctx.set_tunable(k, v)
+        ctx.set_sssp_delta(saved_delta)
+
+
 def reduce_over_ranks(dev_ms, edges, dist=None, device="cpu"):
     """Replicas: the job's time is the slowest rank's device time and its
     work the sum of every rank's traversed edges (no data-path collective:
@@ -297,6 +321,8 @@ def run_medusa(args):
             sb_last, ss_last = sb, ss
         torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
+    # the timed (tuned) outputs against the plain BSP loop's, bit for bit
+    verified = verify_against_bsp(ctx, api, g, lv_dev, d_dev)
     t_max, edges_all = reduce_over_ranks(dev_ms, edges, dist, dev)
     value = edges_all / (t_max / 1e3) / 1e9
 
@@ -351,6 +377,7 @@ def run_medusa(args):
                                               "unit": "GB",
                                               "formula": "BFS 8*E_r+20*V_r+4*V; SSSP 12*E_r+20*V_r+4*V"}},
         "gpu_launches": int(launches),
+        "verified_against_bsp": verified,
         "wall_s": round(wall, 3),
         "clocks": clk.summary(),
     }
@@ -489,7 +516,8 @@ def bench_configs(ctx, api, args, flush):
                       "vertices": V, "edges": g.E,
                       "bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
                       "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk),
-                      "autotuned": {k: float(v) for k, v in tuned3.items()}}
+                      "autotuned": {k: float(v) for k, v in tuned3.items()},
+                      "verified_against_bsp": verify_against_bsp(ctx, api, g, lv, dd)}
     g.close()
     if not args.no_cpu_baseline:
         out["c3_grid"]["cpu_baseline"] = cpu_baseline_traversals(
@@ -549,6 +577,9 @@ def bench_configs(ctx, api, args, flush):
     ctx.set_policy(api.MB_POLICY_FIXED)
     c5["learned_identical"] = bool(np.array_equal(res["fixed"][0], res["learned"][0]) and
                                    np.array_equal(res["fixed"][1], res["learned"][1]))
+    lv.copy_(torch.from_numpy(res["fixed"][0]))
+    dd.copy_(torch.from_numpy(res["fixed"][1].view(np.float32)))
+    c5["verified_against_bsp"] = verify_against_bsp(ctx, api, g, lv, dd)
     per_step = {}
     for app, name, model in ((0, "bfs", api.MB_MODEL_BFS), (1, "sssp", api.MB_MODEL_SSSP)):
         X, T, F = ctx.scheduler_collect(g, app, 0, max_samples=32)

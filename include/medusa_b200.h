@@ -371,8 +371,9 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                 warps relax the dirty vertices below a distance threshold
                                 that rises by MB_TUNE_ASYNC_DELTA whenever every warp is
                                 idle); 0 the BSP supersteps; default 1 (on graphs with
-                                hubs only for the tail, MB_TUNE_ASYNC_BELOW), unless a
-                                near-far width or the persistent grid is set.  Under
+                                hubs only for the tail, MB_TUNE_ASYNC_BELOW), unless the
+                                persistent grid is set; never with a near-far width (the
+                                far pile is not the kernel's frontier).  Under
                                 MB_POLICY_FIXED and MB_POLICY_LEARNED (it is how schedule
                                 0 runs the rest of a traversal; the forced and replay
                                 policies name every superstep's schedule), and only on

@@ -1772,11 +1772,14 @@ void run_sssp(Context &ctx, Graph &g, SsspState &st, int32_t source, mb_stats *s
     // kernel for that tail, with no threshold (measured on B200: C2 SSSP
     // 1.05 -> 0.98 ms; C5 unchanged, 5.15 ms).
     const bool hub_free = async_by_default(g, false);
+    // A near-far width turns the kernel off whatever the tunable says: it
+    // starts from the queue frontier only, and vertices parked in the far
+    // pile would never be expanded.
     const int32_t async =
         unit ? 1
-             : (!policy_ok || !st.weights_ok
+             : (!policy_ok || !st.weights_ok || delta != 0.f
                     ? 0
-                    : (t_async >= 0 ? (int32_t)t_async : (delta == 0.f && !ctx.persist ? 1 : 0)));
+                    : (t_async >= 0 ? (int32_t)t_async : (!ctx.persist ? 1 : 0)));
     float async_delta = ctx.tunable[MB_TUNE_ASYNC_DELTA] >= 0 ? (float)ctx.tunable[MB_TUNE_ASYNC_DELTA]
                                                                : (hub_free ? st.async_delta : 0.f);
     if (unit)

@@ -298,3 +298,25 @@ def test_async_sssp_fractional_weights_equal_the_bsp_loop(gpu_ctx, api):
         for k in ("sssp_async", "async_delta", "async_below"):
             gpu_ctx.set_tunable(k, -1)
         g.close()
+
+
+@pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12"])
+def test_near_far_width_turns_the_kernel_off(actx, name):
+    """The asynchronous kernel starts from the queue frontier only, so with
+    near-far buckets on (vertices parked in the far pile) it must not run,
+    whatever the tunable says: distances stay the reference's for every
+    width, with the kernel asked for from the first superstep and as a tail."""
+    c = load_golden(name)
+    g = actx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
+    try:
+        for below in (0, 1, 64):
+            actx.set_tunable("async_below", below)
+            for width in (1.0, 37.0, 500.0, -1.0):
+                actx.set_sssp_delta(width)
+                for i, s in enumerate(c["sources"]):
+                    d, _ = g.sssp([int(s)])
+                    np.testing.assert_array_equal(d[0].view(np.uint32), c["sssp_dist"][i].view(np.uint32),
+                                                  err_msg="width %g below %d" % (width, below))
+    finally:
+        actx.set_sssp_delta(0.0)
+        g.close()

@@ -54,3 +54,49 @@ def test_dominant_branch_and_its_roofline():
     ratio = bench.measured_traffic_ratio("k_push_edge_bm + k_nbm2q")
     assert r["traffic"] == round(ratio * byts / 2)
     assert abs(r["share_of_traced_time"] - 0.08 / 0.12) < 1e-3
+
+
+def test_verify_against_bsp_compares_and_restores_the_tuned_settings():
+    """The bench checks its tuned outputs against one default BSP run and
+    puts every tuned setting back afterwards."""
+    import torch
+    from medusa_b200 import api
+
+    class Ctx:
+        def __init__(self):
+            self.t = {k: -1 for k in api.TUNABLES}
+            self.sssp_delta = 0.0
+            self.seen = None
+
+        def get_tunable(self, k):
+            return self.t[k]
+
+        def set_tunable(self, k, v):
+            self.t[k] = v
+
+        def set_sssp_delta(self, d):
+            self.sssp_delta = d
+
+    ctx = Ctx()
+
+    class G:
+        def bfs(self, src, out):
+            ctx.seen = dict(ctx.t)
+            out.copy_(torch.arange(4, dtype=torch.int32))
+            return out, {}
+
+        def sssp(self, src, out):
+            out.copy_(torch.tensor([0.0, 1.0, 2.0, 3.0]))
+            return out, {}
+
+    ctx.t["sssp_async"] = 1
+    ctx.t["async_below"] = 1 << 20
+    ctx.sssp_delta = 100.0
+    lv = torch.arange(4, dtype=torch.int32)
+    r = bench.verify_against_bsp(ctx, api, G(), lv, torch.tensor([0.0, 1.0, 2.0, 3.0]))
+    assert r == {"bfs_levels": True, "sssp_distances": True}
+    # the reference run: defaults, the asynchronous kernels off
+    assert ctx.seen["sssp_async"] == 0 and ctx.seen["bfs_async"] == 0 and ctx.seen["async_below"] == -1
+    assert ctx.t["sssp_async"] == 1 and ctx.t["async_below"] == 1 << 20 and ctx.sssp_delta == 100.0
+    r = bench.verify_against_bsp(ctx, api, G(), lv, torch.tensor([0.0, 1.0, 2.0, 4.0]))
+    assert r == {"bfs_levels": True, "sssp_distances": False}
