@@ -1039,7 +1039,9 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
 
 // ---- asynchronous SSSP (kBranchAsync) ---------------------------------------
 // The rest of the traversal, from the current queue frontier to the
-// fixpoint, in ONE cooperative launch with no superstep barriers: a chaotic
+// fixpoint (never entered with near-far buckets on: their far pile is not
+// part of that frontier), in ONE cooperative launch with no superstep
+// barriers: a chaotic
 // relaxation ordered by a distance threshold, in the manner of Meyer &
 // Sanders' delta-stepping (J. Algorithms 49, 2003) run asynchronously.
 //  - a.adirty is the dirty bitmap: v's bit is set when dist[v] dropped and
@@ -1053,11 +1055,14 @@ __global__ void __launch_bounds__(kPushThreads) k_persist(SsspArgs a, int cap) {
 //    owner from the hub's distance read at that claim, so one hub's edges
 //    spread over many warps and no warp gets a long serial batch;
 //  - warp g owns the bitmap words g, g + G, g + 2G, ... (G = warps of the
-//    grid; interleaved, so the low-numbered hubs of R-MAT graphs spread out).
-//    Only the owner clears bits: it claims the bits of vertices whose
-//    distance is below the threshold T with one atomicAnd per word, re-reads
-//    their distances and relaxes their out-edges warp-wide, 32 edges per
-//    strip; a lower distance is atomicMin'ed and the neighbour's bit set;
+//    grid; interleaved, so the low-numbered hubs of R-MAT graphs spread out)
+//    and scans them: it claims the bits of vertices whose distance is below
+//    the threshold T with one atomicAnd per word, re-reads their distances
+//    and relaxes their out-edges warp-wide, 32 edges per strip; a lower
+//    distance is atomicMin'ed and the neighbour's bit set.  A warp that
+//    itself set the bit of a vertex below T claims it back and relaxes it
+//    next (local continuation).  A claim is an atomicAnd that returned the
+//    bit set, so every set bit has exactly one claimer;
 //  - termination: AsyncState::p counts the bits a warp may set (added, and
 //    its return awaited, before the warp sets any) and AsyncState::d the
 //    part it did not set plus every finished claim.  Both only grow, and
