@@ -122,36 +122,30 @@ __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
             v = __ldg(&a.col[e]);
             w = __ldg(&a.wt[e]);
         }
-        // per edge the loop shuffles only what changes: the head's line
-        // offset (v * 32, 32-bit: V * 32 < 2^31) and the weight every edge,
-        // the tail only where it differs from the previous edge's
-        const int32_t v32 = v >= 0 ? v * 32 : -1;
-        const int32_t u_prev = __shfl_up_sync(0xffffffffu, u, 1);
-        const uint32_t newtail = __ballot_sync(0xffffffffu, lane == 0 || u != u_prev);
-        const uint32_t nvalid = __popc(__ballot_sync(0xffffffffu, v >= 0));  // a prefix of the lanes
-        bool act = false;  // this lane's source is active at the current tail
-        uint32_t newly = 0;  // newly: edges whose head this warp touched first
+        int32_t cu = -1;
+        uint32_t fm = 0, newly = 0;  // newly: edges whose head this warp touched first
         float du = 0.f;
         for (int k = 0; k < kWarpEdges; k++) {
-            if ((uint32_t)k >= nvalid) break;  // warp-uniform: past the last frontier edge
-            const int32_t vk32 = __shfl_sync(0xffffffffu, v32, k);
+            const int32_t vk = __shfl_sync(0xffffffffu, v, k);
+            if (vk < 0) break;  // warp-uniform: past the last frontier edge
+            const int32_t uk = __shfl_sync(0xffffffffu, u, k);
             const float wk = __shfl_sync(0xffffffffu, w, k);
-            if ((newtail >> k) & 1u) {  // warp-uniform: a new tail vertex
-                const int32_t uk = __shfl_sync(0xffffffffu, u, k);
-                act = (front[uk] >> lane) & 1u;
+            if (uk != cu) {  // warp-uniform: a new tail vertex
+                cu = uk;
+                fm = front[uk];
                 du = __ldcg(&a.dist[(size_t)uk * 32 + lane]);
             }
             bool imp = false;
-            if (act) {
+            if ((fm >> lane) & 1u) {
                 const float nd = du + wk;
-                float *pv = a.dist + (vk32 + lane);
+                float *pv = &a.dist[(size_t)vk * 32 + lane];
                 if (nd < __ldcg(pv)) {
                     atomicMin((unsigned *)pv, __float_as_uint(nd));
                     imp = true;
                 }
             }
             const uint32_t mask = __ballot_sync(0xffffffffu, imp);
-            if (mask && lane == 0 && atomicOr(&a.nxt[vk32 >> 5], mask) == 0u) newly |= 1u << k;
+            if (mask && lane == 0 && atomicOr(&a.nxt[vk], mask) == 0u) newly |= 1u << k;
         }
         // one aggregated append per warp: lane e appends its edge's head
         newly = __shfl_sync(0xffffffffu, newly, 0);
