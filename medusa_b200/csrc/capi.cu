@@ -738,9 +738,7 @@ int mb_sssp(mb_ctx *ctx, const mb_graph *gc, const int32_t *sources, int32_t nsr
         for (int32_t s : src)
             if (s < 0 || s >= V) mb::fail(MB_ERR_INVALID, "source vertex out of range");
         mb_stats total{};
-        // batched: up to 32 sources per traversal; its push addresses a
-        // vertex's 32-distance line with a 32-bit offset (V * 32 < 2^31)
-        if (nsrc > 1 && ctx->c.batching && (int64_t)V * 32 < (int64_t)INT32_MAX) {
+        if (nsrc > 1 && ctx->c.batching) {
             // batches of up to 32 sources, one masked traversal each
             mb::MsSsspState &ms = apps(g).mssssp;
             ms.ensure(g->g);  // before reserving ms.out (a rebuild releases it)
