@@ -1,6 +1,6 @@
 """The asynchronous SSSP kernel's termination protocol, restated on the CPU.
 
-`k_sssp_async` (medusa_b200/csrc/sssp.cu) has no barrier: warps claim dirty
+`k_sssp_async` (medusa_b200/csrc/sssp_async.cuh) has no barrier: warps claim dirty
 vertices, relax their out-edges and set the bits of the vertices whose
 distance dropped, and a warp decides that the run is over when the work
 counters say so -- every slot's `d` counter read first, then every slot's
