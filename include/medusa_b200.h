@@ -401,7 +401,14 @@ int mb_get_trace(mb_ctx *ctx, mb_trace_rec *out, int32_t max, int32_t *n_out);
                                  0: from the first superstep; default: 0 on graphs
                                  without hubs (largest out-degree <= 64), else
                                  max(2^18, E/16) */
-#define MB_NUM_TUNABLES 23
+#define MB_TUNE_MSS_DELTA 23 /* batched SSSP (2..32 sources): near-far width -- the
+                               frontier holds only the (vertex, source) pairs below a
+                               threshold that rises by this much whenever none is
+                               left; 0: plain frontier Bellman-Ford; default: 0.3 x
+                               the mean weight on graphs whose largest out-degree is
+                               above 64 and at most E/1024, else 0 (and 0 when a
+                               weight is negative or NaN) */
+#define MB_NUM_TUNABLES 24
 int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value);
 int mb_get_tunable(const mb_ctx *ctx, int32_t which, int64_t *value);
 

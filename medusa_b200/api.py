@@ -28,14 +28,15 @@ MB_TUNE_SSSP_BM_PUSH_MIN, MB_TUNE_PUSH_BLOCKS_PER_SM, MB_TUNE_VERTEX_BLOCKS_PER_
     MB_TUNE_BULK_STAGE, MB_TUNE_BFS_GAMMA, MB_TUNE_PR_HUB_MIN, MB_TUNE_WAIT_POLLS, \
     MB_TUNE_STEP_CAP, MB_TUNE_SMALL_PUSH_EDGES, MB_TUNE_PR_HUB_CTAS, MB_TUNE_SSSP_ASYNC, \
     MB_TUNE_ASYNC_DELTA, MB_TUNE_ASYNC_BLOCKS_PER_SM, MB_TUNE_BFS_ASYNC, MB_TUNE_BFS_ASYNC_DELTA, \
-    MB_TUNE_ASYNC_BELOW = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22
+    MB_TUNE_ASYNC_BELOW, MB_TUNE_MSS_DELTA = \
+    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23
 TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_sm": 2,
             "tail_edges": 3, "batch_threads": 4, "batch_edges_per_cta": 5,
             "pr_light_vpl": 6, "pr_short_pair": 7, "bfs_alpha": 8, "bfs_beta": 9,
             "bulk_stage": 10, "bfs_gamma": 11, "pr_hub_min": 12, "wait_polls": 13,
             "step_cap": 14, "small_push_edges": 15, "pr_hub_ctas": 16, "sssp_async": 17,
             "async_delta": 18, "async_blocks_per_sm": 19, "bfs_async": 20, "bfs_async_delta": 21,
-            "async_below": 22}
+            "async_below": 22, "mss_delta": 23}
 NUM_SCHEDULES = 8
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]

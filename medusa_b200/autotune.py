@@ -122,6 +122,18 @@ def tune_bfs(ctx, g, source=0, reps=3):
     return best, table + t2
 
 
+# near-far widths of the batched SSSP tried (-1: the per-graph default;
+# 0: no buckets)
+MSS_DELTAS = [-1, 0, 50, 100, 150, 200, 400, 800, 2000]
+
+
+def tune_batched_sssp(ctx, g, sources, reps=3):
+    """The near-far width of the batched SSSP (2..32 sources per traversal)
+    over `sources` on graph g; leaves the fastest set."""
+    run = lambda: g.sssp(list(sources))[1]
+    return tune(ctx, run, {"mss_delta": MSS_DELTAS}, reps)
+
+
 def tune_traversals(ctx, g, source=0, reps=3):
     """Every BFS/SSSP tunable at once, timing one BFS plus one SSSP (the
     tunables are per context and the two apps share the push grid)."""

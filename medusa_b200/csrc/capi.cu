@@ -311,6 +311,8 @@ int mb_set_tunable(mb_ctx *ctx, int32_t which, int64_t value) {
         return set_error(ctx, MB_ERR_INVALID, "asynchronous BFS is 0 or 1");
     if (which == MB_TUNE_BFS_ASYNC_DELTA && value > (1 << 30))
         return set_error(ctx, MB_ERR_INVALID, "asynchronous BFS delta must be <= 2^30");
+    if (which == MB_TUNE_MSS_DELTA && value > (1 << 30))
+        return set_error(ctx, MB_ERR_INVALID, "batched SSSP delta must be <= 2^30");
     if (which == MB_TUNE_ASYNC_BLOCKS_PER_SM && (value == 0 || value > 8))
         return set_error(ctx, MB_ERR_INVALID, "asynchronous SSSP blocks per SM must be 1..8");
     if (ctx->c.tunable[which] == value) return MB_OK;  // nothing to rebuild

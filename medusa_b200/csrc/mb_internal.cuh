@@ -137,7 +137,7 @@ struct Context {
     int pr_order = MB_PR_ORDER_REFERENCE;  // PageRank summation order
     // launch and routing parameters (MB_TUNE_*); -1: the built-in default
     int64_t tunable[MB_NUM_TUNABLES] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
-                                       -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+                                       -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
     uint64_t tune_gen = 0;  // bumped on every change (loop graphs are rebuilt)
     int blocks_per_sm(int which, int dflt) const {
         return tunable[which] > 0 ? (int)tunable[which] : dflt;

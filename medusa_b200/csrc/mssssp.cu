@@ -10,13 +10,25 @@
 // valued float distances, exact minima), so dist_out[s*V + v] equals 32
 // single-source runs bit for bit.  No reference counterpart exists for the
 // batching itself.
+//
+// Near-far buckets (width delta > 0, MB_TUNE_MSS_DELTA): the frontier holds
+// only the (vertex, source) pairs whose distance is below a threshold T;
+// the commit moves a touched vertex's other pairs into far[v] (the vertex
+// joins a far list the first time), and when no near pair is left a far
+// pass raises T to the least deferred distance + delta and moves the pairs
+// now below it back into the queue.  Each pair is still relaxed until no
+// distance drops, so the distances are the same fixpoint; what changes is
+// how often an edge is relaxed before its tail's distance is final.
 #include <algorithm>
+#include <cmath>
 #include "mssssp.cuh"
+#include "sssp.cuh"
 
 namespace mb {
 namespace {
 
 constexpr int kWarpEdges = 32;  // consecutive edges a warp relaxes per pass
+constexpr uint32_t kMsInfBits = 0x7f800000u;  // +inf
 
 struct MsCtrl {
     unsigned long long q[2];
@@ -25,6 +37,12 @@ struct MsCtrl {
     int32_t supersteps;
     int32_t done;
     unsigned long long work;  // edges relaxed (for all sources of a batch)
+    // near-far buckets (delta > 0)
+    float T;            // pairs at distance >= T wait in far[v]
+    uint32_t fmin;      // float bits: least distance of a waiting pair (a lower bound)
+    int32_t fl;         // the far list that receives newly waiting vertices
+    int32_t advance;    // 1: the queue is empty and pairs wait
+    uint32_t nfar[2];   // far list lengths
 };
 
 struct MsArgs {
@@ -34,10 +52,14 @@ struct MsArgs {
     const float *wt;
     float *dist;  // [V][32]
     uint32_t *front[2], *nxt;
+    unsigned long long *nxt2;  // the same buffer with near-far: far bits << 32 | near bits
     int32_t *touched;
     int32_t *qv[2];
     uint32_t *qo[2];
     int32_t *tf[2];
+    uint32_t *far;      // [V] mask of the pairs waiting above T
+    int32_t *farl[2];   // far lists (a vertex is on the live one iff far[v] != 0)
+    float delta;        // near-far width; 0: plain frontier Bellman-Ford
     int32_t nsrc;
     MsCtrl *c;
 };
@@ -55,6 +77,11 @@ __global__ void k_mss_init(MsArgs a, const int32_t *sources) {
     c->cur = 0;
     c->supersteps = 0;
     c->work = 0;
+    c->T = a.delta > 0.f ? a.delta : __uint_as_float(kMsInfBits);
+    c->fmin = kMsInfBits;
+    c->fl = 0;
+    c->advance = 0;
+    c->nfar[0] = c->nfar[1] = 0u;
     uint32_t n = 0, m = 0;
     for (int i = 0; i < a.nsrc; i++) {
         const int32_t v = sources[i];
@@ -76,10 +103,24 @@ __global__ void k_mss_init(MsArgs a, const int32_t *sources) {
     c->done = n == 0;
 }
 
+// fmn of every lane into c->fmin (distances are non-negative: their float
+// bits order like the numbers)
+__device__ __forceinline__ void publish_fmin(MsCtrl *c, float fmn) {
+    const unsigned m = __reduce_min_sync(0xffffffffu, __float_as_uint(fmn));
+    if ((threadIdx.x & 31) == 0 && m < kMsInfBits) atomicMin(&c->fmin, m);
+}
+
 // Each warp relaxes kWarpEdges consecutive frontier edges (edge-balanced over
 // the queue's scanned out-degrees), one edge at a time for all 32 sources.
+// kNF (near-far buckets): an improved pair is marked near (new distance
+// below T) or far in the head's 64-bit mask; a pair improved both ways in
+// one superstep ends below T, so the commit takes near over far.
+template <bool kNF>
 __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
     MsCtrl *c = a.c;
+    if (c->done) return;
+    const float T = kNF ? c->T : 0.f;
+    float fmn = __uint_as_float(kMsInfBits);  // least far distance this warp set
     const int cur = c->cur;
     const unsigned long long q = c->q[cur];
     const uint32_t n = (uint32_t)(q >> 32), m = (uint32_t)q;
@@ -135,17 +176,28 @@ __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
                 fm = front[uk];
                 du = __ldcg(&a.dist[(size_t)uk * 32 + lane]);
             }
-            bool imp = false;
+            bool imp = false, nearb = false;
             if ((fm >> lane) & 1u) {
                 const float nd = du + wk;
                 float *pv = &a.dist[(size_t)vk * 32 + lane];
                 if (nd < __ldcg(pv)) {
                     atomicMin((unsigned *)pv, __float_as_uint(nd));
                     imp = true;
+                    if (kNF) {
+                        if (nd < T) nearb = true;
+                        else fmn = fminf(fmn, nd);
+                    }
                 }
             }
             const uint32_t mask = __ballot_sync(0xffffffffu, imp);
-            if (mask && lane == 0 && atomicOr(&a.nxt[vk], mask) == 0u) newly |= 1u << k;
+            if (kNF) {
+                const uint32_t mn = __ballot_sync(0xffffffffu, nearb);
+                if (mask && lane == 0 &&
+                    atomicOr(&a.nxt2[vk], ((unsigned long long)(mask & ~mn) << 32) | mn) == 0ull)
+                    newly |= 1u << k;
+            } else if (mask && lane == 0 && atomicOr(&a.nxt[vk], mask) == 0u) {
+                newly |= 1u << k;
+            }
         }
         // one aggregated append per warp: lane e appends its edge's head
         newly = __shfl_sync(0xffffffffu, newly, 0);
@@ -157,43 +209,151 @@ __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
             if (mine) a.touched[base + __popc(newly & lanemask_lt())] = v;
         }
     }
+    if (kNF) publish_fmin(c, fmn);
+}
+
+// Warp-cooperative split of every lane's (vertex v, source mask m): the bits
+// of m whose source's distance to v is below T come back, and fmn takes the
+// least distance among the other bits.  All 32 lanes call it; lanes with
+// m == 0 take no part (their v is not read).  Eight vertices' lines are
+// loaded at a time, so their reads overlap.
+__device__ __forceinline__ uint32_t split_near(const float *dist, int32_t v, uint32_t m, float T,
+                                               float &fmn) {
+    const int lane = threadIdx.x & 31;
+    uint32_t near = 0u;
+    const uint32_t any = __ballot_sync(0xffffffffu, m != 0u);
+    for (int k0 = 0; k0 < 32; k0 += 8) {
+        if (!((any >> k0) & 0xffu)) continue;  // warp-uniform
+        float d[8];
+        uint32_t mk[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int32_t vk = __shfl_sync(0xffffffffu, v, k0 + j);
+            mk[j] = __shfl_sync(0xffffffffu, m, k0 + j);
+            d[j] = mk[j] ? __ldcg(&dist[(size_t)vk * 32 + lane]) : 0.f;  // the vertex's line
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const uint32_t nm = __ballot_sync(0xffffffffu, d[j] < T) & mk[j];
+            if (lane == k0 + j) near = nm;
+            if (((mk[j] & ~nm) >> lane) & 1u) fmn = fminf(fmn, d[j]);
+        }
+    }
+    return near;
+}
+
+// Warp-aggregated append of the predicated lanes' v to list[*cnt ...].
+__device__ __forceinline__ void append_warp(bool pred, int32_t v, uint32_t *cnt, int32_t *list) {
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) list[base + __popc(mask & lanemask_lt())] = v;
 }
 
 // commit: clear the old frontier masks; touched vertices take their new
-// masks and join the next queue
+// masks and join the next queue.  With near-far buckets (kNF) only their
+// near pairs do; the far ones wait in far[v].
+template <bool kNF>
 __global__ void k_mss_commit(MsArgs a) {
     MsCtrl *c = a.c;
+    if (c->done) return;
     const int cur = c->cur, nx = cur ^ 1;
     const uint32_t nold = (uint32_t)(c->q[cur] >> 32), nt = c->touched;
     uint32_t *front_cur = cur ? a.front[1] : a.front[0];
     uint32_t *front_nx = cur ? a.front[0] : a.front[1];
     const int32_t *qv = cur ? a.qv[1] : a.qv[0];
+    const int fl = kNF ? c->fl : 0;
     const int lane = threadIdx.x & 31;
     const int64_t total = (int64_t)nold + nt;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < total;
          base += warps * 32) {
         const int64_t i = base + lane;
-        bool join = false;
+        bool join = false, wait = false;
         int32_t v = 0;
         uint32_t deg = 0;
         if (i < nold) {
             front_cur[qv[i]] = 0u;
         } else if (i < total) {
             v = a.touched[i - nold];
-            const uint32_t nb = a.nxt[v];
-            a.nxt[v] = 0u;
-            front_nx[v] = nb;
+            uint32_t near;
             deg = (uint32_t)a.outdeg[v];
-            join = deg > 0;
+            if (kNF) {
+                const unsigned long long b = a.nxt2[v];
+                a.nxt2[v] = 0ull;
+                near = (uint32_t)b;
+                const uint32_t fm = (uint32_t)(b >> 32) & ~near;
+                // a vertex without out-edges relaxes nothing: no bucket
+                if (deg > 0 && fm) wait = atomicOr(&a.far[v], fm) == 0u;  // first: list it
+            } else {
+                near = a.nxt[v];
+                a.nxt[v] = 0u;
+            }
+            front_nx[v] = near;
+            join = deg > 0 && near != 0u;
         }
+        if (kNF) append_warp(wait, v, &c->nfar[fl], fl ? a.farl[1] : a.farl[0]);
         enqueue_warp(join, v, deg, &c->q[nx], nx ? a.qv[1] : a.qv[0], nx ? a.qo[1] : a.qo[0],
                      nx ? a.tf[1] : a.tf[0]);
     }
 }
 
+// The queue ran dry with pairs waiting: T becomes the least waiting distance
+// + delta (so at least that pair is below it), and the far lists swap.
+__global__ void k_mss_advance(MsArgs a) {
+    MsCtrl *c = a.c;
+    if (!c->advance) return;
+    c->T = __uint_as_float(c->fmin) + a.delta;
+    c->fmin = kMsInfBits;
+    c->fl ^= 1;
+    c->nfar[c->fl] = 0u;
+}
+
+// The far pass after k_mss_advance: every vertex of the old far list puts
+// its pairs now below T into the frontier (front[cur], queue cur); the rest
+// stay in far[v] and the vertex moves to the live far list.
+__global__ void k_mss_far(MsArgs a) {
+    MsCtrl *c = a.c;
+    if (!c->advance) return;
+    const int fl = c->fl, scan = fl ^ 1, cur = c->cur;
+    const uint32_t n = c->nfar[scan];
+    const float T = c->T;
+    const int32_t *list = scan ? a.farl[1] : a.farl[0];
+    uint32_t *front_cur = cur ? a.front[1] : a.front[0];
+    float fmn = __uint_as_float(kMsInfBits);
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n;
+         base += warps * 32) {
+        const int64_t i = base + lane;
+        int32_t v = 0;
+        uint32_t m = 0u;
+        if (i < n) {
+            v = list[i];
+            m = a.far[v];
+        }
+        const uint32_t near = split_near(a.dist, v, m, T, fmn);
+        const uint32_t rem = m & ~near;
+        if (i < n) {
+            a.far[v] = rem;
+            if (near) front_cur[v] = near;
+        }
+        append_warp(rem != 0u, v, &c->nfar[fl], fl ? a.farl[1] : a.farl[0]);
+        enqueue_warp(near != 0u, v, near ? (uint32_t)a.outdeg[v] : 0u, &c->q[cur],
+                     cur ? a.qv[1] : a.qv[0], cur ? a.qo[1] : a.qo[0], cur ? a.tf[1] : a.tf[0]);
+    }
+    publish_fmin(c, fmn);
+}
+
+// The host queues several supersteps between two reads of the control
+// block: once the run is done, every kernel of a superstep returns at once.
 __global__ void k_mss_begin(MsArgs a) {
     MsCtrl *c = a.c;
+    if (c->done) return;
+    c->advance = 0;
     c->touched = 0;
     c->q[c->cur ^ 1] = 0ull;
     c->work += (uint32_t)c->q[c->cur];
@@ -201,10 +361,14 @@ __global__ void k_mss_begin(MsArgs a) {
 
 __global__ void k_mss_end(MsArgs a) {
     MsCtrl *c = a.c;
+    if (c->done) return;
     c->q[c->cur] = 0ull;
     c->cur ^= 1;
     c->supersteps++;
-    c->done = (c->q[c->cur] >> 32) == 0;
+    const bool empty = (c->q[c->cur] >> 32) == 0;
+    const bool waiting = c->nfar[c->fl] != 0u;
+    c->done = empty && !waiting;
+    c->advance = empty && waiting;
 }
 
 // [V][32] -> out[s*V + v] for the batch's sources (32x32 tiles transposed
@@ -251,18 +415,42 @@ void MsSsspState::ensure(const Graph &g) {
     dist.reserve(sizeof(float) * 32 * vb);
     front[0].reserve(4 * vb);
     front[1].reserve(4 * vb);
-    nxt.reserve(4 * vb);
+    nxt.reserve(8 * vb);  // 64-bit masks with near-far buckets
     touched.reserve(4 * vb);
     const size_t tiles = (size_t)(E / kTile) + 2;
     for (int i = 0; i < 2; i++) {
         qv[i].reserve(4 * vb);
         qo[i].reserve(4 * vb);
         tf[i].reserve(4 * tiles);
+        farl[i].reserve(4 * vb);
     }
+    far.reserve(4 * vb);
+    bool bad = false;
+    sssp_weight_stats(g, &mean_w, &bad);
+    weights_ok = !bad;
     ctrl.reserve(sizeof(MsCtrl));
     stats.reserve(2 * sizeof(unsigned long long));
     srcs.reserve(32 * sizeof(int32_t));
     built = true;
+}
+
+float mss_default_delta(const Graph &g, double mean_w) {
+    // measured (32 sources, CUDA events): R-MAT 2^20 / 2^24 and 2^22 / 2^26
+    // (a = 0.45, weights 1..1000) run fastest at widths 100-200, 1.2-1.45x
+    // faster than without buckets; wider ones lose their gain (400: none).
+    // With a hub of more than E/1024 out-edges (a = 0.57) every width is
+    // slower: the traversal takes 17 supersteps without buckets.  Graphs
+    // without hubs want widths from 0.8x (uniform) to 4x (grid) the mean
+    // weight, and smaller ones are 1.3-3x slower: they are left to tuning.
+    if (g.E == 0 || g.max_outdeg <= 64 || (int64_t)g.max_outdeg > g.E / 1024) return 0.f;
+    return (float)std::max(1.0, std::floor(mean_w * 0.3));
+}
+
+float mss_delta(const Context &ctx, const Graph &g, const MsSsspState &st) {
+    if (!st.weights_ok) return 0.f;
+    const int64_t t = ctx.tunable[MB_TUNE_MSS_DELTA];
+    if (t >= 0) return (float)t;
+    return mss_default_delta(g, st.mean_w);
 }
 
 void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources, int32_t nsrc,
@@ -281,12 +469,18 @@ void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources,
     a.front[0] = st.front[0].as<uint32_t>();
     a.front[1] = st.front[1].as<uint32_t>();
     a.nxt = st.nxt.as<uint32_t>();
+    a.nxt2 = st.nxt.as<unsigned long long>();
     a.touched = st.touched.as<int32_t>();
     for (int i = 0; i < 2; i++) {
         a.qv[i] = st.qv[i].as<int32_t>();
         a.qo[i] = st.qo[i].as<uint32_t>();
         a.tf[i] = st.tf[i].as<int32_t>();
     }
+    a.far = st.far.as<uint32_t>();
+    a.farl[0] = st.farl[0].as<int32_t>();
+    a.farl[1] = st.farl[1].as<int32_t>();
+    a.delta = mss_delta(ctx, g, st);
+    const bool nf = a.delta > 0.f;
     a.nsrc = nsrc;
     a.c = st.ctrl.as<MsCtrl>();
     const size_t vb = (size_t)g.V;
@@ -302,7 +496,8 @@ void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources,
         k_mss_fill<<<gv, 256, 0, s>>>(a.dist, (int64_t)vb * 32);
         MB_CUDA(cudaMemsetAsync(a.front[0], 0, 4 * vb, s));
         MB_CUDA(cudaMemsetAsync(a.front[1], 0, 4 * vb, s));
-        MB_CUDA(cudaMemsetAsync(a.nxt, 0, 4 * vb, s));
+        MB_CUDA(cudaMemsetAsync(a.nxt, 0, (nf ? 8 : 4) * vb, s));
+        if (nf) MB_CUDA(cudaMemsetAsync(a.far, 0, 4 * vb, s));
         MB_CUDA(cudaMemsetAsync(st.stats.p, 0, 2 * sizeof(unsigned long long), s));
         k_mss_init<<<1, 32, 0, s>>>(a, st.srcs.as<int32_t>());
         launches += 2;
@@ -310,17 +505,34 @@ void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources,
         // every superstep lowers some distance; integer distances below 2^24
         // bound the count well below this cap
         const int64_t cap = step_cap(ctx, (int64_t)g.V * 4 + 16);
-        for (int64_t it = 0;; it++) {
+        // the control block is read after the first superstep and then after
+        // every kSupersteps queued ones (the kernels of a superstep queued
+        // past the last one return at once)
+        constexpr int kSupersteps = 4;
+        for (int64_t it = 0;;) {
             MB_CUDA(cudaMemcpyAsync(hc, a.c, sizeof(MsCtrl), cudaMemcpyDeviceToHost, s));
             MB_CUDA(cudaStreamSynchronize(s));
             if (hc->done) break;
             if (it > cap) fail(MB_ERR_TIMEOUT, "batched sssp: superstep cap reached");
-            k_mss_begin<<<1, 1, 0, s>>>(a);
-            k_mss_push<<<gv, 256, 0, s>>>(a);
-            k_mss_commit<<<gv, 256, 0, s>>>(a);
-            k_mss_end<<<1, 1, 0, s>>>(a);
-            launches += 4;
-            MB_CHECK_LAUNCH();
+            const int batch = it == 0 ? 1 : kSupersteps;
+            for (int b = 0; b < batch; b++, it++) {
+                if (nf) {  // refill the queue from the far pairs when it ran dry
+                    k_mss_advance<<<1, 1, 0, s>>>(a);
+                    k_mss_far<<<gv, 256, 0, s>>>(a);
+                    launches += 2;
+                }
+                k_mss_begin<<<1, 1, 0, s>>>(a);
+                if (nf) {
+                    k_mss_push<true><<<gv, 256, 0, s>>>(a);
+                    k_mss_commit<true><<<gv, 256, 0, s>>>(a);
+                } else {
+                    k_mss_push<false><<<gv, 256, 0, s>>>(a);
+                    k_mss_commit<false><<<gv, 256, 0, s>>>(a);
+                }
+                k_mss_end<<<1, 1, 0, s>>>(a);
+                launches += 4;
+                MB_CHECK_LAUNCH();
+            }
         }
         k_mss_out<<<gv, 256, 0, s>>>(a, dist_dev, st.stats.as<unsigned long long>());
         launches++;

@@ -4,12 +4,14 @@ single-kernel captures) and quick timings:
     python -m medusa_b200.profile_cases CASE [--reps N] [--hostloop]
 
 CASE: c2-bfs, c2-sssp (R-MAT 2^20 / 2^24, source 0), c2-msssp (the same
-graph, SSSP from sources 0..31 in one batched traversal), c4a-msssp (R-MAT
+graph, SSSP from sources 0..31 in one batched traversal; NAME-msssp on any
+graph below), c4a-msssp (R-MAT
 2^22 / 2^26, sources 0..31), c1-pr (uniform
 2^18 / 2^22, 10 supersteps), c5-bfs, c5-sssp (R-MAT 2^24 / 2^28,
 (0.57,0.19,0.19,0.05)), c5-pr (20 supersteps), c3-bfs, c3-sssp (1448^2
 grid), c5s-bfs, c5s-sssp, c5s-pr (the C5 generator at 2^21 / 2^25: a case
-small enough for full ncu captures), path-bfs, path-sssp (a directed path
+small enough for full ncu captures), unif-bfs, unif-sssp (uniform random
+2^20 / 2^24, weights 1..1000), path-bfs, path-sssp (a directed path
 of 200 vertices, persistent tail off: every superstep is one select kernel
 and one push over a one-vertex frontier -- the fixed cost of a superstep).
 --pr-order fixed|reference picks PageRank's summation order (default: the
@@ -36,6 +38,8 @@ def params(case):
         return api.rmat_params(22, 1 << 26, 0.45, 0.15, 0.15, seed=SEED, wmin=1, wmax=1000)
     if case.startswith("c1"):
         return api.uniform_params(1 << 18, 1 << 22, seed=SEED)
+    if case.startswith("unif"):
+        return api.uniform_params(1 << 20, 1 << 24, seed=SEED, wmin=1, wmax=1000)
     if case.startswith("c5s"):
         return api.rmat_params(21, 1 << 25, 0.57, 0.19, 0.19, seed=SEED, wmin=1, wmax=1000)
     if case.startswith("c5"):

@@ -27,6 +27,24 @@ def test_tune_traversals_keeps_results(gpu_ctx):
         gpu_ctx.set_sssp_delta(0.0)
 
 
+def test_tune_batched_sssp_keeps_results(gpu_ctx):
+    """The batched SSSP's near-far width: every candidate tried, the best
+    left set, the distances unchanged."""
+    from medusa_b200 import api, autotune
+    g = gpu_ctx.generate(api.grid_params(96, 96, seed=4))
+    try:
+        srcs = list(range(0, 9216, 300))[:32]
+        d0, _ = g.sssp(srcs)
+        best, table = autotune.tune_batched_sssp(gpu_ctx, g, srcs, reps=1)
+        assert set(best) == {"mss_delta"} and len(table) == len(autotune.MSS_DELTAS)
+        assert gpu_ctx.get_tunable("mss_delta") == best["mss_delta"]
+        d1, _ = g.sssp(srcs)
+        np.testing.assert_array_equal(d0.view(np.uint32), d1.view(np.uint32))
+    finally:
+        g.close()
+        gpu_ctx.set_tunable("mss_delta", -1)
+
+
 def test_tune_batch(gpu_ctx):
     from medusa_b200 import api, autotune
     b = gpu_ctx.batch_generate([api.rmat_params(s, 8 << s, 0.45, 0.15, 0.15, seed=s)

@@ -490,9 +490,13 @@ def test_batched_bfs_c4_size_certificates(gpu_ctx, api):
     g.close()
 
 
+@pytest.mark.parametrize("delta", [-1, 0, 1, 7, 100, 5000], ids=lambda d: "delta%d" % d)
 @pytest.mark.parametrize("name", ["rmat_s10", "grid_24", "hub", "rmat_skew_s12", "tiny", "empty"])
-def test_batched_sssp_equals_single_source_runs(gpu_ctx, api, name):
-    """32-source batched SSSP: distances of every source equal the oracle's."""
+def test_batched_sssp_equals_single_source_runs(gpu_ctx, api, name, delta):
+    """32-source batched SSSP: distances of every source equal the oracle's,
+    with plain frontier Bellman-Ford (delta 0), the default near-far width
+    and widths from 1 (one bucket per distance) to past the largest
+    distance (a single bucket)."""
     c = load_golden(name)
     g = gpu_ctx.graph_from_edges(c["V"], c["src"], c["dst"], c["w"])
     rng = np.random.default_rng(5)
@@ -500,9 +504,37 @@ def test_batched_sssp_equals_single_source_runs(gpu_ctx, api, name):
     srcs[:len(c["sources"])] = list(c["sources"])
     if len(srcs) > 2:
         srcs[2] = srcs[1]
-    d, st = g.sssp(srcs)
+    gpu_ctx.set_tunable("mss_delta", delta)
+    try:
+        d, st = g.sssp(srcs)
+    finally:
+        gpu_ctx.set_tunable("mss_delta", -1)
     aa = O.AAGraph(c["V"], c["src"], c["dst"], c["w"])
     for i, s in enumerate(srcs):
         want, _ = O.sssp(c["V"], aa, None, None, s)
         np.testing.assert_array_equal(d[i], want, err_msg="source %d (#%d)" % (s, i))
+    g.close()
+
+
+def test_batched_sssp_near_far_full_size(gpu_ctx, api):
+    """32 sources on the 2^20 / 2^24 R-MAT: near-far buckets at the default
+    width and at 100 give the same distances as plain frontier Bellman-Ford;
+    source 5 also equals its single-source run."""
+    p = api.rmat_params(20, 1 << 24, 0.45, 0.15, 0.15, seed=1, wmin=1, wmax=1000)
+    g = gpu_ctx.generate(p)
+    srcs = list(range(32))
+    try:
+        gpu_ctx.set_tunable("mss_delta", 0)
+        d0, st0 = g.sssp(srcs)
+        for delta in (-1, 100):
+            gpu_ctx.set_tunable("mss_delta", delta)
+            d1, st1 = g.sssp(srcs)
+            np.testing.assert_array_equal(d1, d0, err_msg="delta %d" % delta)
+            assert st1["edges_traversed"] == st0["edges_traversed"]
+    finally:
+        gpu_ctx.set_tunable("mss_delta", -1)
+    gpu_ctx.set_batching(False)
+    one, _ = g.sssp([5])
+    gpu_ctx.set_batching(True)
+    np.testing.assert_array_equal(d0[5], one[0])
     g.close()
