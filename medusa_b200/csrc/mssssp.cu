@@ -176,27 +176,27 @@ __global__ void __launch_bounds__(256) k_mss_push(MsArgs a) {
                 fm = front[uk];
                 du = __ldcg(&a.dist[(size_t)uk * 32 + lane]);
             }
-            bool imp = false, nearb = false;
+            bool imp = false;
+            float nd = 0.f;
             if ((fm >> lane) & 1u) {
-                const float nd = du + wk;
+                nd = du + wk;
                 float *pv = &a.dist[(size_t)vk * 32 + lane];
                 if (nd < __ldcg(pv)) {
                     atomicMin((unsigned *)pv, __float_as_uint(nd));
                     imp = true;
-                    if (kNF) {
-                        if (nd < T) nearb = true;
-                        else fmn = fminf(fmn, nd);
-                    }
+                    if (kNF && !(nd < T)) fmn = fminf(fmn, nd);
                 }
             }
             const uint32_t mask = __ballot_sync(0xffffffffu, imp);
-            if (kNF) {
-                const uint32_t mn = __ballot_sync(0xffffffffu, nearb);
-                if (mask && lane == 0 &&
-                    atomicOr(&a.nxt2[vk], ((unsigned long long)(mask & ~mn) << 32) | mn) == 0ull)
+            if (mask) {  // warp-uniform
+                if (kNF) {
+                    const uint32_t mn = __ballot_sync(0xffffffffu, imp && nd < T);
+                    if (lane == 0 &&
+                        atomicOr(&a.nxt2[vk], ((unsigned long long)(mask & ~mn) << 32) | mn) == 0ull)
+                        newly |= 1u << k;
+                } else if (lane == 0 && atomicOr(&a.nxt[vk], mask) == 0u) {
                     newly |= 1u << k;
-            } else if (mask && lane == 0 && atomicOr(&a.nxt[vk], mask) == 0u) {
-                newly |= 1u << k;
+                }
             }
         }
         // one aggregated append per warp: lane e appends its edge's head
