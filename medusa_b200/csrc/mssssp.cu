@@ -253,32 +253,29 @@ __device__ __forceinline__ void append_warp(bool pred, int32_t v, uint32_t *cnt,
     if (pred) list[base + __popc(mask & lanemask_lt())] = v;
 }
 
-// commit: clear the old frontier masks; touched vertices take their new
-// masks and join the next queue.  With near-far buckets (kNF) only their
-// near pairs do; the far ones wait in far[v].
+// commit: touched vertices take their new masks and join the next queue.
+// With near-far buckets (kNF) only their near pairs do; the far ones wait
+// in far[v].  A mask is read only by the push over the queue it was
+// written for (every queue entry's mask is assigned by this kernel or the
+// far pass just before), so old masks are left as they are.
 template <bool kNF>
 __global__ void k_mss_commit(MsArgs a) {
     MsCtrl *c = a.c;
     if (c->done) return;
-    const int cur = c->cur, nx = cur ^ 1;
-    const uint32_t nold = (uint32_t)(c->q[cur] >> 32), nt = c->touched;
-    uint32_t *front_cur = cur ? a.front[1] : a.front[0];
-    uint32_t *front_nx = cur ? a.front[0] : a.front[1];
-    const int32_t *qv = cur ? a.qv[1] : a.qv[0];
+    const int nx = c->cur ^ 1;
+    const uint32_t nt = c->touched;
+    uint32_t *front_nx = nx ? a.front[1] : a.front[0];
     const int fl = kNF ? c->fl : 0;
     const int lane = threadIdx.x & 31;
-    const int64_t total = (int64_t)nold + nt;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < total;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < nt;
          base += warps * 32) {
         const int64_t i = base + lane;
         bool join = false, wait = false;
         int32_t v = 0;
         uint32_t deg = 0;
-        if (i < nold) {
-            front_cur[qv[i]] = 0u;
-        } else if (i < total) {
-            v = a.touched[i - nold];
+        if (i < nt) {
+            v = a.touched[i];
             uint32_t near;
             deg = (uint32_t)a.outdeg[v];
             if (kNF) {
@@ -292,8 +289,8 @@ __global__ void k_mss_commit(MsArgs a) {
                 near = a.nxt[v];
                 a.nxt[v] = 0u;
             }
-            front_nx[v] = near;
             join = deg > 0 && near != 0u;
+            if (join) front_nx[v] = near;
         }
         if (kNF) append_warp(wait, v, &c->nfar[fl], fl ? a.farl[1] : a.farl[0]);
         enqueue_warp(join, v, deg, &c->q[nx], nx ? a.qv[1] : a.qv[0], nx ? a.qo[1] : a.qo[0],
