@@ -20,7 +20,8 @@ the library's device time.  --hostloop runs the host-driven loop (kernels in
 conditional-node graphs are invisible to ncu); --trace prints each superstep
 of the last repetition (BFS 8 B per frontier out-edge + 20 B per frontier
 vertex, SSSP 12 + 20, as algorithmic bytes).  --set NAME=VALUE sets a
-tunable (medusa_b200.api.TUNABLES) before the runs; repeatable."""
+tunable (medusa_b200.api.TUNABLES) before the runs; repeatable.
+--sssp-delta W sets the single-source near-far width."""
 import argparse
 import sys
 
@@ -59,6 +60,8 @@ def main(argv=None):
     ap.add_argument("--pr-order", choices=["fixed", "reference"], default=None)
     ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
                     help="a tunable for the runs (e.g. sssp_async=1)")
+    ap.add_argument("--sssp-delta", type=float, default=None,
+                    help="single-source SSSP near-far width (0: none; -1: the per-graph default)")
     args = ap.parse_args(argv)
     ctx = api.Context(0)
     if args.hostloop:
@@ -66,6 +69,8 @@ def main(argv=None):
     for kv in args.set:
         name, value = kv.split("=", 1)
         ctx.set_tunable(name, int(value))
+    if args.sssp_delta is not None:
+        ctx.set_sssp_delta(args.sssp_delta)
     if args.pr_order:
         ctx.set_pagerank_order(api.MB_PR_ORDER_FIXED if args.pr_order == "fixed"
                                else api.MB_PR_ORDER_REFERENCE)
