@@ -17,9 +17,10 @@ distances come back device->host inside the timed region.
 `pagerank`: PageRank on the reference's CPU-runnable configuration (uniform,
 2^18 vertices, 2^22 edges, 10 supersteps from 1/N), edges/s per superstep.
 
-`configs`: C3 (1448x1448 road-like grid, BFS + SSSP from the corner), C4a
-(64 BFS + 32 SSSP sources on R-MAT 2^22/2^26, batched vs one loop per
-source, identical outputs) and C5 (R-MAT 2^24/2^28, (0.57,0.19,0.19,0.05):
+`configs`: C3 (1448x1448 road-like grid, BFS + SSSP from the corner, fixed
+vs learned schedule), C4a (64 BFS + 32 SSSP sources on R-MAT 2^22/2^26,
+batched and learned+batched vs one loop per source, identical outputs) and
+C5 (R-MAT 2^24/2^28, (0.57,0.19,0.19,0.05):
 BFS, SSSP and 20 PageRank supersteps, fixed vs learned schedule with HBM
 roofline fractions, plus per-superstep fixed / learned / oracle-best costs)
 and C4b (256 R-MAT graphs of uneven sizes, 20 PageRank supersteps + one BFS
@@ -508,16 +509,25 @@ def bench_configs(ctx, api, args, flush):
     tuned3 = {} if args.no_autotune else autotune.tune_traversals(ctx, g, 0, reps=2)[0]
     lv = torch.empty(V, dtype=torch.int32, device="cuda")
     dd = torch.empty(V, dtype=torch.float32, device="cuda")
-    for _ in range(2):
-        g.bfs([0], out=lv)
-        g.sssp([0], out=dd)
-    mb, sb = _timed(lambda: g.bfs([0], out=lv)[1], reps, flush)
-    ms_, ss = _timed(lambda: g.sssp([0], out=dd)[1], reps, flush)
+    # the fixed rule, then the learned scheduler (the same tuned parameters)
+    arms, res = {}, {}
+    for name, policy in (("learned", api.MB_POLICY_LEARNED), ("fixed", api.MB_POLICY_FIXED)):
+        ctx.set_policy(policy)
+        for _ in range(2):
+            g.bfs([0], out=lv)
+            g.sssp([0], out=dd)
+        mb, sb = _timed(lambda: g.bfs([0], out=lv)[1], reps, flush)
+        ms_, ss = _timed(lambda: g.sssp([0], out=dd)[1], reps, flush)
+        arms[name] = {"bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
+                      "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk)}
+        res[name] = (lv.cpu().numpy().copy(), dd.cpu().numpy().view(np.uint32).copy())
     out["c3_grid"] = {"workload": "grid 1448x1448, 10% edges dropped, 0.5% shortcuts, weights "
                                   "int [1,100], seed 1, source 0 (corner)",
                       "vertices": V, "edges": g.E,
-                      "bfs": _trav(sb, mb, bfs_bytes(sb, V), pk),
-                      "sssp": _trav(ss, ms_, sssp_bytes(ss, V), pk),
+                      "bfs": arms["fixed"]["bfs"], "sssp": arms["fixed"]["sssp"],
+                      "learned": arms["learned"],
+                      "learned_identical": bool(np.array_equal(res["fixed"][0], res["learned"][0]) and
+                                                np.array_equal(res["fixed"][1], res["learned"][1])),
                       "autotuned": {k: float(v) for k, v in tuned3.items()},
                       "verified_against_bsp": verify_against_bsp(ctx, api, g, lv, dd)}
     g.close()
@@ -537,8 +547,11 @@ def bench_configs(ctx, api, args, flush):
     c4 = {"workload": "R-MAT 2^22 vertices, 2^26 edges, (0.45,0.15,0.15,0.25), seed 1; "
                       "BFS sources 0..63, SSSP sources 0..31", "vertices": V, "edges": g.E}
     outs = {}
-    for name, batching in (("plain", False), ("batched", True)):
+    for name, batching, policy in (("plain", False, api.MB_POLICY_FIXED),
+                                   ("batched", True, api.MB_POLICY_FIXED),
+                                   ("learned_batched", True, api.MB_POLICY_LEARNED)):
         ctx.set_batching(batching)
+        ctx.set_policy(policy)
         g.bfs(list(range(64)), out=lv)
         g.sssp(list(range(32)), out=dd)
         mb, sb = _timed(lambda: g.bfs(list(range(64)), out=lv)[1], 1, flush)
@@ -550,9 +563,11 @@ def bench_configs(ctx, api, args, flush):
                                    / ((mb + ms_) / 1e3) / 1e9, 3),
                     "bfs_ms": round(mb, 3), "sssp_ms": round(ms_, 3)}
     ctx.set_batching(True)
-    c4["batched"]["vs_plain"] = round(c4["batched"]["gteps"] / c4["plain"]["gteps"], 3)
-    c4["identical"] = bool(np.array_equal(outs["plain"][0], outs["batched"][0]) and
-                           np.array_equal(outs["plain"][1], outs["batched"][1]))
+    ctx.set_policy(api.MB_POLICY_FIXED)
+    for name in ("batched", "learned_batched"):
+        c4[name]["vs_plain"] = round(c4[name]["gteps"] / c4["plain"]["gteps"], 3)
+    c4["identical"] = all(np.array_equal(outs["plain"][k], outs[name][k])
+                          for name in ("batched", "learned_batched") for k in (0, 1))
     out["c4a_batched"] = c4
     g.close()
     del lv, dd, outs
