@@ -1,8 +1,10 @@
 // mssssp.cu -- batched SSSP: up to 32 sources in one traversal.
 //
 // Distances are stored vertex-major, dist[v*32 + s], so the 32 distances of a
-// vertex fill one 128-byte line.  front[v] is the 32-bit mask of the sources
-// whose distance to v dropped in the last superstep.  A warp relaxes one edge
+// vertex fill one 128-byte line.  front[v], for a vertex of the current
+// queue, is the 32-bit mask of the sources whose distance to v dropped in
+// the last superstep (entries of other vertices are stale and never read).
+// A warp relaxes one edge
 // (u,v,w) for every source at once -- lane s holds source s -- so reading
 // and updating dist[v][*] is one coalesced line; the lanes that improved are
 // combined with __ballot_sync into v's mask of the next frontier.
@@ -12,13 +14,14 @@
 // batching itself.
 //
 // Near-far buckets (width delta > 0, MB_TUNE_MSS_DELTA): the frontier holds
-// only the (vertex, source) pairs whose distance is below a threshold T;
-// the commit moves a touched vertex's other pairs into far[v] (the vertex
-// joins a far list the first time), and when no near pair is left a far
-// pass raises T to the least deferred distance + delta and moves the pairs
-// now below it back into the queue.  Each pair is still relaxed until no
-// distance drops, so the distances are the same fixpoint; what changes is
-// how often an edge is relaxed before its tail's distance is final.
+// only the (vertex, source) pairs whose distance is below a threshold T.
+// The push marks each improved pair near or far in the head's 64-bit mask;
+// the commit queues the near pairs and moves the far ones into far[v] (the
+// vertex joins a far list the first time), and when no near pair is left a
+// far pass raises T to the least waiting distance + delta and moves the
+// pairs now below it back into the queue.  Each pair is still relaxed until
+// no distance drops, so the distances are the same fixpoint; what changes
+// is how often an edge is relaxed before its tail's distance is final.
 #include <algorithm>
 #include <cmath>
 #include "mssssp.cuh"
