@@ -38,6 +38,10 @@ TUNABLES = {"sssp_bm_push_min": 0, "push_blocks_per_sm": 1, "vertex_blocks_per_s
             "async_delta": 18, "async_blocks_per_sm": 19, "bfs_async": 20, "bfs_async_delta": 21,
             "async_below": 22, "mss_delta": 23}
 NUM_SCHEDULES = 8
+# schedule ids (MB_SCHED_* in include/medusa_b200.h)
+MB_SCHED_PUSH_EDGE_QUEUE, MB_SCHED_PUSH_WARP_QUEUE, MB_SCHED_PUSH_EDGE_BITMAP, \
+    MB_SCHED_PUSH_WARP_BITMAP, MB_SCHED_PULL_THREAD, MB_SCHED_PULL_WARP, MB_SCHED_PUSH_UNFUSED, \
+    MB_SCHED_PULL_UNFUSED = range(8)
 SCHEDULE_NAMES = ["push_edge_queue", "push_warp_queue", "push_edge_bitmap", "push_warp_bitmap",
                   "pull_thread", "pull_warp", "push_unfused", "pull_unfused"]
 MEDUSA_MAX = np.float32(1e9)

@@ -88,6 +88,15 @@ def evaluate(ctx, X, T, S, model=api.MB_MODEL_BFS):
     t_learned = T[idx, pick]
     ok = (t_fixed > 0) & (t_learned > 0)
     best = np.where(T > 0, T, np.inf).min(axis=1)
-    return {"fixed_ms": float(t_fixed[ok].sum()), "learned_ms": float(t_learned[ok].sum()),
-            "oracle_best_ms": float(best[ok].sum()), "samples": int(ok.sum()),
-            "unmeasured": int((~ok).sum())}
+    out = {"fixed_ms": float(t_fixed[ok].sum()), "learned_ms": float(t_learned[ok].sum()),
+           "oracle_best_ms": float(best[ok].sum()), "samples": int(ok.sum()),
+           "unmeasured": int((~ok).sum())}
+    # the reference's single schedule (its edge-centric superstep,
+    # MB_SCHED_PUSH_UNFUSED) where it was timed: what the model gains over it
+    ref = T[:, api.MB_SCHED_PUSH_UNFUSED]
+    ok_r = ok & (ref > 0)
+    if ok_r.any():
+        out["reference_schedule_ms"] = float(ref[ok_r].sum())
+        out["learned_ms_on_those"] = float(t_learned[ok_r].sum())
+        out["reference_samples"] = int(ok_r.sum())
+    return out

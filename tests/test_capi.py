@@ -46,6 +46,17 @@ def test_tunable_ids_match_the_header(api):
     assert sorted(ids.values()) == list(range(count))
 
 
+def test_schedule_ids_match_the_header(api):
+    """The Python MB_SCHED_* ids and SCHEDULE_NAMES follow the header's."""
+    text = open(os.path.join(ROOT, "include", "medusa_b200.h")).read()
+    ids = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (MB_SCHED_\w+) (\d+)", text)}
+    count = int(re.search(r"#define MB_NUM_SCHEDULES (\d+)", text).group(1))
+    assert count == api.NUM_SCHEDULES == len(api.SCHEDULE_NAMES)
+    assert ids and all(getattr(api, k) == v for k, v in ids.items())
+    for k, v in ids.items():
+        assert api.SCHEDULE_NAMES[v] == k[len("MB_SCHED_"):].lower()
+
+
 def test_version(api):
     assert "sm_100a" in api.version()
 

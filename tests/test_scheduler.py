@@ -138,10 +138,16 @@ def test_traces_are_well_formed(trained):
 
 
 @pytest.mark.gpu
-def test_learned_beats_or_matches_fixed_rule_on_held_out_traces(trained):
-    """What the trained networks gain over the fixed rule, per superstep
-    summed, on graphs they never saw (seed 99), printed; they must not lose
-    by more than timer noise."""
+def test_learned_gains_over_the_reference_schedule_on_held_out_traces(trained):
+    """What the trained networks gain, per superstep summed, on graphs they
+    never saw (seed 99), printed.  The method without them is the
+    reference's single fixed schedule (its edge-centric superstep over all
+    E edges, SSSP/UserOperators.h:200-264): the networks must beat it (by
+    more than 5%; at this size every superstep is ~10 us of launch-bound
+    work, so the sweep loses less than at scale).  Against this library's
+    own hand-tuned fixed rule, which is
+    within a few percent of the per-superstep best on these families, they
+    must not lose by more than timer noise."""
     from medusa_b200 import scheduler as S
     ctx, info, _, test = trained
     assert sorted(info) == [0, 1, 2]
@@ -151,6 +157,9 @@ def test_learned_beats_or_matches_fixed_rule_on_held_out_traces(trained):
         r = S.evaluate(ctx, X, T, F, model)
         print(name, "held-out:", r)
         assert r["samples"] >= 0.9 * len(X)
+        if model != 1:  # batched traces time push and pull only
+            assert r["reference_samples"] >= 0.9 * r["samples"], (name, r)
+            assert r["learned_ms_on_those"] * 1.05 <= r["reference_schedule_ms"], (name, r)
         # per-superstep times of 2^13-vertex graphs are ~10 us: allow timer noise
         assert r["learned_ms"] <= 1.15 * r["fixed_ms"], (name, r)
 
