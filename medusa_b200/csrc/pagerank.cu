@@ -313,7 +313,8 @@ __global__ void __launch_bounds__(kPrThreads) k_pr_light(PrArgs a) {
 //   kPrLight < n <= hub_min: sliced ELL -- vertices sorted by in-degree, 32
 //     per group; row j of a group holds slot j of each of its vertices, so a
 //     warp reads a row with one coalesced load and lane l folds its own
-//     vertex in order (k_pr_sell);
+//     vertex in order (k_pr_sell, on a second side stream beside the light
+//     kernel);
 //   n > hub_min: the contributions staged by every SM into one contiguous run
 //     per vertex (k_pr_hub_stage), then one CTA per vertex runs the parallel
 //     integer scan of pr_order.cuh over it (k_pr_hub_exact), on a side
@@ -392,6 +393,13 @@ __global__ void __launch_bounds__(256) k_pr_sell(ExactArgs a) {
 #ifndef MB_STAGE_ITEM
 #define MB_STAGE_ITEM 1024
 #endif
+// The sliced ELL runs on its own stream beside the light kernel and the hub
+// scans, on half its resident grid.  Measured per 20 supersteps against the
+// three in line on one stream: C5 27.7 against 28.0 ms, the C5 generator
+// at 2^21 / 2^25 3.77 against 4.60, R-MAT 2^20 / 2^24 1.00 against 1.23
+// (forked before the staging kernel instead, C5 lost 7%: the staging that
+// the big hubs' scans wait for ran slower).
+constexpr int kSellGridDiv = 2;
 constexpr int kStageItem = MB_STAGE_ITEM;
 constexpr int kStageU = 8;
 __global__ void __launch_bounds__(256) k_pr_hub_stage(ExactArgs a) {
@@ -937,6 +945,9 @@ void PrState::ensure_exact(Context &ctx, const Graph &g, int32_t hub_min) {
     if (!side) MB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     if (!ev_fork) MB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     if (!ev_join) MB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    if (!side2) MB_CUDA(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
+    if (!ev_fork2) MB_CUDA(cudaEventCreateWithFlags(&ev_fork2, cudaEventDisableTiming));
+    if (!ev_join2) MB_CUDA(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
     x_hub_min = hub_min;
     exact_built = true;
 }
@@ -1081,7 +1092,15 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                             x, nbig, st.x_nhub);
                     MB_CHECK_LAUNCH();
                 }
-                if (st.ngroups) k_pr_sell<<<grid_sell, 256, 0, cs>>>(x);
+                // the sliced ELL on its own stream with half the GPU: its
+                // longest groups (sequential folds) set its length, and the
+                // light kernel fills the SMs its tail leaves idle
+                if (st.ngroups) {
+                    MB_CUDA(cudaEventRecord(st.ev_fork2, cs));
+                    MB_CUDA(cudaStreamWaitEvent(st.side2, st.ev_fork2, 0));
+                    k_pr_sell<<<std::max(grid_sell / kSellGridDiv, 1), 256, 0, st.side2>>>(x);
+                    MB_CHECK_LAUNCH();
+                }
                 if (st.x_nlight) {
                     PrArgs la = a;
                     la.light_v = st.x_light_v.as<int32_t>();
@@ -1094,6 +1113,10 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                 if (st.x_nhub) {
                     MB_CUDA(cudaEventRecord(st.ev_join, st.side));
                     MB_CUDA(cudaStreamWaitEvent(cs, st.ev_join, 0));
+                }
+                if (st.ngroups) {
+                    MB_CUDA(cudaEventRecord(st.ev_join2, st.side2));
+                    MB_CUDA(cudaStreamWaitEvent(cs, st.ev_join2, 0));
                 }
                 continue;
             }

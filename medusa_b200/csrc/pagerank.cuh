@@ -37,6 +37,9 @@ struct PrState {
     // the hub kernel runs on a side stream beside the others (fork / join)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // the sliced-ELL kernel on a second side stream beside the others
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
     cudaGraphExec_t exec = nullptr;  // captured run (init + iters supersteps)
     int32_t g_iters = -1, g_sched = -1, g_order = -1;
     uint64_t g_tune = ~0ull;  // tunables generation of the captured run
@@ -57,8 +60,11 @@ struct PrState {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (side) cudaStreamDestroy(side);
-        ev_fork = ev_join = nullptr;
-        side = nullptr;
+        if (ev_fork2) cudaEventDestroy(ev_fork2);
+        if (ev_join2) cudaEventDestroy(ev_join2);
+        if (side2) cudaStreamDestroy(side2);
+        ev_fork = ev_join = ev_fork2 = ev_join2 = nullptr;
+        side = side2 = nullptr;
         built = false;
     }
     void release_exact() {
