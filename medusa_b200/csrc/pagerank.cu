@@ -942,12 +942,7 @@ void PrState::ensure_exact(Context &ctx, const Graph &g, int32_t hub_min) {
     copy_sync(s, stage_off.p, soff.data(), 8 * soff.size());
     if (nstage_items) copy_sync(s, stage_items.p, items.data(), sizeof(int4) * items.size());
     MB_CUDA(cudaStreamSynchronize(s));
-    if (!side) MB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-    if (!ev_fork) MB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-    if (!ev_join) MB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-    if (!side2) MB_CUDA(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
-    if (!ev_fork2) MB_CUDA(cudaEventCreateWithFlags(&ev_fork2, cudaEventDisableTiming));
-    if (!ev_join2) MB_CUDA(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
+    ensure_streams();
     x_hub_min = hub_min;
     exact_built = true;
 }
@@ -962,6 +957,7 @@ void run_pagerank(Context &ctx, Graph &g, PrState &st, int32_t iters, float init
                                 : kHubMinDefault;
     if (ref_order) build_meg_order(ctx, g, st);
     if (ref_order && !unfused) st.ensure_exact(ctx, g, hub_min);
+    st.ensure_streams();
     cudaStream_t s = ctx.stream;
     auto args = [&](int parity) {
         PrArgs a;

@@ -45,6 +45,15 @@ struct PrState {
     uint64_t g_tune = ~0ull;  // tunables generation of the captured run
     float g_init = 0.f;
     const float *g_init_vec = nullptr;  // the initial rank vector the capture reads
+    // the side streams and their fork / join events (once)
+    void ensure_streams() {
+        if (!side) MB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        if (!ev_fork) MB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        if (!ev_join) MB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        if (!side2) MB_CUDA(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
+        if (!ev_fork2) MB_CUDA(cudaEventCreateWithFlags(&ev_fork2, cudaEventDisableTiming));
+        if (!ev_join2) MB_CUDA(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
+    }
     ~PrState() { release(); }
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
