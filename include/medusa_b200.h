@@ -155,6 +155,16 @@ int mb_set_graph_capture(mb_ctx *ctx, int enable);
 int mb_graph_from_edges(mb_ctx *ctx, int32_t num_vertices, int64_t num_edges,
                         const int32_t *src, const int32_t *dst, const float *w,
                         uint32_t flags, mb_graph **out);
+/* Build a graph from a caller's CSR: row_ptr[V+1] (row_ptr[0] = 0,
+ * non-decreasing, row_ptr[V] = E), col[E] and optional weights w[E] (host or
+ * device memory); each row keeps the order given, and the reverse CSR and
+ * msgDstID are built on the device.  MB_ERR_INVALID for a bad row_ptr or a
+ * column id outside [0, V).  Replaces D_EdgeArray::Fill / D_VertexArray::Fill
+ * of the reference's CSR arrays (SSSP/EdgeDataType.cu:364-391,
+ * SSSP/VertexDataType.cu:88-160) with the reverse layout built by
+ * EdgeArray::buildAA (SSSP/EdgeDataType.cu:138-186). */
+int mb_graph_upload(mb_ctx *ctx, int32_t num_vertices, int64_t num_edges, const int32_t *row_ptr,
+                    const int32_t *col, const float *w, mb_graph **out);
 /* Generate a seeded synthetic graph directly in device memory (no reference
  * counterpart: the reference reads GTgraph files). */
 int mb_graph_generate(mb_ctx *ctx, const mb_gen_params *params, uint32_t flags,
@@ -291,6 +301,13 @@ int mb_vis_edge_lines(mb_ctx *ctx, const mb_graph *g, const float *pos, float *l
  * at [vbase[i], vbase[i+1]) (mb_batch_vertex_offsets); host or device. */
 typedef struct mb_batch mb_batch;
 int mb_batch_generate(mb_ctx *ctx, int32_t n, const mb_gen_params *params, mb_batch **out);
+/* The same from the caller's graphs: graph i has num_vertices[i] vertices
+ * (>= 1) and the num_edges[i] edges that follow graph i-1's in src / dst
+ * (host or device memory; ids local to the graph).  num_vertices and
+ * num_edges are host arrays of n entries. */
+int mb_graph_upload_batch(mb_ctx *ctx, int32_t n, const int32_t *num_vertices,
+                          const int64_t *num_edges, const int32_t *src, const int32_t *dst,
+                          mb_batch **out);
 int mb_batch_info(const mb_batch *b, int32_t *num_graphs, int64_t *total_vertices,
                   int64_t *total_edges);
 int mb_batch_vertex_offsets(const mb_batch *b, int64_t *vbase);

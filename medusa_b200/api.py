@@ -99,6 +99,7 @@ def _load():
         "mb_set_persistent_grid": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_set_batching": (ctypes.c_int, [P, ctypes.c_int]),
         "mb_graph_from_edges": (ctypes.c_int, [P, I32, I64, P, P, P, U32, ctypes.POINTER(P)]),
+        "mb_graph_upload": (ctypes.c_int, [P, I32, I64, P, P, P, ctypes.POINTER(P)]),
         "mb_graph_generate": (ctypes.c_int, [P, ctypes.POINTER(GenParams), U32,
                                              ctypes.POINTER(P)]),
         "mb_generate_edges_host": (ctypes.c_int, [ctypes.POINTER(GenParams), P, P, P,
@@ -124,6 +125,7 @@ def _load():
         "mb_vis_node_quads": (ctypes.c_int, [P, I32, P, P, P]),
         "mb_vis_edge_lines": (ctypes.c_int, [P, P, P, P]),
         "mb_batch_generate": (ctypes.c_int, [P, I32, P, ctypes.POINTER(P)]),
+        "mb_graph_upload_batch": (ctypes.c_int, [P, I32, P, P, P, P, ctypes.POINTER(P)]),
         "mb_batch_info": (ctypes.c_int, [P, ctypes.POINTER(I32), ctypes.POINTER(I64),
                                          ctypes.POINTER(I64)]),
         "mb_batch_vertex_offsets": (ctypes.c_int, [P, P]),
@@ -555,6 +557,19 @@ class Context:
                                        flags, ctypes.byref(g)), self.h)
         return Graph(self, g.value)
 
+    def graph_upload(self, V, row, col, w=None):
+        """Graph from a CSR (mb_graph_upload): row[V+1], col[E], optional w[E];
+        each row keeps its order."""
+        row = row if hasattr(row, "data_ptr") else np.ascontiguousarray(row, dtype=np.int32)
+        col = col if hasattr(col, "data_ptr") else np.ascontiguousarray(col, dtype=np.int32)
+        if w is not None and not hasattr(w, "data_ptr"):
+            w = np.ascontiguousarray(w, dtype=np.float32)
+        E = int(col.shape[0])
+        g = ctypes.c_void_p()
+        _check(lib.mb_graph_upload(self.h, int(V), E, _ptr(row), _ptr(col) if E else None,
+                                   _ptr(w) if (E and w is not None) else None, ctypes.byref(g)), self.h)
+        return Graph(self, g.value)
+
     def graph_from_gtgraph(self, text, reference_order=True):
         """Graph from GTgraph text: bytes, a str path, or a device uint8 tensor
         (parsed on the GPU)."""
@@ -576,6 +591,19 @@ class Context:
         h = ctypes.c_void_p()
         _check(lib.mb_batch_generate(self.h, len(params_list), ctypes.cast(arr, ctypes.c_void_p),
                                      ctypes.byref(h)), self.h)
+        return Batch(self, h.value)
+
+    def batch_upload(self, graphs):
+        """A batch from the caller's graphs (mb_graph_upload_batch): a list of
+        (V, src, dst) with ids local to each graph."""
+        nv = np.ascontiguousarray([int(V) for V, _, _ in graphs], dtype=np.int32)
+        ne = np.ascontiguousarray([len(s) for _, s, _ in graphs], dtype=np.int64)
+        src = np.ascontiguousarray(np.concatenate([np.asarray(s, np.int32) for _, s, _ in graphs]))
+        dst = np.ascontiguousarray(np.concatenate([np.asarray(d, np.int32) for _, _, d in graphs]))
+        h = ctypes.c_void_p()
+        _check(lib.mb_graph_upload_batch(self.h, len(graphs), nv.ctypes.data, ne.ctypes.data,
+                                         src.ctypes.data if len(src) else None,
+                                         dst.ctypes.data if len(dst) else None, ctypes.byref(h)), self.h)
         return Batch(self, h.value)
 
     def generate(self, params, reference_order=True):

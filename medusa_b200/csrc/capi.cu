@@ -487,6 +487,49 @@ int mb_graph_from_edges(mb_ctx *ctx, int32_t V, int64_t E, const int32_t *src, c
     return MB_OK;
 }
 
+int mb_graph_upload(mb_ctx *ctx, int32_t V, int64_t E, const int32_t *row_ptr, const int32_t *col,
+                    const float *w, mb_graph **out) {
+    if (!ctx || !out) return set_error(ctx, MB_ERR_INVALID, "null context or out");
+    *out = nullptr;
+    if (V < 1) return set_error(ctx, MB_ERR_INVALID, "num_vertices must be >= 1");
+    if (!row_ptr || E < 0 || (E > 0 && !col)) return set_error(ctx, MB_ERR_INVALID, "bad CSR arrays");
+    if (E > 0x7FFFFFFFll) return set_error(ctx, MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
+    mb_graph *g = new (std::nothrow) mb_graph();
+    if (!g) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        std::vector<int32_t> rp((size_t)V + 1);
+        mb::copy_sync(ctx->c.stream, rp.data(), row_ptr, sizeof(int32_t) * rp.size());
+        if (rp[0] != 0 || rp[(size_t)V] != E) mb::fail(MB_ERR_INVALID, "row_ptr must run from 0 to num_edges");
+        for (int32_t v = 0; v < V; v++)
+            if (rp[(size_t)v + 1] < rp[(size_t)v]) mb::fail(MB_ERR_INVALID, "row_ptr must not decrease");
+        mb::DevBuf br, bc, bw;
+        try {
+            const size_t eb = sizeof(uint32_t) * (size_t)std::max<int64_t>(E, 1);
+            br.reserve(sizeof(int32_t) * rp.size());
+            bc.reserve(eb);
+            if (w) bw.reserve(eb);
+            mb::copy_sync(ctx->c.stream, br.p, rp.data(), sizeof(int32_t) * rp.size());
+            if (E > 0) {
+                mb::copy_sync(ctx->c.stream, bc.p, col, 4 * (size_t)E);
+                if (w) mb::copy_sync(ctx->c.stream, bw.p, w, 4 * (size_t)E);
+            }
+            mb::graph_build_from_device_csr(ctx->c, g->g, V, E, br.as<int32_t>(), bc.as<uint32_t>(),
+                                            w ? bw.as<float>() : nullptr);
+        } catch (...) {
+            br.release(); bc.release(); bw.release();
+            throw;
+        }
+        br.release(); bc.release(); bw.release();
+    });
+    if (rc != MB_OK) {
+        mb_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return MB_OK;
+}
+
 int mb_graph_generate(mb_ctx *ctx, const mb_gen_params *p, uint32_t flags, mb_graph **out) {
     if (!ctx || !out || !p) return set_error(ctx, MB_ERR_INVALID, "null argument");
     *out = nullptr;
@@ -600,6 +643,34 @@ int mb_batch_generate(mb_ctx *ctx, int32_t n, const mb_gen_params *params, mb_ba
             if (params[i].kind != MB_GEN_GRID && params[i].num_edges > 0x7FFFFFFFll)
                 mb::fail(MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
         mb::batch_generate(ctx->c, b->b, params, n);
+    });
+    if (rc != MB_OK) {
+        mb_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return MB_OK;
+}
+
+int mb_graph_upload_batch(mb_ctx *ctx, int32_t n, const int32_t *nv, const int64_t *ne,
+                          const int32_t *src, const int32_t *dst, mb_batch **out) {
+    if (!ctx || !out || !nv || !ne) return set_error(ctx, MB_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (n < 1) return set_error(ctx, MB_ERR_INVALID, "a batch holds at least one graph");
+    int64_t total = 0;
+    for (int32_t i = 0; i < n; i++) {
+        if (nv[i] < 1) return set_error(ctx, MB_ERR_INVALID, "num_vertices must be >= 1");
+        if (ne[i] < 0) return set_error(ctx, MB_ERR_INVALID, "num_edges must be >= 0");
+        if (ne[i] > 0x7FFFFFFFll) return set_error(ctx, MB_ERR_UNSUPPORTED, "num_edges must be < 2^31");
+        total += ne[i];
+    }
+    if (total > 0 && (!src || !dst)) return set_error(ctx, MB_ERR_INVALID, "bad edge arrays");
+    mb_batch *b = new (std::nothrow) mb_batch();
+    if (!b) return set_error(ctx, MB_ERR_OOM, "host allocation failed");
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        b->device = ctx->c.device;
+        mb::batch_from_edges(ctx->c, b->b, n, nv, ne, src, dst);
     });
     if (rc != MB_OK) {
         mb_batch_destroy(b);

@@ -272,6 +272,40 @@ void graph_build_from_device_edges(Context &ctx, Graph &g, int32_t V, int64_t E,
     cnt.release(); vals.release(); flag.release();
 }
 
+// CSR -> edge list: edge e's source is the last v with row[v] <= e (row
+// checked on the host: row[0] = 0, non-decreasing, row[V] = E, so the
+// search interval [0, V] always brackets e).
+__global__ void k_csr_expand(const int32_t *row, int32_t V, int64_t E, uint32_t *src) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int32_t lo = 0, hi = V;  // row[lo] <= e < row[hi]
+        while (hi - lo > 1) {
+            const int32_t mid = lo + ((hi - lo) >> 1);
+            if ((int64_t)__ldg(&row[mid]) <= e) lo = mid; else hi = mid;
+        }
+        src[e] = (uint32_t)lo;
+    }
+}
+
+void graph_build_from_device_csr(Context &ctx, Graph &g, int32_t V, int64_t E, const int32_t *d_row,
+                                 uint32_t *d_col, float *d_w) {
+    DevBuf src;
+    try {
+        src.reserve(sizeof(uint32_t) * (size_t)std::max<int64_t>(E, 1));
+        if (E > 0) {
+            k_csr_expand<<<grid_for(E, 256, ctx.num_sms * 16), 256, 0, ctx.stream>>>(d_row, V, E,
+                                                                                     src.as<uint32_t>());
+            MB_CHECK_LAUNCH();
+        }
+        // the stable sort by source keeps each row in the order given
+        graph_build_from_device_edges(ctx, g, V, E, src.as<uint32_t>(), d_col, d_w, 0);
+    } catch (...) {
+        src.release();
+        throw;
+    }
+    src.release();
+}
+
 // ---------------------------------------------------------------------------
 // generator front ends
 

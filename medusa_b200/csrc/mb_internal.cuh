@@ -102,6 +102,10 @@ void radix_sort_pairs(Context &ctx, uint32_t *keys, uint32_t *vals, int64_t n, i
 void graph_build_from_device_edges(Context &ctx, Graph &g, int32_t V, int64_t E,
                                    uint32_t *d_src, uint32_t *d_dst, float *d_w,
                                    uint32_t flags);
+// A caller's CSR (row checked on the host) -> graph; each row keeps its
+// order.  d_col is used as scratch.
+void graph_build_from_device_csr(Context &ctx, Graph &g, int32_t V, int64_t E, const int32_t *d_row,
+                                 uint32_t *d_col, float *d_w);
 // GTgraph text (host or device bytes) -> graph (gtgraph.cu).
 void graph_from_gtgraph(Context &ctx, Graph &g, const char *text, int64_t len, uint32_t flags);
 

@@ -262,20 +262,59 @@ __global__ void k_multi(MultiArgs a) {
 
 }  // namespace
 
+// Keep the CSR and the reverse CSR of graph i (all the batch kernel reads)
+// and count it into the batch's vertex offsets.
+static void batch_take(Batch &b, int32_t i) {
+    b.graphs[i].esrc.release();
+    b.graphs[i].wt.release();
+    b.graphs[i].rwt.release();
+    b.graphs[i].mslot.release();
+    b.vbase.push_back(b.vbase.back() + b.graphs[i].V);
+    b.total_E += b.graphs[i].E;
+}
+
 void batch_generate(Context &ctx, Batch &b, const mb_gen_params *params, int32_t n) {
     b.release();
     b.graphs.resize(n);
     b.vbase.assign(1, 0);
     for (int32_t i = 0; i < n; i++) {
         graph_generate(ctx, b.graphs[i], params[i], MB_ORDER_REFERENCE);
-        // the batch kernel needs the CSR and the reverse CSR only
-        b.graphs[i].esrc.release();
-        b.graphs[i].wt.release();
-        b.graphs[i].rwt.release();
-        b.graphs[i].mslot.release();
-        b.vbase.push_back(b.vbase.back() + b.graphs[i].V);
-        b.total_E += b.graphs[i].E;
+        batch_take(b, i);
     }
+    batch_finish(b);
+}
+
+void batch_from_edges(Context &ctx, Batch &b, int32_t n, const int32_t *nv, const int64_t *ne,
+                      const int32_t *src, const int32_t *dst) {
+    b.release();
+    b.graphs.resize(n);
+    b.vbase.assign(1, 0);
+    int64_t e0 = 0;
+    for (int32_t i = 0; i < n; i++) {
+        DevBuf bs, bd;
+        try {
+            const size_t eb = sizeof(uint32_t) * (size_t)std::max<int64_t>(ne[i], 1);
+            bs.reserve(eb);
+            bd.reserve(eb);
+            copy_sync(ctx.stream, bs.p, src + e0, 4 * (size_t)ne[i]);
+            copy_sync(ctx.stream, bd.p, dst + e0, 4 * (size_t)ne[i]);
+            graph_build_from_device_edges(ctx, b.graphs[i], nv[i], ne[i], bs.as<uint32_t>(),
+                                          bd.as<uint32_t>(), nullptr, MB_ORDER_REFERENCE);
+        } catch (...) {
+            bs.release();
+            bd.release();
+            throw;
+        }
+        bs.release();
+        bd.release();
+        batch_take(b, i);
+        e0 += ne[i];
+    }
+    batch_finish(b);
+}
+
+void batch_finish(Batch &b) {
+    const int32_t n = (int32_t)b.graphs.size();
     b.total_V = b.vbase.back();
     const size_t vb = (size_t)std::max<int64_t>(b.total_V, 1);
     for (int i = 0; i < 2; i++) {

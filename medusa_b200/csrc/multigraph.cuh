@@ -43,6 +43,13 @@ struct Batch {
 
 // Build the batch's graphs (reference order) from generator parameters.
 void batch_generate(Context &ctx, Batch &b, const mb_gen_params *params, int32_t n);
+// Build the batch's graphs (reference order) from the caller's edge lists:
+// graph i has nv[i] vertices and the ne[i] edges that follow graph i-1's in
+// src / dst (host or device memory), with ids local to the graph.
+void batch_from_edges(Context &ctx, Batch &b, int32_t n, const int32_t *nv, const int64_t *ne,
+                      const int32_t *src, const int32_t *dst);
+// The batch's work buffers, after its graphs are built.
+void batch_finish(Batch &b);
 
 // One persistent cooperative launch: for every graph, `pr_iters` PageRank
 // supersteps from 1/V_g, then one BFS from sources[g] (nullptr: vertex 0).
