@@ -40,6 +40,9 @@ struct PrState {
     // the sliced-ELL kernel on a second side stream beside the others
     cudaStream_t side2 = nullptr;
     cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
+    // the warp-per-hub scans on a third, beside the big hubs' CTAs
+    cudaStream_t side3 = nullptr;
+    cudaEvent_t ev_join3 = nullptr;
     cudaGraphExec_t exec = nullptr;  // captured run (init + iters supersteps)
     int32_t g_iters = -1, g_sched = -1, g_order = -1;
     uint64_t g_tune = ~0ull;  // tunables generation of the captured run
@@ -53,6 +56,8 @@ struct PrState {
         if (!side2) MB_CUDA(cudaStreamCreateWithFlags(&side2, cudaStreamNonBlocking));
         if (!ev_fork2) MB_CUDA(cudaEventCreateWithFlags(&ev_fork2, cudaEventDisableTiming));
         if (!ev_join2) MB_CUDA(cudaEventCreateWithFlags(&ev_join2, cudaEventDisableTiming));
+        if (!side3) MB_CUDA(cudaStreamCreateWithFlags(&side3, cudaStreamNonBlocking));
+        if (!ev_join3) MB_CUDA(cudaEventCreateWithFlags(&ev_join3, cudaEventDisableTiming));
     }
     ~PrState() { release(); }
     void release() {
@@ -72,8 +77,10 @@ struct PrState {
         if (ev_fork2) cudaEventDestroy(ev_fork2);
         if (ev_join2) cudaEventDestroy(ev_join2);
         if (side2) cudaStreamDestroy(side2);
-        ev_fork = ev_join = ev_fork2 = ev_join2 = nullptr;
-        side = side2 = nullptr;
+        if (ev_join3) cudaEventDestroy(ev_join3);
+        if (side3) cudaStreamDestroy(side3);
+        ev_fork = ev_join = ev_fork2 = ev_join2 = ev_join3 = nullptr;
+        side = side2 = side3 = nullptr;
         built = false;
     }
     void release_exact() {
