@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(256) k_pr_sell(ExactArgs a) {
 // at 2^21 / 2^25 3.77 against 4.60, R-MAT 2^20 / 2^24 1.00 against 1.23
 // (forked before the staging kernel instead, C5 lost 7%: the staging that
 // the big hubs' scans wait for ran slower).
-constexpr int kSellGridDiv = 2;
+constexpr int kSellGridDiv = 2;  // C5: 24.0 ms per 20 supersteps, against 25.1 at 1 and 28.0 at 3
 constexpr int kStageItem = MB_STAGE_ITEM;
 constexpr int kStageU = 8;
 __global__ void __launch_bounds__(256) k_pr_hub_stage(ExactArgs a) {
