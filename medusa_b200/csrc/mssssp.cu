@@ -42,7 +42,7 @@ struct MsCtrl {
     unsigned long long work;  // edges relaxed (for all sources of a batch)
     // near-far buckets (delta > 0)
     float T;            // pairs at distance >= T wait in far[v]
-    uint32_t fmin;      // float bits: least distance of a waiting pair (a lower bound)
+    uint32_t fmin;      // float bits: least distance recorded for a parked pair since the last far pass
     int32_t fl;         // the far list that receives newly waiting vertices
     int32_t advance;    // 1: the queue is empty and pairs wait
     uint32_t nfar[2];   // far list lengths
@@ -301,8 +301,15 @@ __global__ void k_mss_commit(MsArgs a) {
     }
 }
 
-// The queue ran dry with pairs waiting: T becomes the least waiting distance
-// + delta (so at least that pair is below it), and the far lists swap.
+// The queue ran dry with pairs waiting: T becomes fmin + delta and the far
+// lists swap.  fmin >= T (recorded under the current threshold) and the
+// pair that set it has a distance <= fmin, so the far pass requeues it --
+// unless that pair was also improved below T in the same superstep (near
+// won, it is not parked).  Then the pass may requeue nothing; it leaves
+// fmin exact (the least parked distance), and the next superstep, empty,
+// ends in another far pass that does requeue.  (A parked pair whose
+// distance dropped later through a near improvement lies below T and is
+// simply requeued once more.)
 __global__ void k_mss_advance(MsArgs a) {
     MsCtrl *c = a.c;
     if (!c->advance) return;
