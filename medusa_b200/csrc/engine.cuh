@@ -96,7 +96,9 @@ struct Ctrl {
     uint32_t pad_bar;
     int32_t persist_go;       // persistent grid: run another superstep
     int32_t peaked;           // SSSP: a frontier reached p.async_below out-edges
-    int32_t pad_peaked;
+    uint32_t far_min;         // SSSP near-far: float bits of the least distance the last split kept (+inf: none)
+    float thresh_prev;        // SSSP near-far: the threshold before the last raise
+    int32_t pad_far;
 };
 
 // Frontier buffers and graph shape every engine kernel sees.
@@ -206,8 +208,19 @@ __device__ inline void choose_next(Ctrl *c, int app, int32_t V, int64_t E) {
     }
     if (n == 0 || m == 0) {  // nothing left to expand
         if (app == APP_SSSP && ctl_ld<kL2>(&c->far_n[c->fcur]) > 0) {
-            // near-far: next bucket
-            c->thresh += c->p.delta;
+            // near-far: next bucket.  The threshold rises by delta, and past
+            // the least distance the last split kept in the far pile (empty
+            // buckets are skipped: their count would not be bounded by the
+            // superstep cap); one float step further where a sum rounds back.
+            const float fm = __uint_as_float(ctl_ld<kL2>(&c->far_min));
+            const bool known = fm < __uint_as_float(0x7f800000u);
+            float t = c->thresh + c->p.delta;
+            if (known) t = fmaxf(t, fm + c->p.delta);
+            if (!(t > c->thresh)) t = __uint_as_float(__float_as_uint(c->thresh) + 1u);
+            if (known && !(t > fm)) t = __uint_as_float(__float_as_uint(fm) + 1u);
+            c->thresh_prev = c->thresh;
+            c->thresh = t;
+            c->far_min = 0x7f800000u;
             c->sched = kSchedSplit;
             c->branch = route(c, kSchedSplit);
             return;

@@ -313,7 +313,11 @@ __global__ void k_mss_commit(MsArgs a) {
 __global__ void k_mss_advance(MsArgs a) {
     MsCtrl *c = a.c;
     if (!c->advance) return;
-    c->T = __uint_as_float(c->fmin) + a.delta;
+    const float fm = __uint_as_float(c->fmin);
+    float t = fm + a.delta;
+    if (fm < __uint_as_float(kMsInfBits) && !(t > fm))
+        t = __uint_as_float(c->fmin + 1u);  // the sum rounded back: one float step
+    c->T = t;
     c->fmin = kMsInfBits;
     c->fl ^= 1;
     c->nfar[c->fl] = 0u;

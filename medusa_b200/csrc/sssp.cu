@@ -955,14 +955,17 @@ __global__ void __launch_bounds__(kTailThreads, MB_TAIL_MIN_BLOCKS) k_tail(SsspA
     ctrl_shadow_out(gc, &s_ctrl);
 }
 
-// Near-far split: the threshold was just raised by delta; every far-pile
-// vertex now below it joins the near queue, the rest move to the other pile.
+// Near-far split: the threshold was just raised (by delta, and past the
+// least distance the last split kept); every far-pile vertex now below it
+// joins the near queue, the rest move to the other pile, and the least
+// distance kept is recorded for the next raise.
 __device__ __forceinline__ void work_far_split(const SsspArgs &a) {
     Ctrl *c = a.f.ctrl;
     const int f = c->fcur;
     const uint32_t n = c->far_n[f];
     const int32_t *src = pick(a.far, f);
-    const float thresh = c->thresh, thresh_prev = c->thresh - c->p.delta;
+    const float thresh = c->thresh, thresh_prev = c->thresh_prev;
+    float kept_min = __uint_as_float(0x7f800000u);  // least distance this warp keeps parked
     const int nxt = c->cur ^ 1;
     const int32_t sv = c->step + 1;
     const int lane = threadIdx.x & 31;
@@ -990,6 +993,7 @@ __device__ __forceinline__ void work_far_split(const SsspArgs &a) {
                 }
             } else {
                 keep = true;
+                kept_min = fminf(kept_min, d);
             }
         }
         enqueue_warp(near && deg > 0, v, deg, &c->q[nxt], pick(a.f.qv, nxt), pick(a.f.qo, nxt),
@@ -1004,6 +1008,10 @@ __device__ __forceinline__ void work_far_split(const SsspArgs &a) {
             if (keep) pick(a.far, f ^ 1)[b + __popc(mask & lanemask_lt())] = v;
         }
     }
+    // the next raise skips to this (distances are non-negative: float bits
+    // order like the numbers)
+    const unsigned km = __reduce_min_sync(0xffffffffu, __float_as_uint(kept_min));
+    if (lane == 0 && km < 0x7f800000u) atomicMin(&c->far_min, km);
     flush_counts(c, cn, 0);
 }
 
@@ -1065,6 +1073,8 @@ __global__ void k_sssp_init(SsspArgs a) {
         c->work = 0;
         c->pending = 0;
         c->thresh = c->p.delta;
+        c->thresh_prev = 0.f;
+        c->far_min = 0x7f800000u;
         c->far_n[0] = 0;
         c->far_n[1] = 0;
         c->fcur = 0;

@@ -227,6 +227,39 @@ def test_sssp_every_delta_identical(gpu_ctx, api, name):
         g.close()
 
 
+def test_sssp_near_far_skips_empty_buckets(gpu_ctx, api):
+    """Distances far apart in units of the width: a directed 8-vertex path of
+    weight-1000 edges (plus a shortcut) spans 7000 buckets of width 1, far
+    more than the superstep cap (4 V + 16 = 48); the raise skips to the
+    least parked distance, so every width ends with the oracle's distances.
+    Weights of 3e7 put distances past 2^24, where T + 1 rounds back to T:
+    the threshold then steps one float past the least parked distance."""
+    n = 8
+    src = np.concatenate([np.arange(n - 1), [0]]).astype(np.int32)
+    dst = np.concatenate([np.arange(1, n), [5]]).astype(np.int32)
+    for wv in (1000.0, 3.0e7):
+        w = np.full(n, wv, np.float32)
+        w[-1] = 4.5 * wv  # the shortcut 0 -> 5
+        g = gpu_ctx.graph_from_edges(n, src, dst, w)
+        want, _ = O.sssp(n, src, dst, w, 0)
+        try:
+            for delta in (1.0, 0.5, 3.0, 999.0):
+                gpu_ctx.set_sssp_delta(delta)
+                d, st = g.sssp([0])
+                np.testing.assert_array_equal(d[0], want, err_msg="weights %g, delta %g" % (wv, delta))
+                assert st["supersteps"] <= 4 * n + 16
+            # batched, with near-far buckets over the (vertex, source) pairs
+            gpu_ctx.set_sssp_delta(0.0)
+            gpu_ctx.set_tunable("mss_delta", 1)
+            db, _ = g.sssp([0, 1, 0])
+            np.testing.assert_array_equal(db[0], want)
+            np.testing.assert_array_equal(db[1], O.sssp(n, src, dst, w, 1)[0])
+        finally:
+            gpu_ctx.set_sssp_delta(0.0)
+            gpu_ctx.set_tunable("mss_delta", -1)
+            g.close()
+
+
 def test_oracle_replay_policy(gpu_ctx, api):
     """A per-superstep schedule list (alternating push/pull) gives the same levels."""
     c = load_golden("rmat_s10")
