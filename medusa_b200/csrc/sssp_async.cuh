@@ -275,6 +275,10 @@ __device__ __forceinline__ void async_idle(Ctrl *c, AsyncState *S, uint32_t *s_i
     const float m = __uint_as_float(mb);
     float tn = T + delta;
     if (m < __uint_as_float(kInfBits) && m + delta > tn) tn = m + delta;
+    // where a sum rounds back (distances past 2^24, a small step), one float
+    // step past the least distance seen above T, so that vertex is below tn
+    if (!(tn > T)) tn = __uint_as_float(__float_as_uint(T) + 1u);
+    if (m < __uint_as_float(kInfBits) && !(tn > m)) tn = __uint_as_float(mb + 1u);
     const uint32_t r2 = atomicExch((unsigned *)&S->idle[(ph + 1) & 1].v, 0u);
     const uint32_t nph = ph + 1u + (r2 >> 31) + (mb >> 31);  // both shifts zero
     atomicExch(&S->pt.v, ((unsigned long long)nph << 32) | __float_as_uint(tn));

@@ -274,6 +274,27 @@ def test_async_sssp_zero_weights_and_a_zero_cycle(actx, api):
         g.close()
 
 
+def test_async_sssp_threshold_past_2_24(actx, api):
+    """Distances past 2^24 with a threshold step of 1, where T + 1 rounds
+    back to T: the step goes one float past the least distance above T, so
+    the run ends with the oracle's distances."""
+    n = 8
+    src = np.concatenate([np.arange(n - 1), [0]]).astype(np.int32)
+    dst = np.concatenate([np.arange(1, n), [5]]).astype(np.int32)
+    w = np.full(n, 3.0e7, np.float32)
+    w[-1] = 1.35e8
+    g = actx.graph_from_edges(n, src, dst, w)
+    try:
+        want, _ = O.sssp(n, src, dst, w, 0)
+        for delta in (1, 2, 100):
+            actx.set_tunable("async_delta", delta)
+            got, st = g.sssp([0])
+            np.testing.assert_array_equal(got[0], want, err_msg="delta %d" % delta)
+    finally:
+        actx.set_tunable("async_delta", -1)
+        g.close()
+
+
 def test_async_sssp_fractional_weights_equal_the_bsp_loop(gpu_ctx, api):
     """Non-integer weights: the distances are the least fixpoint of
     d[v] = min over in-edges of fl(d[u] + w), which every order of
