@@ -514,8 +514,10 @@ void run_mssssp(Context &ctx, Graph &g, MsSsspState &st, const int32_t *sources,
         launches += 2;
         MB_CHECK_LAUNCH();
         // every superstep lowers some distance; integer distances below 2^24
-        // bound the count well below this cap
-        const int64_t cap = step_cap(ctx, (int64_t)g.V * 4 + 16);
+        // bound the count well below this cap.  With buckets a bucket may
+        // advance a single (vertex, source) pair, so the cap scales with the
+        // sources.
+        const int64_t cap = step_cap(ctx, ((int64_t)g.V * 4 + 16) * (nf ? nsrc : 1));
         // the control block is read after the first superstep and then after
         // every kSupersteps queued ones (the kernels of a superstep queued
         // past the last one return at once)

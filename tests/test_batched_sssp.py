@@ -95,6 +95,27 @@ def test_one_source_in_every_lane(bctx, api):
         g.close()
 
 
+def test_buckets_with_every_pair_at_its_own_distance(bctx, api):
+    """A 20-vertex path whose edge weights make every (vertex, source)
+    distance distinct, 20 sources, width 1: a bucket may advance a single
+    pair, 190 buckets in all -- more than 4 V + 16 supersteps, within the
+    cap of the bucketed loop (which scales with the sources)."""
+    n = 20
+    src = np.arange(n - 1, dtype=np.int32)
+    dst = src + 1
+    w = (1000 + 37 * np.arange(n - 1) ** 2).astype(np.float32)
+    g = bctx.graph_from_edges(n, src, dst, w)
+    try:
+        bctx.set_tunable("mss_delta", 1)
+        srcs = list(range(n))
+        got, st = g.sssp(srcs)
+        for i, s0 in enumerate(srcs):
+            np.testing.assert_array_equal(got[i], O.sssp(n, src, dst, w, s0)[0])
+        assert st["supersteps"] > 4 * n + 16
+    finally:
+        g.close()
+
+
 def test_superstep_cap_with_buckets(bctx, api):
     """A superstep cap of 1 stops the bucketed loop with MB_ERR_TIMEOUT; the
     same context then runs it to the oracle's distances."""
