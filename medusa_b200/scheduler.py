@@ -51,10 +51,10 @@ def collect(ctx, seeds, apps=(0, 1), scales=(14,)):
 def train(ctx, seeds=(101, 102), scales=(14,), epochs=1500, lr=3e-3, seed=7, rounds=2):
     """Train both models; returns {model: (final loss, samples)}.
 
-    Round 1 learns from traces along the fixed rule's trajectories.  Each
-    further round collects traces along the trained policy's own
-    trajectories (states where it departed from the fixed rule), adds them
-    to the set and retrains (dataset aggregation)."""
+    The first training pass learns from traces along the fixed rule's
+    trajectories.  Each further pass (`rounds` in all) collects traces along
+    the trained policy's own trajectories (states where it departed from the
+    fixed rule), adds them to the set and retrains (dataset aggregation)."""
     out = {}
     sets = {api.MB_MODEL_BFS: ((0,), [], []), api.MB_MODEL_SSSP: ((1,), [], []),
             api.MB_MODEL_BATCHED: ((2,), [], [])}
