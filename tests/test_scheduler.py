@@ -37,6 +37,41 @@ def test_features_are_absolute_log_counts():
     np.testing.assert_allclose(f, [10 / 32, 20 / 32, 0, 0, 1.0, 1.0])
 
 
+def test_evaluate_sums_each_policy_over_the_measured_samples():
+    """scheduler.evaluate on a fake context: the fixed rule's, the model's
+    and the best schedule's summed times over the samples where both the
+    fixed and the model's choice were timed, and the reference's single
+    schedule (MB_SCHED_PUSH_UNFUSED) over those where it was timed too."""
+    from medusa_b200 import api, scheduler as S
+
+    class Fake:
+        def __init__(self, picks):
+            self.picks = np.asarray(picks)
+
+        def scheduler_pick(self, X, model, fallback=None):
+            return self.picks
+
+    T = np.full((4, api.NUM_SCHEDULES), -1.0)
+    T[0, [0, 4, 6]] = [2.0, 1.0, 9.0]
+    T[1, [0, 4, 6]] = [3.0, 5.0, 8.0]
+    T[2, [0, 4]] = [1.0, 1.5]           # the reference's schedule not timed
+    T[3, [0]] = [4.0]                   # the model's choice not timed: left out
+    X = np.zeros((4, 6), np.float32)
+    fixed = np.array([0, 0, 0, 0])
+    r = S.evaluate(Fake([4, 0, 4, 4]), X, T, fixed, api.MB_MODEL_BFS)
+    assert r["samples"] == 3 and r["unmeasured"] == 1
+    assert r["fixed_ms"] == 2.0 + 3.0 + 1.0
+    assert r["learned_ms"] == 1.0 + 3.0 + 1.5
+    assert r["oracle_best_ms"] == 1.0 + 3.0 + 1.0
+    assert r["reference_samples"] == 2
+    assert r["reference_schedule_ms"] == 9.0 + 8.0
+    assert r["learned_ms_on_those"] == 1.0 + 3.0
+    # traces that never timed the reference's schedule (batched BFS) report none
+    T2 = T.copy()
+    T2[:, api.MB_SCHED_PUSH_UNFUSED] = -1.0
+    assert "reference_schedule_ms" not in S.evaluate(Fake([4, 0, 4, 4]), X, T2, fixed)
+
+
 def test_targets_prefer_fast_schedules():
     q = M.targets(np.array([[1.0, 2.0, -1, 1.0, 4.0, 1.1, 9.0, 1.0]]))
     assert q[0, 2] == 0 and np.isclose(q.sum(), 1)
