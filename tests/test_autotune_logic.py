@@ -59,3 +59,33 @@ def test_joint_search_tries_a_switch_with_each_of_its_parameters():
                                       reps=1)
     assert best == {"a": 1, "b": 200} and ctx.t == {"a": 1, "b": 200}
     assert len(table) == 5  # the current setting, then the four others
+
+
+def test_batched_sssp_width_search_keeps_the_fastest_width():
+    """tune_batched_sssp times every candidate width over the given sources
+    and leaves the fastest set."""
+    from medusa_b200 import autotune
+
+    class Ctx:
+        def __init__(self):
+            self.t = {"mss_delta": -1}
+
+        def get_tunable(self, name):
+            return self.t[name]
+
+        def set_tunable(self, name, value):
+            self.t[name] = value
+
+    ctx = Ctx()
+    seen = []
+
+    class Graph:
+        def sssp(self, sources):
+            seen.append(list(sources))
+            d = ctx.t["mss_delta"]
+            return None, {"device_ms": 5.0 if d <= 0 else abs(d - 150) / 50 + 1.0}
+
+    best, table = autotune.tune_batched_sssp(ctx, Graph(), range(32), reps=1)
+    assert best == {"mss_delta": 150} and ctx.t["mss_delta"] == 150
+    assert sorted(t["mss_delta"] for t, _ in table) == sorted(autotune.MSS_DELTAS)
+    assert all(s == list(range(32)) for s in seen)
